@@ -1,0 +1,32 @@
+"""B200-native RNS-CKKS evaluator path (sm_100a kernels behind a C ABI, include/ckg.h).
+
+This directory is imported under the module name ``ckks_train_b200`` (its name has a
+hyphen, so loaders register it by path; see ``load_package`` in bench.py).
+"""
+
+from .heops import (  # noqa: F401
+    BSGS,
+    HOIST,
+    LAZY_RELIN,
+    COUNTER_FIELDS,
+    Ciphertext,
+    Context,
+    CudaEvaluator,
+    Decode,
+    Device,
+    EvalConfig,
+    HekitError,
+    InvalidParams,
+    Key,
+    LevelMismatch,
+    LIB_PATH,
+    NoLevelsLeft,
+    OutOfMemory,
+    Plaintext,
+    ScaleMismatch,
+    Timeout,
+    build,
+    launch_count,
+    lib,
+    primes_for_bits,
+)

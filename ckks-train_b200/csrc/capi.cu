@@ -1,0 +1,504 @@
+// extern "C" entry points of include/ckg.h: handle wrapping, argument checks and the
+// translation of C++ errors and CUDA failures into status codes (nothing throws or
+// aborts across the boundary).
+#include <cstring>
+#include <string>
+
+#include "../../include/ckg.h"
+#include "evaluator.hpp"
+
+using namespace ckg;
+
+struct ckg_ctx {
+  std::unique_ptr<Context> c;
+};
+struct ckg_key {
+  KeyPtr k;
+};
+struct ckg_eval {
+  std::unique_ptr<Evaluator> e;
+};
+struct ckg_ct {
+  Ct c;
+};
+struct ckg_pt {
+  Pt p;
+};
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CKG_API_BEGIN try {
+#define CKG_API_END                                                       \
+  }                                                                       \
+  catch (const Error& e) {                                                \
+    return fail(e.code, e.what());                                        \
+  }                                                                       \
+  catch (const std::bad_alloc&) {                                         \
+    return fail(CKG_OOM, "out of host memory");                           \
+  }                                                                       \
+  catch (const std::invalid_argument& e) {                                \
+    return fail(CKG_INVALID_PARAMS, e.what());                            \
+  }                                                                       \
+  catch (const std::exception& e) {                                       \
+    return fail(CKG_DEVICE, std::string("internal error: ") + e.what()); \
+  }                                                                       \
+  return CKG_OK;
+
+// Launch errors surface here (asynchronous faults at the next synchronisation).
+static void check_launch() { CKG_CUDA(cudaGetLastError()); }
+
+static Context& ctx_of(ckg_ctx* c) {
+  if (!c || !c->c) throw Error(CKG_INVALID_PARAMS, "null context");
+  return *c->c;
+}
+
+extern "C" {
+
+const char* ckg_last_error(void) { return g_last_error.c_str(); }
+uint32_t ckg_abi_version(void) { return 1; }
+uint64_t ckg_launch_count(void) { return g_launches.load(); }
+
+int ckg_primes_for_bits(uint32_t log_n, const uint32_t* q_bits, uint32_t nq, const uint32_t* p_bits, uint32_t np,
+                        uint64_t* q_out, uint64_t* p_out) {
+  CKG_API_BEGIN
+  if (log_n < 1 || log_n > 17) throw Error(CKG_INVALID_PARAMS, "log_n outside [1, 17]");
+  if (!nq || !np) throw Error(CKG_INVALID_PARAMS, "q_bits and p_bits must be non-empty");
+  std::vector<uint64_t> q, p;
+  primes_for_bits(log_n, std::vector<uint32_t>(q_bits, q_bits + nq), std::vector<uint32_t>(p_bits, p_bits + np), q, p);
+  memcpy(q_out, q.data(), nq * 8);
+  memcpy(p_out, p.data(), np * 8);
+  CKG_API_END
+}
+
+int ckg_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* p, uint32_t np, uint32_t dnum,
+                   int device, void* stream, ckg_ctx** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  auto h = new ckg_ctx;
+  try {
+    h->c = std::make_unique<Context>(log_n, std::vector<uint64_t>(q, q + nq), std::vector<uint64_t>(p, p + np), dnum,
+                                     device, (cudaStream_t)stream);
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  *out = h;
+  CKG_API_END
+}
+
+void ckg_ctx_destroy(ckg_ctx* ctx) { delete ctx; }
+
+int ckg_ctx_sync(ckg_ctx* ctx) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  c.activate();
+  CKG_CUDA(cudaStreamSynchronize(c.stream));
+  CKG_API_END
+}
+
+void* ckg_ctx_stream(ckg_ctx* ctx) { return ctx && ctx->c ? (void*)ctx->c->stream : nullptr; }
+
+// ---- device-buffer primitives ----------------------------------------------------------
+
+static void check_primes(const Context& c, const uint32_t* primes, uint32_t n) {
+  for (uint32_t i = 0; i < n; ++i)
+    if (primes[i] >= c.primes.size()) throw Error(CKG_INVALID_PARAMS, "prime index out of range");
+}
+
+int ckg_ntt(ckg_ctx* ctx, const uint64_t* src, uint64_t* dst, const uint32_t* primes, uint32_t nlimbs, int inverse) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  check_primes(c, primes, nlimbs);
+  c.activate();
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < nlimbs; ++i) refs.push_back(LimbRef{src + i * c.n, dst + i * c.n, primes[i], 0});
+  ntt_limbs(c, refs, inverse != 0);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_poly_binary(ckg_ctx* ctx, int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint32_t first_prime,
+                    uint32_t nlimbs) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (op < 0 || op > 2) throw Error(CKG_INVALID_PARAMS, "op must be 0 (add), 1 (sub) or 2 (mul)");
+  if (first_prime + nlimbs > c.primes.size()) throw Error(CKG_INVALID_PARAMS, "prime index out of range");
+  c.activate();
+  std::vector<BinRef> refs;
+  for (uint32_t i = 0; i < nlimbs; ++i)
+    refs.push_back(BinRef{a + i * c.n, b + i * c.n, out + i * c.n, first_prime + i, 0});
+  launch_binary(c.dt, refs.data(), (int)refs.size(), op, c.stream);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_poly_negate(ckg_ctx* ctx, const uint64_t* a, uint64_t* out, uint32_t first_prime, uint32_t nlimbs) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (first_prime + nlimbs > c.primes.size()) throw Error(CKG_INVALID_PARAMS, "prime index out of range");
+  c.activate();
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < nlimbs; ++i) refs.push_back(LimbRef{a + i * c.n, out + i * c.n, first_prime + i, 0});
+  launch_unary(c.dt, refs.data(), (int)refs.size(), 0, nullptr, nullptr, c.stream);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_poly_mul_scalar(ckg_ctx* ctx, const uint64_t* a, uint64_t scalar, uint64_t* out, uint32_t first_prime,
+                        uint32_t nlimbs) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (first_prime + nlimbs > c.primes.size()) throw Error(CKG_INVALID_PARAMS, "prime index out of range");
+  c.activate();
+  ScalarTable st{};
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < nlimbs; ++i) {
+    const uint32_t p = first_prime + i;
+    st.w[p] = scalar % c.mods[p].q;
+    st.ws[p] = c.mods[p].shoup(st.w[p]);
+    refs.push_back(LimbRef{a + i * c.n, out + i * c.n, p, 0});
+  }
+  launch_scalar(c.dt, refs.data(), (int)refs.size(), st, c.stream);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_automorphism(ckg_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t nlimbs, uint64_t galois_elt) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (galois_elt % 2 == 0 || galois_elt >= 2 * c.n) throw Error(CKG_INVALID_PARAMS, "Galois element must be odd and < 2N");
+  if (nlimbs > c.primes.size()) throw Error(CKG_INVALID_PARAMS, "too many limbs");
+  c.activate();
+  const uint32_t* perm = c.perm(galois_elt);
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < nlimbs; ++i) refs.push_back(LimbRef{in + i * c.n, out + i * c.n, i, 0});
+  launch_unary(c.dt, refs.data(), (int)refs.size(), 3, nullptr, perm, c.stream);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_rescale(ckg_ctx* ctx, const uint64_t* in, uint32_t level, uint64_t* out) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (level > c.L) throw Error(CKG_INVALID_PARAMS, "level above max_level");
+  if (level == 0) throw Error(CKG_NO_LEVELS_LEFT, "cannot rescale at level 0");
+  c.activate();
+  rescale_many(c, {in}, level, {out});
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_mod_up(ckg_ctx* ctx, const uint64_t* in, uint32_t level, uint32_t digit, uint64_t* out_q, uint64_t* out_p) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (level > c.L) throw Error(CKG_INVALID_PARAMS, "level above max_level");
+  if (digit >= c.digits_at(level)) throw Error(CKG_INVALID_PARAMS, "digit out of range for this level");
+  c.activate();
+  auto conv = c.alloc(conv_limbs(c, level) * c.n);
+  mod_up_many(c, {in}, level, {conv->p});
+  const uint64_t* base = conv->p + conv_offset_limbs(c, level, digit) * c.n;
+  const uint32_t s = c.digit_start(digit), e = c.digit_end(digit, level), a = e - s;
+  std::vector<LimbRef> refs;
+  uint32_t t = 0;
+  for (uint32_t i = 0; i <= level; ++i) {
+    if (i >= s && i < e) refs.push_back(LimbRef{in + i * c.n, out_q + i * c.n, i, 0});
+    else refs.push_back(LimbRef{base + (t++) * c.n, out_q + i * c.n, i, 0});
+  }
+  for (uint32_t j = 0; j < c.k; ++j)
+    refs.push_back(LimbRef{base + (level + 1 - a + j) * c.n, out_p + j * c.n, c.p_prime(j), 0});
+  launch_unary(c.dt, refs.data(), (int)refs.size(), 2, nullptr, nullptr, c.stream);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_mod_down(ckg_ctx* ctx, const uint64_t* q_part, uint32_t level, const uint64_t* p_part, uint64_t* out) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (level > c.L) throw Error(CKG_INVALID_PARAMS, "level above max_level");
+  c.activate();
+  mod_down_many(c, {ModDownJob{q_part, p_part, out, nullptr, nullptr}}, level);
+  check_launch();
+  CKG_API_END
+}
+
+static int key_upload(ckg_ctx* ctx, const uint64_t* src, bool device_src, uint32_t parts, uint32_t q_limbs,
+                      uint64_t galois_elt, ckg_key** out) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (!parts || parts > c.dnum) throw Error(CKG_INVALID_PARAMS, "key parts must be in 1..=dnum");
+  if (!q_limbs || q_limbs > c.L + 1) throw Error(CKG_INVALID_PARAMS, "key data limbs must be in 1..=L+1");
+  if (galois_elt && (galois_elt % 2 == 0 || galois_elt >= 2 * c.n))
+    throw Error(CKG_INVALID_PARAMS, "Galois element must be odd and < 2N");
+  c.activate();
+  auto k = std::make_shared<DevKey>();
+  k->ctx = &c;
+  k->parts = parts;
+  k->q_limbs = q_limbs;
+  k->elt = galois_elt;
+  const size_t words = (size_t)parts * 2 * (q_limbs + c.k) * c.n;
+  k->buf = c.alloc(words);
+  CKG_CUDA(cudaMemcpyAsync(k->buf->p, src, words * 8, device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           c.stream));
+  CKG_CUDA(cudaStreamSynchronize(c.stream));
+  *out = new ckg_key{k};
+  CKG_API_END
+}
+
+int ckg_key_upload(ckg_ctx* ctx, const uint64_t* host_key, uint32_t parts, uint32_t q_limbs, uint64_t galois_elt,
+                   ckg_key** out) {
+  return key_upload(ctx, host_key, false, parts, q_limbs, galois_elt, out);
+}
+
+int ckg_key_upload_device(ckg_ctx* ctx, const uint64_t* dev_key, uint32_t parts, uint32_t q_limbs, uint64_t galois_elt,
+                          ckg_key** out) {
+  return key_upload(ctx, dev_key, true, parts, q_limbs, galois_elt, out);
+}
+
+void ckg_key_free(ckg_key* key) { delete key; }
+uint64_t ckg_key_bytes(const ckg_key* key) { return key && key->k ? key->k->buf->words * 8 : 0; }
+
+int ckg_key_switch(ckg_ctx* ctx, const ckg_key* key, const uint64_t* in, uint32_t level, uint64_t* out_b,
+                   uint64_t* out_a) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (!key || !key->k) throw Error(CKG_INVALID_PARAMS, "null key");
+  if (level > c.L) throw Error(CKG_INVALID_PARAMS, "level above max_level");
+  c.activate();
+  KsJob j;
+  j.in = in;
+  j.key = key->k.get();
+  j.out_b = out_b;
+  j.out_a = out_a;
+  key_switch_many(c, {j}, level);
+  check_launch();
+  CKG_API_END
+}
+
+// ---- evaluator -------------------------------------------------------------------------
+
+static Evaluator& ev_of(ckg_eval* e) {
+  if (!e || !e->e) throw Error(CKG_INVALID_PARAMS, "null evaluator");
+  return *e->e;
+}
+static const Ct& ct_of(const ckg_ct* c) {
+  if (!c || !c->c) throw Error(CKG_INVALID_PARAMS, "null ciphertext");
+  return c->c;
+}
+static const Pt& pt_of(const ckg_pt* p) {
+  if (!p || !p->p) throw Error(CKG_INVALID_PARAMS, "null plaintext");
+  return p->p;
+}
+static int emit(const Ct& c, ckg_ct** out) {
+  check_launch();
+  *out = new ckg_ct{c};
+  return CKG_OK;
+}
+
+int ckg_eval_create(ckg_ctx* ctx, const ckg_key* relin, const ckg_key* const* galois, uint32_t ngal, uint32_t flags,
+                    ckg_eval** out) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  std::vector<KeyPtr> g;
+  for (uint32_t i = 0; i < ngal; ++i) {
+    if (!galois[i] || !galois[i]->k || !galois[i]->k->elt)
+      throw Error(CKG_INVALID_PARAMS, "Galois keys need their Galois element");
+    g.push_back(galois[i]->k);
+  }
+  EvalConfig cfg{(flags & CKG_HOIST) != 0, (flags & CKG_BSGS) != 0, (flags & CKG_LAZY_RELIN) != 0};
+  *out = new ckg_eval{std::make_unique<Evaluator>(&c, relin ? relin->k : nullptr, g, cfg)};
+  CKG_API_END
+}
+
+void ckg_eval_destroy(ckg_eval* ev) { delete ev; }
+
+int ckg_eval_fork(const ckg_eval* ev, ckg_eval** out) {
+  CKG_API_BEGIN
+  if (!ev || !ev->e) throw Error(CKG_INVALID_PARAMS, "null evaluator");
+  *out = new ckg_eval{ev->e->fork()};
+  CKG_API_END
+}
+
+uint32_t ckg_eval_config(const ckg_eval* ev) {
+  const EvalConfig& c = ev->e->config();
+  return (c.hoist ? CKG_HOIST : 0) | (c.bsgs ? CKG_BSGS : 0) | (c.lazy_relin ? CKG_LAZY_RELIN : 0);
+}
+
+void ckg_eval_counter(const ckg_eval* ev, uint64_t out[7]) {
+  auto w = ev->e->counter().words();
+  memcpy(out, w.data(), 7 * 8);
+}
+void ckg_eval_reset_counter(ckg_eval* ev) { ev->e->reset_counter(); }
+void ckg_eval_add_counts(ckg_eval* ev, const uint64_t c[7]) {
+  OpCounter o;
+  o.rotations = c[0];
+  o.relins = c[1];
+  o.ct_ct_tensor = c[2];
+  o.ct_pt_mults = c[3];
+  o.rescales = c[4];
+  o.sse_switches = c[5];
+  o.bootstraps = c[6];
+  ev->e->add_counts(o);
+}
+int ckg_eval_has_relin_key(const ckg_eval* ev) { return ev->e->has_relin_key() ? 1 : 0; }
+int ckg_eval_has_galois_key(const ckg_eval* ev, int32_t step) { return ev->e->has_galois_key(step) ? 1 : 0; }
+
+int ckg_ct_upload(ckg_eval* ev, const uint64_t* host, uint32_t ncomp, uint32_t level, double scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).upload(host, false, ncomp, level, scale), out);
+  CKG_API_END
+}
+
+int ckg_ct_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t ncomp, uint32_t level, double scale,
+                         ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).upload(dev, true, ncomp, level, scale), out);
+  CKG_API_END
+}
+
+static void copy_out(const Ct& c, uint64_t* dst, cudaMemcpyKind kind) {
+  Context& x = *c->ctx;
+  x.activate();
+  const size_t words = (size_t)(c->level + 1) * x.n;
+  if (c->comp_stride == words) {
+    CKG_CUDA(cudaMemcpyAsync(dst, c->comp(0), c->ncomp * words * 8, kind, x.stream));
+  } else {
+    CKG_CUDA(cudaMemcpy2DAsync(dst, words * 8, c->comp(0), c->comp_stride * 8, words * 8, c->ncomp, kind, x.stream));
+  }
+}
+
+int ckg_ct_download(const ckg_ct* ct, uint64_t* host) {
+  CKG_API_BEGIN
+  const Ct& c = ct_of(ct);
+  copy_out(c, host, cudaMemcpyDeviceToHost);
+  CKG_CUDA(cudaStreamSynchronize(c->ctx->stream));
+  CKG_API_END
+}
+
+int ckg_ct_download_device(const ckg_ct* ct, uint64_t* dev) {
+  CKG_API_BEGIN
+  copy_out(ct_of(ct), dev, cudaMemcpyDeviceToDevice);
+  CKG_API_END
+}
+
+void ckg_ct_info(const ckg_ct* ct, uint32_t* ncomp, uint32_t* level, double* scale) {
+  if (ncomp) *ncomp = ct->c->ncomp;
+  if (level) *level = ct->c->level;
+  if (scale) *scale = ct->c->scale;
+}
+
+ckg_ct* ckg_ct_clone(const ckg_ct* ct) { return new ckg_ct{ct->c}; }
+void ckg_ct_free(ckg_ct* ct) { delete ct; }
+int ckg_eval_owns(const ckg_eval* ev, const ckg_ct* ct) { return ev && ev->e && ct && ev->e->owns(ct->c) ? 1 : 0; }
+
+int ckg_pt_upload(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out) {
+  CKG_API_BEGIN
+  *out = new ckg_pt{ev_of(ev).upload_pt(host, false, level, scale)};
+  check_launch();
+  CKG_API_END
+}
+int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, double scale, ckg_pt** out) {
+  CKG_API_BEGIN
+  *out = new ckg_pt{ev_of(ev).upload_pt(dev, true, level, scale)};
+  check_launch();
+  CKG_API_END
+}
+ckg_pt* ckg_pt_clone(const ckg_pt* pt) { return new ckg_pt{pt->p}; }
+void ckg_pt_free(ckg_pt* pt) { delete pt; }
+
+#define CKG_BIN(name, method)                                                  \
+  int name(ckg_eval* ev, const ckg_ct* a, const ckg_ct* b, ckg_ct** out) {     \
+    CKG_API_BEGIN                                                              \
+    return emit(ev_of(ev).method(ct_of(a), ct_of(b)), out);                    \
+    CKG_API_END                                                                \
+  }
+#define CKG_UN(name, method)                                  \
+  int name(ckg_eval* ev, const ckg_ct* a, ckg_ct** out) {     \
+    CKG_API_BEGIN                                             \
+    return emit(ev_of(ev).method(ct_of(a)), out);             \
+    CKG_API_END                                               \
+  }
+
+CKG_BIN(ckg_add, add)
+CKG_BIN(ckg_sub, sub)
+CKG_BIN(ckg_mul_no_relin, mul_no_relin)
+CKG_BIN(ckg_mul, mul)
+CKG_UN(ckg_negate, negate)
+CKG_UN(ckg_relinearize, relinearize)
+CKG_UN(ckg_rescale_ct, rescale)
+CKG_UN(ckg_conjugate, conjugate)
+
+int ckg_add_plain(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).add_plain(ct_of(a), pt_of(p)), out);
+  CKG_API_END
+}
+int ckg_mul_plain(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).mul_plain(ct_of(a), pt_of(p)), out);
+  CKG_API_END
+}
+int ckg_mul_scalar(ckg_eval* ev, const ckg_ct* a, double value, double target_scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).mul_scalar(ct_of(a), value, target_scale), out);
+  CKG_API_END
+}
+int ckg_mul_plain_to_scale(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, double target_scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).mul_plain_to_scale(ct_of(a), pt_of(p), target_scale), out);
+  CKG_API_END
+}
+int ckg_mod_switch_to_level(ckg_eval* ev, const ckg_ct* a, uint32_t level, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).mod_switch_to_level(ct_of(a), level), out);
+  CKG_API_END
+}
+int ckg_relabel(ckg_eval* ev, const ckg_ct* a, double scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).relabel(ct_of(a), scale), out);
+  CKG_API_END
+}
+int ckg_rotate(ckg_eval* ev, const ckg_ct* a, int32_t steps, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).rotate(ct_of(a), steps), out);
+  CKG_API_END
+}
+
+int ckg_hoisted_rotate(ckg_eval* ev, const ckg_ct* a, const int32_t* steps, uint32_t nsteps, ckg_ct** outs) {
+  CKG_API_BEGIN
+  auto v = ev_of(ev).hoisted_rotate(ct_of(a), std::vector<int32_t>(steps, steps + nsteps));
+  check_launch();
+  for (size_t i = 0; i < v.size(); ++i) outs[i] = new ckg_ct{v[i]};
+  CKG_API_END
+}
+
+int ckg_exact_product_scale(const ckg_eval* ev, uint32_t level, double target_scale, double* out) {
+  CKG_API_BEGIN
+  if (!ev || !ev->e) throw Error(CKG_INVALID_PARAMS, "null evaluator");
+  *out = ev->e->exact_product_scale(level, target_scale);
+  CKG_API_END
+}
+
+int ckg_matvec_plain(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_pt* const* entries, const ckg_ct* x,
+                     ckg_ct** out) {
+  CKG_API_BEGIN
+  std::vector<Pt> e;
+  for (uint32_t i = 0; i < d; ++i) e.push_back(entries[i] ? entries[i]->p : nullptr);
+  return emit(ev_of(ev).matvec_plain(d, stride, e, ct_of(x)), out);
+  CKG_API_END
+}
+
+int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* const* entries, const ckg_ct* x,
+                   ckg_ct** out) {
+  CKG_API_BEGIN
+  std::vector<Ct> e;
+  for (uint32_t i = 0; i < d; ++i) e.push_back(entries[i] ? entries[i]->c : nullptr);
+  return emit(ev_of(ev).matvec_enc(d, stride, e, ct_of(x)), out);
+  CKG_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,482 @@
+// Device context set-up (prime constants, twiddle and conversion tables) and the
+// polynomial-level algorithms of the evaluator path. See engine.hpp for the layouts.
+#include <cstring>
+
+#include "engine.hpp"
+
+namespace ckg {
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    throw Error(ST_OOM, std::string("out of device memory: ") + what);
+  }
+  throw Error(ST_DEVICE, std::string(cudaGetErrorName(e)) + " (" + cudaGetErrorString(e) + ") at " + what);
+}
+
+DevBuf::~DevBuf() {
+  if (!p) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  if (pooled) cudaFreeAsync(p, st);
+  else cudaFree(p);
+  if (cur != device) cudaSetDevice(cur);
+}
+
+void Context::activate() const { CKG_CUDA(cudaSetDevice(device)); }
+
+DevBufPtr Context::alloc(size_t words) {
+  auto b = std::make_shared<DevBuf>();
+  b->st = stream;
+  b->device = device;
+  b->words = words;
+  if (words) CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, stream));
+  return b;
+}
+
+namespace {
+
+// Conversion table record (kernels.cuh ConvLayout) for sources `src` -> targets `dst`
+// (global prime indices): sum_j y_j [S/s_j]_t - e [S]_t - [h]_t with h = (S-1)/2.
+std::vector<uint64_t> conv_table(const std::vector<HostMod>& mods, const std::vector<uint32_t>& src,
+                                 const std::vector<uint32_t>& dst) {
+  std::vector<uint64_t> w;
+  const size_t ns = src.size();
+  for (size_t j = 0; j < ns; ++j) {
+    const HostMod& m = mods[src[j]];
+    uint64_t qhat = 1;
+    for (size_t i = 0; i < ns; ++i)
+      if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
+    uint64_t qhinv = m.inv(qhat);
+    double inv = 1.0 / (double)m.q;
+    uint64_t inv_bits;
+    memcpy(&inv_bits, &inv, 8);
+    w.push_back(src[j]);
+    w.push_back(qhinv);
+    w.push_back(m.shoup(qhinv));
+    w.push_back(m.q >> 1);
+    w.push_back(inv_bits);
+  }
+  for (uint32_t t : dst) {
+    const HostMod& m = mods[t];
+    uint64_t S = 1 % m.q;
+    for (uint32_t s : src) S = m.mul(S, mods[s].q % m.q);
+    // h = (S - 1)/2 mod t = (S - 1) * 2^-1
+    uint64_t h = m.mul(m.sub(S, 1 % m.q), (m.q + 1) / 2);
+    w.push_back(t);
+    w.push_back(m.q - S);
+    w.push_back(m.q - h);
+    w.push_back(0);
+    for (size_t j = 0; j < ns; ++j) {
+      uint64_t qhat = 1 % m.q;
+      for (size_t i = 0; i < ns; ++i)
+        if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
+      w.push_back(qhat);
+    }
+  }
+  return w;
+}
+
+}  // namespace
+
+Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vector<uint64_t>& p, uint32_t dnum_,
+                 int device_, cudaStream_t st)
+    : device(device_), log_n(log_n_) {
+  if (log_n < 5 || log_n > 17) throw Error(ST_INVALID_PARAMS, "log_n must be in 5..=17");
+  if (q.empty() || p.empty()) throw Error(ST_INVALID_PARAMS, "q and p must be non-empty");
+  if (dnum_ == 0 || q.size() % dnum_ != 0) throw Error(ST_INVALID_PARAMS, "dnum must divide the number of q primes");
+  if (q.size() / dnum_ > (size_t)kMaxSrc || p.size() > (size_t)kMaxSrc)
+    throw Error(ST_INVALID_PARAMS, "at most 16 primes per digit and 16 special primes");
+  if (dnum_ > (uint32_t)kMaxDigits) throw Error(ST_INVALID_PARAMS, "at most 16 digits");
+  if (q.size() + p.size() > 64) throw Error(ST_INVALID_PARAMS, "at most 64 primes");
+  n = 1ULL << log_n;
+  nq = q.size();
+  k = p.size();
+  dnum = dnum_;
+  alpha = nq / dnum;
+  L = nq - 1;
+  primes = q;
+  primes.insert(primes.end(), p.begin(), p.end());
+  for (size_t i = 0; i < primes.size(); ++i) {
+    uint64_t v = primes[i];
+    if (v < 3 || v >= (1ULL << 60) || !is_prime(v) || (v - 1) % (2 * n) != 0)
+      throw Error(ST_INVALID_PARAMS, "modulus " + std::to_string(v) + " is not an NTT-friendly prime below 2^60");
+    for (size_t j = 0; j < i; ++j)
+      if (primes[j] == v) throw Error(ST_INVALID_PARAMS, "duplicate modulus " + std::to_string(v));
+    mods.emplace_back(v);
+  }
+  CKG_CUDA(cudaSetDevice(device));
+  if (st) {
+    stream = st;
+  } else {
+    CKG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  {  // keep freed pool memory cached: steady-state ops allocate without driver calls
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
+  const size_t np = primes.size();
+  // per-prime constants
+  std::vector<PrimeConst> pc(np);
+  std::vector<ulonglong2> twf(np * n), twi(np * n);
+  for (size_t i = 0; i < np; ++i) {
+    const HostMod& m = mods[i];
+    PrimeConst& c = pc[i];
+    c.q = m.q;
+    c.two_q = 2 * m.q;
+    c.b = bit_length(m.q);
+    c.mu = (uint64_t)(((u128)1 << (2 * c.b)) / m.q);
+    uint64_t psi = minimal_root(n, m), psi_inv = m.inv(psi), ninv = m.inv(n);
+    c.ninv = ninv;
+    c.ninv_s = m.shoup(ninv);
+    uint64_t p = 1, pi = 1;
+    for (uint64_t e = 0; e < n; ++e) {
+      uint64_t r = bitrev(e, log_n);
+      twf[i * n + r] = make_ulonglong2(p, m.shoup(p));
+      twi[i * n + r] = make_ulonglong2(pi, m.shoup(pi));
+      p = m.mul(p, psi);
+      pi = m.mul(pi, psi_inv);
+    }
+    c.wninv = m.mul(twi[i * n + 1].x, ninv);
+    c.wninv_s = m.shoup(c.wninv);
+    c.r64 = (uint64_t)(((u128)1 << 64) % m.q);
+    c.r64_s = m.shoup(c.r64);
+    c.one_s = m.shoup(1);
+  }
+  CKG_CUDA(cudaMalloc(&d_prime, np * sizeof(PrimeConst)));
+  CKG_CUDA(cudaMalloc(&d_tw_fwd, np * n * sizeof(ulonglong2)));
+  CKG_CUDA(cudaMalloc(&d_tw_inv, np * n * sizeof(ulonglong2)));
+  CKG_CUDA(cudaMemcpy(d_prime, pc.data(), np * sizeof(PrimeConst), cudaMemcpyHostToDevice));
+  CKG_CUDA(cudaMemcpy(d_tw_fwd, twf.data(), np * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+  CKG_CUDA(cudaMemcpy(d_tw_inv, twi.data(), np * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+  dt = DevTables{d_prime, d_tw_fwd, d_tw_inv, (int)log_n};
+
+  // conversion tables
+  std::vector<uint64_t> conv;
+  auto push = [&](const std::vector<uint64_t>& t) {
+    size_t off = conv.size();
+    conv.insert(conv.end(), t.begin(), t.end());
+    return off;
+  };
+  modup_off.assign((size_t)nq * dnum, 0);
+  moddown_off.assign(nq, 0);
+  rescale_off.assign(nq, 0);
+  std::vector<uint32_t> pidx;
+  for (uint32_t t = 0; t < k; ++t) pidx.push_back(p_prime(t));
+  for (uint32_t l = 0; l <= L; ++l) {
+    for (uint32_t j = 0; j < digits_at(l); ++j) {
+      std::vector<uint32_t> src, dst;
+      for (uint32_t i = digit_start(j); i < digit_end(j, l); ++i) src.push_back(i);
+      for (uint32_t i = 0; i <= l; ++i)
+        if (i < digit_start(j) || i >= digit_end(j, l)) dst.push_back(i);
+      dst.insert(dst.end(), pidx.begin(), pidx.end());
+      modup_off[(size_t)l * dnum + j] = push(conv_table(mods, src, dst));
+    }
+    std::vector<uint32_t> qs;
+    for (uint32_t i = 0; i <= l; ++i) qs.push_back(i);
+    moddown_off[l] = push(conv_table(mods, pidx, qs));
+    if (l >= 1) {
+      qs.pop_back();
+      rescale_off[l] = push(conv_table(mods, {l}, qs));
+    }
+  }
+  CKG_CUDA(cudaMalloc(&d_conv, conv.size() * 8));
+  CKG_CUDA(cudaMemcpy(d_conv, conv.data(), conv.size() * 8, cudaMemcpyHostToDevice));
+  // finish constants
+  for (uint32_t i = 0; i <= L; ++i) {
+    const HostMod& m = mods[i];
+    uint64_t pm = 1;
+    for (uint32_t t = 0; t < k; ++t) pm = m.mul(pm, primes[p_prime(t)] % m.q);
+    uint64_t v = m.inv(pm);
+    pinv.push_back({v, m.shoup(v)});
+  }
+  qlinv.assign(nq, {});
+  for (uint32_t l = 1; l <= L; ++l)
+    for (uint32_t i = 0; i < l; ++i) {
+      const HostMod& m = mods[i];
+      uint64_t v = m.inv(primes[l] % m.q);
+      qlinv[l].push_back({v, m.shoup(v)});
+    }
+  CKG_CUDA(cudaDeviceSynchronize());
+}
+
+Context::~Context() {
+  cudaSetDevice(device);
+  cudaStreamSynchronize(stream);
+  for (auto& kv : perms) cudaFree(kv.second);
+  cudaFree(d_prime);
+  cudaFree(d_tw_fwd);
+  cudaFree(d_tw_inv);
+  cudaFree(d_conv);
+  if (own_stream) cudaStreamDestroy(stream);
+}
+
+const uint32_t* Context::perm(uint64_t elt) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = perms.find(elt);
+  if (it != perms.end()) return it->second;
+  auto v = galois_perm(n, elt);
+  uint32_t* d = nullptr;
+  CKG_CUDA(cudaMalloc(&d, n * 4));
+  CKG_CUDA(cudaMemcpy(d, v.data(), n * 4, cudaMemcpyHostToDevice));
+  perms[elt] = d;
+  return d;
+}
+
+// -------------------------------------------------------------------------------------
+
+void ntt_limbs(Context& c, const std::vector<LimbRef>& refs, bool inverse) {
+  if (!refs.empty()) launch_ntt(c.dt, refs.data(), (int)refs.size(), inverse, c.stream);
+}
+
+void ntt_poly(Context& c, const uint64_t* src, uint64_t* dst, uint32_t first_prime, uint32_t count, bool inverse) {
+  std::vector<LimbRef> refs(count);
+  for (uint32_t i = 0; i < count; ++i) refs[i] = LimbRef{src + i * c.n, dst + i * c.n, first_prime + i, 0};
+  ntt_limbs(c, refs, inverse);
+}
+
+void rescale_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l, const std::vector<uint64_t*>& out) {
+  const size_t np = in.size(), N = c.n;
+  if (!np) return;
+  if (l < 1) throw Error(ST_NO_LEVELS_LEFT, "cannot rescale at level 0");
+  auto scratch = c.alloc(np * (1 + l) * N);
+  std::vector<LimbRef> refs;
+  std::vector<ConvJob> jobs;
+  for (size_t i = 0; i < np; ++i) {
+    uint64_t* last = scratch->p + i * (1 + l) * N;
+    refs.push_back(LimbRef{in[i] + (size_t)l * N, last, l, 0});
+    jobs.push_back(ConvJob{last, last + N, c.d_conv + c.rescale_off[l], N, N});
+  }
+  ntt_limbs(c, refs, true);
+  launch_bconv(c.dt, jobs.data(), (int)jobs.size(), 1, (int)l, c.stream);
+  refs.clear();
+  std::vector<FinRef> fin;
+  for (size_t i = 0; i < np; ++i) {
+    uint64_t* t = scratch->p + i * (1 + l) * N + N;
+    for (uint32_t j = 0; j < l; ++j) {
+      refs.push_back(LimbRef{t + j * N, t + j * N, j, 0});
+      fin.push_back(FinRef{in[i] + j * N, t + j * N, nullptr, nullptr, out[i] + j * N, c.qlinv[l][j].first,
+                           c.qlinv[l][j].second, j, 0});
+    }
+  }
+  ntt_limbs(c, refs, false);
+  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+}
+
+void mod_down_many(Context& c, const std::vector<ModDownJob>& jobs, uint32_t l) {
+  const size_t nj = jobs.size(), N = c.n, per = c.k + l + 1;
+  if (!nj) return;
+  auto scratch = c.alloc(nj * per * N);
+  std::vector<LimbRef> refs;
+  std::vector<ConvJob> conv;
+  for (size_t i = 0; i < nj; ++i) {
+    uint64_t* pc = scratch->p + i * per * N;
+    for (uint32_t t = 0; t < c.k; ++t) refs.push_back(LimbRef{jobs[i].ppart + t * N, pc + t * N, c.p_prime(t), 0});
+    conv.push_back(ConvJob{pc, pc + c.k * N, c.d_conv + c.moddown_off[l], N, N});
+  }
+  ntt_limbs(c, refs, true);
+  launch_bconv(c.dt, conv.data(), (int)nj, (int)c.k, (int)(l + 1), c.stream);
+  refs.clear();
+  std::vector<FinRef> fin;
+  for (size_t i = 0; i < nj; ++i) {
+    uint64_t* t = scratch->p + i * per * N + c.k * N;
+    for (uint32_t j = 0; j <= l; ++j) {
+      refs.push_back(LimbRef{t + j * N, t + j * N, j, 0});
+      fin.push_back(FinRef{jobs[i].qpart + j * N, t + j * N, jobs[i].add ? jobs[i].add + j * N : nullptr,
+                           jobs[i].add_perm, jobs[i].out + j * N, c.pinv[j].first, c.pinv[j].second, j, 0});
+    }
+  }
+  ntt_limbs(c, refs, false);
+  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+}
+
+size_t conv_limbs(const Context& c, uint32_t l) {
+  size_t s = 0;
+  for (uint32_t j = 0; j < c.digits_at(l); ++j) s += (l + 1) - (c.digit_end(j, l) - c.digit_start(j)) + c.k;
+  return s;
+}
+
+size_t conv_offset_limbs(const Context& c, uint32_t l, uint32_t jj) {
+  size_t s = 0;
+  for (uint32_t j = 0; j < jj; ++j) s += (l + 1) - (c.digit_end(j, l) - c.digit_start(j)) + c.k;
+  return s;
+}
+
+namespace {
+
+// Global prime index of target t of digit j at level l: data primes outside the digit in
+// increasing order, then the special primes.
+inline uint32_t target_prime(const Context& c, uint32_t l, uint32_t j, uint32_t t) {
+  const uint32_t s = c.digit_start(j), a = c.digit_end(j, l) - s;
+  if (t < s) return t;
+  if (t < l + 1 - a) return t + a;
+  return c.p_prime(t - (l + 1 - a));
+}
+
+// ModUp with caller-provided coefficient scratch ((l+1) limbs per input).
+void mod_up_into(Context& c, const std::vector<const uint64_t*>& in, uint32_t l, const std::vector<uint64_t*>& conv_out,
+                 const std::vector<uint64_t*>& coeff) {
+  const size_t N = c.n;
+  std::vector<LimbRef> refs;
+  for (size_t i = 0; i < in.size(); ++i)
+    for (uint32_t j = 0; j <= l; ++j) refs.push_back(LimbRef{in[i] + j * N, coeff[i] + j * N, j, 0});
+  ntt_limbs(c, refs, true);
+  // group the conversions by shape (a level-clipped last digit differs)
+  std::map<std::pair<int, int>, std::vector<ConvJob>> groups;
+  for (size_t i = 0; i < in.size(); ++i)
+    for (uint32_t j = 0; j < c.digits_at(l); ++j) {
+      const uint32_t s = c.digit_start(j), a = c.digit_end(j, l) - s, T = l + 1 - a + c.k;
+      groups[{(int)a, (int)T}].push_back(ConvJob{coeff[i] + s * N, conv_out[i] + conv_offset_limbs(c, l, j) * N,
+                                                 c.d_conv + c.modup_off[(size_t)l * c.dnum + j], N, N});
+    }
+  for (auto& g : groups)
+    launch_bconv(c.dt, g.second.data(), (int)g.second.size(), g.first.first, g.first.second, c.stream);
+  refs.clear();
+  for (size_t i = 0; i < in.size(); ++i)
+    for (uint32_t j = 0; j < c.digits_at(l); ++j) {
+      const uint32_t a = c.digit_end(j, l) - c.digit_start(j), T = l + 1 - a + c.k;
+      uint64_t* base = conv_out[i] + conv_offset_limbs(c, l, j) * N;
+      for (uint32_t t = 0; t < T; ++t) refs.push_back(LimbRef{base + t * N, base + t * N, target_prime(c, l, j, t), 0});
+    }
+  ntt_limbs(c, refs, false);
+}
+
+}  // namespace
+
+void mod_up_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l, const std::vector<uint64_t*>& conv_out) {
+  if (in.empty()) return;
+  auto scratch = c.alloc(in.size() * (l + 1) * c.n);
+  std::vector<uint64_t*> coeff;
+  for (size_t i = 0; i < in.size(); ++i) coeff.push_back(scratch->p + i * (l + 1) * c.n);
+  mod_up_into(c, in, l, conv_out, coeff);
+}
+
+size_t key_switch_scratch_words(const Context& c, uint32_t l) {
+  // coefficient copy of the input, converted digits, two extended accumulators,
+  // ModDown scratch for both accumulators
+  return ((l + 1) + conv_limbs(c, l) + 2 * (l + 1 + c.k) + 2 * (c.k + l + 1)) * c.n;
+}
+
+namespace {
+
+void check_ks(const Context& c, const KsJob& j, uint32_t l) {
+  if (!j.key) throw Error(ST_INVALID_PARAMS, "missing key");
+  if (j.key->ctx != &c) throw Error(ST_INVALID_PARAMS, "key is not over this context");
+  if (l + 1 > j.key->q_limbs) throw Error(ST_INVALID_PARAMS, "level above the key's maximum level");
+  if (c.digits_at(l) > j.key->parts) throw Error(ST_INVALID_PARAMS, "key has too few parts for this level");
+}
+
+// Inner product + ModDown of a group of jobs whose digits are in conv[i]; acc buffers and
+// ModDown scratch are provided.
+void ks_tail(Context& c, const std::vector<KsJob>& jobs, uint32_t l, const std::vector<const uint64_t*>& conv,
+             const std::vector<uint64_t*>& acc, const std::vector<uint64_t*>& mdscratch) {
+  const size_t N = c.n, ext = l + 1 + c.k;
+  IpBatch proto{};
+  proto.level = (int)l;
+  proto.ndig = (int)c.digits_at(l);
+  proto.alpha = (int)c.alpha;
+  proto.L = (int)c.L;
+  proto.k = (int)c.k;
+  std::vector<IpJob> ip;
+  // Keys with different data-limb counts need separate launches (the layout stride).
+  std::map<uint32_t, std::vector<size_t>> by_key_q;
+  for (size_t i = 0; i < jobs.size(); ++i) by_key_q[jobs[i].key->q_limbs].push_back(i);
+  for (auto& kv : by_key_q) {
+    ip.clear();
+    proto.key_q = (int)kv.first;
+    for (size_t i : kv.second) {
+      IpJob jb{};
+      jb.in = jobs[i].in;
+      for (uint32_t j = 0; j < c.digits_at(l); ++j) jb.conv[j] = conv[i] + conv_offset_limbs(c, l, j) * N;
+      jb.key = jobs[i].key->buf->p;
+      jb.out_b = acc[i];
+      jb.out_a = acc[i] + ext * N;
+      jb.perm = jobs[i].perm;
+      ip.push_back(jb);
+    }
+    launch_inner_product(c.dt, proto, ip.data(), (int)ip.size(), c.stream);
+  }
+  // ModDown of both accumulators of every job, fused with the additions.
+  const size_t per = c.k + l + 1;
+  std::vector<LimbRef> refs;
+  std::vector<ConvJob> cj;
+  for (size_t i = 0; i < jobs.size(); ++i)
+    for (int ba = 0; ba < 2; ++ba) {
+      const uint64_t* x = acc[i] + ba * ext * N;
+      uint64_t* pc = mdscratch[i] + ba * per * N;
+      for (uint32_t t = 0; t < c.k; ++t) refs.push_back(LimbRef{x + (l + 1 + t) * N, pc + t * N, c.p_prime(t), 0});
+      cj.push_back(ConvJob{pc, pc + c.k * N, c.d_conv + c.moddown_off[l], N, N});
+    }
+  ntt_limbs(c, refs, true);
+  launch_bconv(c.dt, cj.data(), (int)cj.size(), (int)c.k, (int)(l + 1), c.stream);
+  refs.clear();
+  std::vector<FinRef> fin;
+  for (size_t i = 0; i < jobs.size(); ++i)
+    for (int ba = 0; ba < 2; ++ba) {
+      const uint64_t* x = acc[i] + ba * ext * N;
+      uint64_t* t = mdscratch[i] + ba * per * N + c.k * N;
+      uint64_t* out = ba == 0 ? jobs[i].out_b : jobs[i].out_a;
+      const uint64_t* add = ba == 0 ? jobs[i].add_b : jobs[i].add_a;
+      const uint32_t* aperm = ba == 0 ? jobs[i].add_b_perm : nullptr;
+      for (uint32_t j = 0; j <= l; ++j) {
+        refs.push_back(LimbRef{t + j * N, t + j * N, j, 0});
+        fin.push_back(FinRef{x + j * N, t + j * N, add ? add + j * N : nullptr, aperm, out + j * N, c.pinv[j].first,
+                             c.pinv[j].second, j, 0});
+      }
+    }
+  ntt_limbs(c, refs, false);
+  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+}
+
+void ks_group(Context& c, const std::vector<KsJob>& jobs, uint32_t l, uint64_t* scratch) {
+  const size_t N = c.n;
+  const size_t coeffw = (l + 1) * N, convw = conv_limbs(c, l) * N, accw = 2 * (l + 1 + c.k) * N;
+  const size_t mdw = 2 * (c.k + l + 1) * N, per = coeffw + convw + accw + mdw;
+  std::vector<const uint64_t*> in, conv;
+  std::vector<uint64_t*> coeff, convw_p, acc, md;
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    uint64_t* base = scratch + i * per;
+    coeff.push_back(base);
+    convw_p.push_back(base + coeffw);
+    acc.push_back(base + coeffw + convw);
+    md.push_back(base + coeffw + convw + accw);
+    conv.push_back(jobs[i].conv ? jobs[i].conv : base + coeffw);
+    if (!jobs[i].conv) in.push_back(jobs[i].in);
+  }
+  // ModUp for the jobs without precomputed digits
+  std::vector<uint64_t*> co, cv;
+  for (size_t i = 0; i < jobs.size(); ++i)
+    if (!jobs[i].conv) {
+      co.push_back(coeff[i]);
+      cv.push_back(convw_p[i]);
+    }
+  if (!in.empty()) mod_up_into(c, in, l, cv, co);
+  ks_tail(c, jobs, l, conv, acc, md);
+}
+
+}  // namespace
+
+void key_switch_with_scratch(Context& c, const KsJob& job, uint32_t l, uint64_t* scratch) {
+  check_ks(c, job, l);
+  ks_group(c, {job}, l, scratch);
+}
+
+void key_switch_many(Context& c, const std::vector<KsJob>& jobs, uint32_t l) {
+  for (auto& j : jobs) check_ks(c, j, l);
+  const size_t per = key_switch_scratch_words(c, l);
+  // Bound the scratch of one group to about 2 GiB.
+  size_t group = std::max<size_t>(1, ((size_t)2 << 30) / (per * 8));
+  for (size_t off = 0; off < jobs.size(); off += group) {
+    size_t cnt = std::min(group, jobs.size() - off);
+    auto scratch = c.alloc(cnt * per);
+    std::vector<KsJob> sub(jobs.begin() + off, jobs.begin() + off + cnt);
+    ks_group(c, sub, l, scratch->p);
+  }
+}
+
+}  // namespace ckg

@@ -1,0 +1,159 @@
+// Device context and the polynomial-level algorithms of the evaluator path built from the
+// kernels: NTT/INTT, rescale, ModUp (exact centered digit lift), ModDown, hybrid key
+// switching (single, batched and hoisted).
+//
+// Layout in HBM: a polynomial at level l is l+1 limbs of N words, limb-major and
+// contiguous; a ciphertext is its components one after another. An element of Q_l * P
+// ("extended" polynomial) is l+1 data limbs followed by the k special limbs. A key is
+// dnum parts, each b then a, each (key_q + k) limbs (data primes 0..key_q-1, then P).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host_math.hpp"
+#include "kernels.cuh"
+#include "launch.hpp"
+
+namespace ckg {
+
+// Status codes of the C ABI (include/ckg.h).
+enum Status {
+  ST_OK = 0,
+  ST_INVALID_PARAMS = 1,
+  ST_SCALE_MISMATCH = 2,
+  ST_LEVEL_MISMATCH = 3,
+  ST_NO_LEVELS_LEFT = 4,
+  ST_DECODE = 5,
+  ST_DEVICE = 6,
+  ST_OOM = 7,
+  ST_TIMEOUT = 8,
+};
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what);
+#define CKG_CUDA(x)                              \
+  do {                                           \
+    cudaError_t e_ = (x);                        \
+    if (e_ != cudaSuccess) ::ckg::throw_cuda(e_, #x); \
+  } while (0)
+
+// A stream-ordered device allocation of `words` u64.
+struct DevBuf {
+  uint64_t* p = nullptr;
+  size_t words = 0;
+  cudaStream_t st = nullptr;
+  int device = 0;
+  bool pooled = true;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf();
+};
+typedef std::shared_ptr<DevBuf> DevBufPtr;
+
+struct Context;
+
+// A key-switching key resident in HBM (one allocation).
+struct DevKey {
+  Context* ctx = nullptr;
+  DevBufPtr buf;
+  uint32_t parts = 0;   // digits the key serves
+  uint32_t q_limbs = 0; // data limbs per part (max level + 1 of the key)
+  uint64_t elt = 0;     // Galois element (0 for a relinearization key)
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  uint32_t log_n = 0;
+  uint64_t n = 0;
+  uint32_t nq = 0, k = 0, dnum = 0, alpha = 0, L = 0;
+  std::vector<uint64_t> primes;  // q_0..q_L, p_0..p_{k-1}
+  std::vector<HostMod> mods;
+  DevTables dt{};
+  PrimeConst* d_prime = nullptr;
+  ulonglong2* d_tw_fwd = nullptr;
+  ulonglong2* d_tw_inv = nullptr;
+  uint64_t* d_conv = nullptr;  // all conversion tables
+  uint64_t* d_consts = nullptr;  // finish constants (Shoup pairs)
+  std::vector<size_t> modup_off;    // [l * dnum + j] word offset into d_conv
+  std::vector<size_t> moddown_off;  // [l]
+  std::vector<size_t> rescale_off;  // [l], l >= 1
+  std::vector<std::pair<uint64_t, uint64_t>> pinv;                 // P^-1 mod q_i
+  std::vector<std::vector<std::pair<uint64_t, uint64_t>>> qlinv;  // [l][i] q_l^-1 mod q_i
+  std::mutex mu;
+  std::map<uint64_t, uint32_t*> perms;  // NTT-form Galois permutations on the device
+
+  Context(uint32_t log_n, const std::vector<uint64_t>& q, const std::vector<uint64_t>& p, uint32_t dnum, int device,
+          cudaStream_t st);
+  ~Context();
+
+  uint32_t digits_at(uint32_t l) const { return (l + alpha) / alpha < dnum ? (l + alpha) / alpha : dnum; }
+  uint32_t digit_start(uint32_t j) const { return j * alpha; }
+  uint32_t digit_end(uint32_t j, uint32_t l) const { return std::min((j + 1) * alpha, l + 1); }
+  uint32_t p_prime(uint32_t t) const { return L + 1 + t; }  // global index of special prime t
+  const uint32_t* perm(uint64_t elt);                       // cached device permutation
+  DevBufPtr alloc(size_t words);                            // stream-ordered, on `stream`
+  void activate() const;                                    // makes `device` current
+};
+
+// ---- polynomial-level algorithms (all asynchronous on ctx.stream) -------------------
+
+// In-place (or out-of-place) NTT of `count` contiguous limbs with primes first..first+count-1.
+void ntt_poly(Context& c, const uint64_t* src, uint64_t* dst, uint32_t first_prime, uint32_t count, bool inverse);
+void ntt_limbs(Context& c, const std::vector<LimbRef>& refs, bool inverse);
+
+// Rescale by the last prime of each level-l input (NTT form): out gets l limbs.
+void rescale_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l, const std::vector<uint64_t*>& out);
+
+// ModDown of extended polynomials (NTT form): out_i = (x_i - conv(round(X/P))_i) * P^-1 (+ add).
+struct ModDownJob {
+  const uint64_t* qpart;  // l+1 limbs
+  const uint64_t* ppart;  // k limbs
+  uint64_t* out;          // l+1 limbs
+  const uint64_t* add;    // optional addend (l+1 limbs)
+  const uint32_t* add_perm;
+};
+void mod_down_many(Context& c, const std::vector<ModDownJob>& jobs, uint32_t l);
+
+// Exact centered lift of every digit of each level-l input (NTT form): conv[j] receives
+// the T_j = l+1-alpha_j+k converted limbs (data primes outside the digit, then P), NTT form.
+// `conv_out[i]` is a buffer of conv_words(l) words per input; digit j starts at conv_offset(j).
+size_t conv_limbs(const Context& c, uint32_t l);
+size_t conv_offset_limbs(const Context& c, uint32_t l, uint32_t j);
+void mod_up_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l, const std::vector<uint64_t*>& conv_out);
+
+// Key switching (keyswitch.rs:230-319) of d (NTT form, level l) with `key`:
+// out_b = ModDown(sum_j d_j b_j) (+ add_b), out_a likewise. With `perm` the digits of `in`
+// are read through the Galois permutation (hoisting); `conv` may carry precomputed digits.
+struct KsJob {
+  const uint64_t* in;
+  const DevKey* key;
+  uint64_t* out_b;
+  uint64_t* out_a;
+  const uint64_t* add_b = nullptr;
+  const uint64_t* add_a = nullptr;
+  const uint32_t* add_b_perm = nullptr;
+  const uint32_t* perm = nullptr;     // digit permutation (hoisted rotation)
+  const uint64_t* conv = nullptr;     // precomputed ModUp of `in` (hoisting); null = compute
+};
+void key_switch_many(Context& c, const std::vector<KsJob>& jobs, uint32_t l);
+
+// Scratch words a key switch of one level-l polynomial needs (for the caller-provided
+// scratch variant).
+size_t key_switch_scratch_words(const Context& c, uint32_t l);
+void key_switch_with_scratch(Context& c, const KsJob& job, uint32_t l, uint64_t* scratch);
+
+}  // namespace ckg

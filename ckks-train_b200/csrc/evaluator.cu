@@ -1,0 +1,550 @@
+// The HeOps evaluator on device-resident ciphertexts. Each method follows the CPU
+// Evaluator method of the same name in crates/ckks-train-ckks/src/evaluator.rs (checks in
+// the same order, the same errors, f64 scale labels and OpCounter increments) and
+// computes bit-identical polynomials with the kernels of kernels.cu.
+#include <cmath>
+#include <cstring>
+
+#include "evaluator.hpp"
+
+namespace ckg {
+
+namespace {
+
+const double kScaleTolerance = 1.0 / 1024.0;          // evaluator.rs:96
+const uint64_t kLabelSearchUlps = 8;                   // evaluator.rs:100
+const double kMaxScalarInt = 4611686018427387904.0;   // evaluator.rs:103 (2^62)
+const double kMinPlainScale = 1048576.0;               // evaluator.rs:108 (2^20)
+
+void check_level(uint32_t a, uint32_t b) {
+  if (a != b) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
+}
+void check_scale(double a, double b) {  // evaluator.rs:833-839
+  if (!(std::fabs(a - b) < kScaleTolerance * std::min(a, b))) throw Error(ST_SCALE_MISMATCH, "scale mismatch");
+}
+void check_plain_scale(double sp) {  // evaluator.rs:111-119
+  if (sp < kMinPlainScale)
+    throw Error(ST_INVALID_PARAMS,
+                "plaintext scale is below 2^20: the target scale is too small for this ciphertext's scale and level");
+}
+void check_ct_scale(double s) {  // ciphertext.rs:53-55
+  if (!(std::isfinite(s) && s > 0.0)) throw Error(ST_INVALID_PARAMS, "ciphertext scale must be positive and finite");
+}
+
+std::pair<uint32_t, uint32_t> bsgs_split(uint32_t d) {  // linalg.rs:419-424
+  uint32_t log_d = __builtin_ctz(d);
+  uint32_t baby = 1u << ((log_d + 1) / 2);
+  return {baby, d / baby};
+}
+
+}  // namespace
+
+Evaluator::Evaluator(Context* ctx, KeyPtr relin, std::vector<KeyPtr> galois, EvalConfig cfg)
+    : ctx_(ctx), relin_(std::move(relin)), galois_(std::move(galois)), cfg_(cfg) {}
+
+OpCounter Evaluator::counter() const {
+  std::lock_guard<std::mutex> lk(mu_);
+  return counter_;
+}
+void Evaluator::reset_counter() { count([](OpCounter& c) { c = OpCounter(); }); }
+void Evaluator::add_counts(const OpCounter& o) {
+  count([&](OpCounter& c) {
+    c.rotations += o.rotations;
+    c.relins += o.relins;
+    c.ct_ct_tensor += o.ct_ct_tensor;
+    c.ct_pt_mults += o.ct_pt_mults;
+    c.rescales += o.rescales;
+    c.sse_switches += o.sse_switches;
+    c.bootstraps += o.bootstraps;
+  });
+}
+std::unique_ptr<Evaluator> Evaluator::fork() const {
+  return std::make_unique<Evaluator>(ctx_, relin_, galois_, cfg_);
+}
+bool Evaluator::has_galois_key(int32_t step) const {
+  uint64_t elt = galois_elt(ctx_->n, step);
+  for (auto& k : galois_)
+    if (k->elt == elt) return true;
+  return false;
+}
+
+Ct Evaluator::new_ct(uint32_t ncomp, uint32_t level, double scale) {
+  check_ct_scale(scale);
+  auto c = std::make_shared<CtObj>();
+  c->ctx = ctx_;
+  c->ncomp = ncomp;
+  c->level = level;
+  c->scale = scale;
+  c->comp_stride = (size_t)(level + 1) * ctx_->n;
+  c->buf = ctx_->alloc(ncomp * c->comp_stride);
+  return c;
+}
+
+Ct Evaluator::upload(const uint64_t* src, bool device_src, uint32_t ncomp, uint32_t level, double scale) {
+  if (ncomp < 2) throw Error(ST_INVALID_PARAMS, "a ciphertext needs at least 2 components");
+  if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+  ctx_->activate();
+  Ct c = new_ct(ncomp, level, scale);
+  CKG_CUDA(cudaMemcpyAsync(c->buf->p, src, c->buf->words * 8,
+                           device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx_->stream));
+  return c;
+}
+
+Pt Evaluator::upload_pt(const uint64_t* src, bool device_src, uint32_t level, double scale) {
+  if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+  ctx_->activate();
+  auto p = std::make_shared<PtObj>();
+  p->ctx = ctx_;
+  p->level = level;
+  p->scale = scale;
+  p->buf = ctx_->alloc((size_t)(level + 1) * ctx_->n);
+  CKG_CUDA(cudaMemcpyAsync(p->buf->p, src, p->buf->words * 8,
+                           device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx_->stream));
+  return p;
+}
+
+void Evaluator::check_basis(const Ct& a) const {
+  if (!a || a->ctx != ctx_) throw Error(ST_INVALID_PARAMS, "operand is not over this evaluator's data basis");
+}
+void Evaluator::check_basis_pt(const Pt& p) const {
+  if (!p || p->ctx != ctx_) throw Error(ST_INVALID_PARAMS, "operand is not over this evaluator's data basis");
+}
+
+// ---- element-wise ops ----------------------------------------------------------------
+
+namespace {
+
+void binary_comp(Context& c, int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint32_t limbs,
+                 std::vector<BinRef>& refs) {
+  for (uint32_t i = 0; i < limbs; ++i) refs.push_back(BinRef{a + i * c.n, b + i * c.n, out + i * c.n, i, 0});
+  (void)op;
+}
+
+void unary_comp(Context& c, const uint64_t* a, uint64_t* out, uint32_t limbs, std::vector<LimbRef>& refs) {
+  for (uint32_t i = 0; i < limbs; ++i) refs.push_back(LimbRef{a + i * c.n, out + i * c.n, i, 0});
+}
+
+}  // namespace
+
+Ct Evaluator::add_sub(const Ct& a, const Ct& b, bool sub) {  // evaluator.rs:699-723
+  check_basis(a);
+  check_basis(b);
+  check_level(a->level, b->level);
+  check_scale(a->scale, b->scale);
+  ctx_->activate();
+  const uint32_t limbs = a->level + 1, nc = std::max(a->ncomp, b->ncomp), common = std::min(a->ncomp, b->ncomp);
+  Ct r = new_ct(nc, a->level, a->scale);
+  std::vector<BinRef> bin;
+  for (uint32_t i = 0; i < common; ++i) binary_comp(*ctx_, 0, a->comp(i), b->comp(i), r->comp_mut(i), limbs, bin);
+  launch_binary(ctx_->dt, bin.data(), (int)bin.size(), sub ? 1 : 0, ctx_->stream);
+  std::vector<LimbRef> cp, ng;
+  for (uint32_t i = common; i < a->ncomp; ++i) unary_comp(*ctx_, a->comp(i), r->comp_mut(i), limbs, cp);
+  for (uint32_t i = common; i < b->ncomp; ++i) unary_comp(*ctx_, b->comp(i), r->comp_mut(i), limbs, sub ? ng : cp);
+  if (!cp.empty()) launch_unary(ctx_->dt, cp.data(), (int)cp.size(), 2, nullptr, nullptr, ctx_->stream);
+  if (!ng.empty()) launch_unary(ctx_->dt, ng.data(), (int)ng.size(), 0, nullptr, nullptr, ctx_->stream);
+  return r;
+}
+
+Ct Evaluator::negate(const Ct& a) {  // evaluator.rs:242-247
+  check_basis(a);
+  ctx_->activate();
+  Ct r = new_ct(a->ncomp, a->level, a->scale);
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < a->ncomp; ++i) unary_comp(*ctx_, a->comp(i), r->comp_mut(i), a->level + 1, refs);
+  launch_unary(ctx_->dt, refs.data(), (int)refs.size(), 0, nullptr, nullptr, ctx_->stream);
+  return r;
+}
+
+Ct Evaluator::add_plain(const Ct& a, const Pt& p) {  // evaluator.rs:251-259
+  check_basis(a);
+  check_basis_pt(p);
+  check_level(a->level, p->level);
+  check_scale(a->scale, p->scale);
+  ctx_->activate();
+  const uint32_t limbs = a->level + 1;
+  Ct r = new_ct(a->ncomp, a->level, a->scale);
+  std::vector<BinRef> bin;
+  binary_comp(*ctx_, 0, a->comp(0), p->data(), r->comp_mut(0), limbs, bin);
+  launch_binary(ctx_->dt, bin.data(), (int)bin.size(), 0, ctx_->stream);
+  std::vector<LimbRef> cp;
+  for (uint32_t i = 1; i < a->ncomp; ++i) unary_comp(*ctx_, a->comp(i), r->comp_mut(i), limbs, cp);
+  launch_unary(ctx_->dt, cp.data(), (int)cp.size(), 2, nullptr, nullptr, ctx_->stream);
+  return r;
+}
+
+Ct Evaluator::mul_plain(const Ct& a, const Pt& p) {  // evaluator.rs:262-271
+  check_basis(a);
+  check_basis_pt(p);
+  check_level(a->level, p->level);
+  ctx_->activate();
+  Ct r = new_ct(a->ncomp, a->level, a->scale * p->scale);
+  std::vector<BinRef> bin;
+  for (uint32_t i = 0; i < a->ncomp; ++i) binary_comp(*ctx_, 2, a->comp(i), p->data(), r->comp_mut(i), a->level + 1, bin);
+  launch_binary(ctx_->dt, bin.data(), (int)bin.size(), 2, ctx_->stream);
+  count([](OpCounter& c) { c.ct_pt_mults++; });
+  return r;
+}
+
+double Evaluator::exact_product_scale(uint32_t level, double target) const {  // evaluator.rs:739-773
+  if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level exceeds max_level");
+  if (!(std::isfinite(target) && target > 0.0))
+    throw Error(ST_INVALID_PARAMS, "target scale must be positive and finite");
+  if (level == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
+  const double q = (double)ctx_->primes[level];
+  const double l0 = target * q;
+  if (!std::isfinite(l0)) throw Error(ST_INVALID_PARAMS, "target scale times q overflows");
+  uint64_t bits;
+  memcpy(&bits, &l0, 8);
+  for (uint64_t k = 0; k <= kLabelSearchUlps; ++k)
+    for (int s = 0; s < 2; ++s) {
+      uint64_t b = s == 0 ? bits + k : bits - k;
+      double l;
+      memcpy(&l, &b, 8);
+      if (l / q == target) return l;
+    }
+  throw Error(ST_SCALE_MISMATCH, "scale mismatch");
+}
+
+Ct Evaluator::mul_scalar(const Ct& a, double value, double target) {  // evaluator.rs:361-376, 777-799
+  check_basis(a);
+  if (!std::isfinite(value)) throw Error(ST_INVALID_PARAMS, "scalar must be finite");
+  const double label = exact_product_scale(a->level, target);
+  check_plain_scale(label / a->scale);
+  const double k = std::round(value * (label / a->scale));
+  if (std::fabs(k) >= kMaxScalarInt) throw Error(ST_INVALID_PARAMS, "scalar at this plaintext scale is >= 2^62");
+  ctx_->activate();
+  Ct r = new_ct(a->ncomp, a->level, label);
+  const uint64_t kk = (uint64_t)std::fabs(k);
+  ScalarTable st{};
+  for (uint32_t i = 0; i <= a->level; ++i) {
+    const HostMod& m = ctx_->mods[i];
+    uint64_t w = kk % m.q;
+    if (k < 0.0 && w) w = m.q - w;  // times |k| then negated, folded into one constant
+    st.w[i] = w;
+    st.ws[i] = m.shoup(w);
+  }
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i < a->ncomp; ++i) unary_comp(*ctx_, a->comp(i), r->comp_mut(i), a->level + 1, refs);
+  launch_scalar(ctx_->dt, refs.data(), (int)refs.size(), st, ctx_->stream);
+  count([](OpCounter& c) { c.ct_pt_mults++; });
+  return r;
+}
+
+Ct Evaluator::mul_plain_to_scale(const Ct& a, const Pt& p, double target) {  // evaluator.rs:393-414
+  check_basis(a);
+  check_basis_pt(p);
+  check_level(a->level, p->level);
+  const double label = exact_product_scale(a->level, target);
+  check_plain_scale(label / a->scale);
+  if (p->scale != label / a->scale) throw Error(ST_SCALE_MISMATCH, "scale mismatch");
+  ctx_->activate();
+  Ct r = new_ct(a->ncomp, a->level, label);
+  std::vector<BinRef> bin;
+  for (uint32_t i = 0; i < a->ncomp; ++i) binary_comp(*ctx_, 2, a->comp(i), p->data(), r->comp_mut(i), a->level + 1, bin);
+  launch_binary(ctx_->dt, bin.data(), (int)bin.size(), 2, ctx_->stream);
+  count([](OpCounter& c) { c.ct_pt_mults++; });
+  return r;
+}
+
+void Evaluator::check_mul_operands(const Ct& a, const Ct& b) const {  // evaluator.rs:479-496
+  check_basis(a);
+  check_basis(b);
+  if (a->ncomp != 2 || b->ncomp != 2)
+    throw Error(ST_INVALID_PARAMS, "multiplication needs 2-component ciphertexts; relinearize first");
+  check_level(a->level, b->level);
+  if (a->level == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
+}
+
+Ct Evaluator::mul_no_relin(const Ct& a, const Ct& b) {  // evaluator.rs:422-439
+  check_mul_operands(a, b);
+  ctx_->activate();
+  Ct r = new_ct(3, a->level, a->scale * b->scale);
+  std::vector<TensorRef> refs;
+  const size_t N = ctx_->n;
+  for (uint32_t i = 0; i <= a->level; ++i)
+    refs.push_back(TensorRef{a->comp(0) + i * N, a->comp(1) + i * N, b->comp(0) + i * N, b->comp(1) + i * N,
+                             r->comp_mut(0) + i * N, r->comp_mut(1) + i * N, r->comp_mut(2) + i * N, i, 0});
+  launch_tensor(ctx_->dt, refs.data(), (int)refs.size(), ctx_->stream);
+  count([](OpCounter& c) { c.ct_ct_tensor++; });
+  return r;
+}
+
+void Evaluator::check_key_basis(const DevKey& k) const {  // evaluator.rs:680-696
+  if (k.ctx != ctx_ || k.parts != ctx_->dnum || k.q_limbs != ctx_->L + 1)
+    throw Error(ST_INVALID_PARAMS, "key is not over this evaluator's bases");
+}
+
+const DevKey& Evaluator::relin_key_checked() const {  // evaluator.rs:470-477
+  if (!relin_) throw Error(ST_INVALID_PARAMS, "evaluator has no relinearization key");
+  check_key_basis(*relin_);
+  return *relin_;
+}
+
+Ct Evaluator::relinearize(const Ct& a) {  // evaluator.rs:441-460
+  check_basis(a);
+  if (a->ncomp != 3) throw Error(ST_INVALID_PARAMS, "relinearize needs a 3-component ciphertext");
+  const DevKey& rk = relin_key_checked();
+  ctx_->activate();
+  Ct r = new_ct(2, a->level, a->scale);
+  KsJob j;
+  j.in = a->comp(2);
+  j.key = &rk;
+  j.out_b = r->comp_mut(0);
+  j.out_a = r->comp_mut(1);
+  j.add_b = a->comp(0);
+  j.add_a = a->comp(1);
+  key_switch_many(*ctx_, {j}, a->level);
+  count([](OpCounter& c) { c.relins++; });
+  return r;
+}
+
+Ct Evaluator::mul(const Ct& a, const Ct& b) {  // evaluator.rs:463-467
+  check_mul_operands(a, b);
+  relin_key_checked();
+  return relinearize(mul_no_relin(a, b));
+}
+
+Ct Evaluator::rescale(const Ct& a) {  // evaluator.rs:498-510
+  check_basis(a);
+  const uint32_t l = a->level;
+  if (l == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
+  ctx_->activate();
+  Ct r = new_ct(a->ncomp, l - 1, a->scale / (double)ctx_->primes[l]);
+  std::vector<const uint64_t*> in;
+  std::vector<uint64_t*> out;
+  for (uint32_t i = 0; i < a->ncomp; ++i) {
+    in.push_back(a->comp(i));
+    out.push_back(r->comp_mut(i));
+  }
+  rescale_many(*ctx_, in, l, out);
+  count([](OpCounter& c) { c.rescales++; });
+  return r;
+}
+
+Ct Evaluator::mod_switch_to_level(const Ct& a, uint32_t level) {  // evaluator.rs:513-525
+  check_basis(a);
+  if (level > a->level) throw Error(ST_INVALID_PARAMS, "cannot switch a ciphertext up to a higher level");
+  auto r = std::make_shared<CtObj>(*a);  // a view: the first level+1 limbs of every component
+  r->level = level;
+  return r;
+}
+
+Ct Evaluator::relabel(const Ct& a, double scale) {  // ops.rs:475-477
+  check_basis(a);
+  check_ct_scale(scale);
+  auto r = std::make_shared<CtObj>(*a);
+  r->scale = scale;
+  return r;
+}
+
+// ---- rotations -----------------------------------------------------------------------
+
+void Evaluator::check_galois_input(const Ct& a) const {  // evaluator.rs:665-676
+  check_basis(a);
+  if (a->ncomp != 2) throw Error(ST_INVALID_PARAMS, "rotation needs a 2-component ciphertext; relinearize first");
+}
+
+std::optional<uint64_t> Evaluator::rotation_elt(int32_t steps) const {  // evaluator.rs:633-638
+  const int64_t slots = (int64_t)ctx_->n / 2;
+  const int64_t k = (((int64_t)steps % slots) + slots) % slots;
+  if (k == 0) return std::nullopt;
+  return galois_elt(ctx_->n, (int32_t)k);
+}
+
+const DevKey& Evaluator::galois_key(uint64_t elt) const {  // evaluator.rs:648-663
+  const uint64_t two_n = 2 * ctx_->n;
+  if (elt % 2 == 0 || elt >= two_n)
+    throw Error(ST_INVALID_PARAMS, "Galois element " + std::to_string(elt) + " must be odd and < 2N");
+  for (auto& k : galois_)
+    if (k->elt == elt) {
+      check_key_basis(*k);
+      return *k;
+    }
+  throw Error(ST_INVALID_PARAMS, "missing galois key");
+}
+
+void Evaluator::check_rotation_keys(const std::vector<int32_t>& steps) const {  // evaluator.rs:621-629
+  for (int32_t s : steps) {
+    auto e = rotation_elt(s);
+    if (e) galois_key(*e);
+  }
+}
+
+Ct Evaluator::apply_galois(const Ct& a, uint64_t elt) {  // evaluator.rs:640-646, 800-805
+  const DevKey& gk = galois_key(elt);
+  ctx_->activate();
+  const uint32_t* perm = ctx_->perm(elt);
+  const uint32_t limbs = a->level + 1;
+  Ct r = new_ct(2, a->level, a->scale);
+  auto tmp = ctx_->alloc((size_t)limbs * ctx_->n);
+  std::vector<LimbRef> refs;
+  unary_comp(*ctx_, a->comp(1), tmp->p, limbs, refs);
+  launch_unary(ctx_->dt, refs.data(), (int)refs.size(), 3, nullptr, perm, ctx_->stream);  // sigma_g(c1)
+  KsJob j;
+  j.in = tmp->p;
+  j.key = &gk;
+  j.out_b = r->comp_mut(0);
+  j.out_a = r->comp_mut(1);
+  j.add_b = a->comp(0);
+  j.add_b_perm = perm;  // + sigma_g(c0)
+  key_switch_many(*ctx_, {j}, a->level);
+  count([](OpCounter& c) { c.rotations++; });
+  return r;
+}
+
+Ct Evaluator::rotate(const Ct& a, int32_t steps) {  // evaluator.rs:534-540
+  check_galois_input(a);
+  auto e = rotation_elt(steps);
+  if (!e) return a;
+  return apply_galois(a, *e);
+}
+
+Ct Evaluator::conjugate(const Ct& a) {  // evaluator.rs:547-550
+  check_galois_input(a);
+  return apply_galois(a, 2 * ctx_->n - 1);
+}
+
+std::vector<Ct> Evaluator::hoisted_rotate(const Ct& a, const std::vector<int32_t>& steps) {  // evaluator.rs:572-616
+  check_galois_input(a);
+  std::vector<Ct> out(steps.size());
+  if (!cfg_.hoist) {
+    check_rotation_keys(steps);
+    for (size_t i = 0; i < steps.size(); ++i) out[i] = rotate(a, steps[i]);
+    return out;
+  }
+  std::vector<std::pair<uint64_t, const DevKey*>> keys(steps.size(), {0, nullptr});
+  bool any = false;
+  for (size_t i = 0; i < steps.size(); ++i) {
+    auto e = rotation_elt(steps[i]);
+    if (e) {
+      keys[i] = {*e, &galois_key(*e)};
+      any = true;
+    }
+  }
+  uint64_t nontrivial = 0;
+  if (any) {
+    ctx_->activate();
+    const uint32_t l = a->level;
+    auto conv = ctx_->alloc(conv_limbs(*ctx_, l) * ctx_->n);
+    mod_up_many(*ctx_, {a->comp(1)}, l, {conv->p});
+    std::vector<KsJob> jobs;
+    std::vector<size_t> idx;
+    for (size_t i = 0; i < steps.size(); ++i) {
+      if (!keys[i].second) continue;
+      const uint32_t* perm = ctx_->perm(keys[i].first);
+      Ct r = new_ct(2, l, a->scale);
+      KsJob j;
+      j.in = a->comp(1);
+      j.key = keys[i].second;
+      j.out_b = r->comp_mut(0);
+      j.out_a = r->comp_mut(1);
+      j.add_b = a->comp(0);
+      j.add_b_perm = perm;
+      j.perm = perm;
+      j.conv = conv->p;
+      jobs.push_back(j);
+      out[i] = r;
+      nontrivial++;
+    }
+    key_switch_many(*ctx_, jobs, l);
+  }
+  for (size_t i = 0; i < steps.size(); ++i)
+    if (!keys[i].second) out[i] = a;
+  count([&](OpCounter& c) { c.rotations += nontrivial; });
+  return out;
+}
+
+// ---- BSGS matrix-vector products (crates/ckks-train-ckks/src/linalg.rs:608-893) -------
+
+namespace {
+
+uint32_t entry_level(const Pt& p) { return p->level; }
+uint32_t entry_level(const Ct& c) { return c->level; }
+double entry_scale(const Pt& p) { return p->scale; }
+double entry_scale(const Ct& c) { return c->scale; }
+
+template <class T>
+void check_diagonals(Context& c, uint32_t d, uint32_t stride, const std::vector<T>& entries) {
+  // Diagonals::from_prerotated (linalg.rs:254-282): shape, stride, one level, one scale.
+  if (d == 0 || (d & (d - 1)) || entries.size() != d)
+    throw Error(ST_INVALID_PARAMS, "entries for d (d must be a power of two, one entry per diagonal)");
+  if (stride == 0 || (c.n / 2) % ((uint64_t)d * stride) != 0)
+    throw Error(ST_INVALID_PARAMS, "d * stride must divide the slot count (stride >= 1)");
+  for (auto& e : entries)
+    if (!e) throw Error(ST_INVALID_PARAMS, "null diagonal entry");
+  for (auto& e : entries)
+    if (entry_level(e) != entry_level(entries[0])) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
+  for (auto& e : entries)
+    if (entry_scale(e) != entry_scale(entries[0])) throw Error(ST_SCALE_MISMATCH, "scale mismatch");
+}
+
+std::vector<int32_t> rotation_steps(uint32_t d, uint32_t stride) {  // linalg.rs:433-457
+  auto bg = bsgs_split(d);
+  std::vector<int32_t> s;
+  for (uint32_t k2 = 1; k2 < bg.first; ++k2) s.push_back((int32_t)(k2 * stride));
+  for (uint32_t k1 = 1; k1 < bg.second; ++k1) s.push_back((int32_t)(bg.first * k1 * stride));
+  return s;
+}
+
+}  // namespace
+
+template <class T, class MulF, class FinF>
+Ct Evaluator::bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, const Ct& x, MulF mul, FinF finish) {
+  const auto bg = bsgs_split(d);
+  const uint32_t baby = bg.first, giant = bg.second;
+  const bool share_giant = cfg_.bsgs;
+  std::vector<int32_t> steps;
+  for (uint32_t k2 = 0; k2 < baby; ++k2) steps.push_back((int32_t)(k2 * stride));
+  std::vector<Ct> xs = hoisted_rotate(x, steps);
+  Ct acc;
+  for (uint32_t k1 = 0; k1 < giant; ++k1) {
+    const int64_t shift = (int64_t)baby * k1 * stride;
+    Ct block;
+    if (!share_giant && shift != 0) {
+      for (uint32_t k2 = 0; k2 < baby; ++k2) {
+        Ct t = finish(mul(entries[k1 * baby + k2], xs[k2]));
+        t = rotate(t, (int32_t)shift);
+        block = block ? add(block, t) : t;
+      }
+    } else {
+      Ct inner;
+      for (uint32_t k2 = 0; k2 < baby; ++k2) {
+        Ct t = mul(entries[k1 * baby + k2], xs[k2]);
+        inner = inner ? add(inner, t) : t;
+      }
+      block = finish(inner);
+      if (shift != 0) block = rotate(block, (int32_t)shift);
+    }
+    acc = acc ? add(acc, block) : block;
+  }
+  return acc;
+}
+
+Ct Evaluator::matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x) {
+  check_diagonals(*ctx_, d, stride, entries);
+  check_galois_input(x);                       // linalg.rs:608-622
+  for (auto& p : entries) check_basis_pt(p);
+  for (auto& p : entries)
+    if (p->level != x->level) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
+  check_rotation_keys(rotation_steps(d, stride));
+  return bsgs(d, stride, entries, x, [&](const Pt& w, const Ct& xr) { return mul_plain(xr, w); },
+              [](const Ct& c) { return c; });
+}
+
+Ct Evaluator::matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x) {
+  check_diagonals(*ctx_, d, stride, entries);
+  check_galois_input(x);                       // linalg.rs:642-678
+  for (auto& c : entries) check_galois_input(c);
+  for (auto& c : entries)
+    if (c->level != x->level) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
+  check_rotation_keys(rotation_steps(d, stride));
+  if (x->level == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
+  relin_key_checked();
+  if (cfg_.lazy_relin)
+    return bsgs(d, stride, entries, x, [&](const Ct& w, const Ct& xr) { return mul_no_relin(w, xr); },
+                [&](const Ct& c) { return relinearize(c); });
+  return bsgs(d, stride, entries, x, [&](const Ct& w, const Ct& xr) { return mul(w, xr); },
+              [](const Ct& c) { return c; });
+}
+
+}  // namespace ckg

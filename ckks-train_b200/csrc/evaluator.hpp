@@ -1,0 +1,119 @@
+// The evaluator behind the C ABI: the HeOps contract (crates/ckks-train-ckks/src/ops.rs)
+// with the checks in the CPU evaluator's order, its errors, f64 scale labels and
+// OpCounter increments (crates/ckks-train-ckks/src/evaluator.rs, counter.rs), on
+// device-resident ciphertexts. Ciphertexts are immutable and shared: every op returns a
+// new one, and clone / relabel / mod_switch_to_level share the input's device buffer.
+#pragma once
+#include <array>
+#include <memory>
+#include <mutex>
+#include <optional>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace ckg {
+
+struct CtObj {
+  Context* ctx = nullptr;
+  DevBufPtr buf;
+  size_t offset = 0;       // words from buf->p to component 0
+  size_t comp_stride = 0;  // words between components (>= (level+1) * N)
+  uint32_t ncomp = 0;
+  uint32_t level = 0;
+  double scale = 0;
+  const uint64_t* comp(uint32_t i) const { return buf->p + offset + i * comp_stride; }
+  uint64_t* comp_mut(uint32_t i) const { return buf->p + offset + i * comp_stride; }
+};
+typedef std::shared_ptr<const CtObj> Ct;
+
+struct PtObj {
+  Context* ctx = nullptr;
+  DevBufPtr buf;
+  uint32_t level = 0;
+  double scale = 0;
+  const uint64_t* data() const { return buf->p; }
+};
+typedef std::shared_ptr<const PtObj> Pt;
+
+struct OpCounter {  // counter.rs:42-58
+  uint64_t rotations = 0, relins = 0, ct_ct_tensor = 0, ct_pt_mults = 0, rescales = 0, sse_switches = 0,
+           bootstraps = 0;
+  std::array<uint64_t, 7> words() const {
+    return {rotations, relins, ct_ct_tensor, ct_pt_mults, rescales, sse_switches, bootstraps};
+  }
+};
+
+struct EvalConfig {  // ops.rs:111-178
+  bool hoist = true, bsgs = true, lazy_relin = true;
+};
+
+typedef std::shared_ptr<DevKey> KeyPtr;
+
+class Evaluator {
+ public:
+  Evaluator(Context* ctx, KeyPtr relin, std::vector<KeyPtr> galois, EvalConfig cfg);
+
+  Context* ctx() const { return ctx_; }
+  const EvalConfig& config() const { return cfg_; }
+  OpCounter counter() const;
+  void reset_counter();
+  void add_counts(const OpCounter& c);
+  std::unique_ptr<Evaluator> fork() const;
+  bool has_relin_key() const { return (bool)relin_; }
+  bool has_galois_key(int32_t step) const;
+  bool owns(const Ct& ct) const { return ct && ct->ctx == ctx_; }
+
+  Ct upload(const uint64_t* src, bool device_src, uint32_t ncomp, uint32_t level, double scale);
+  Pt upload_pt(const uint64_t* src, bool device_src, uint32_t level, double scale);
+
+  Ct add(const Ct& a, const Ct& b) { return add_sub(a, b, false); }
+  Ct sub(const Ct& a, const Ct& b) { return add_sub(a, b, true); }
+  Ct negate(const Ct& a);
+  Ct add_plain(const Ct& a, const Pt& p);
+  Ct mul_plain(const Ct& a, const Pt& p);
+  Ct mul_scalar(const Ct& a, double value, double target);
+  Ct mul_plain_to_scale(const Ct& a, const Pt& p, double target);
+  Ct mul_no_relin(const Ct& a, const Ct& b);
+  Ct relinearize(const Ct& a);
+  Ct mul(const Ct& a, const Ct& b);
+  Ct rescale(const Ct& a);
+  Ct mod_switch_to_level(const Ct& a, uint32_t level);
+  Ct relabel(const Ct& a, double scale);
+  Ct rotate(const Ct& a, int32_t steps);
+  Ct conjugate(const Ct& a);
+  std::vector<Ct> hoisted_rotate(const Ct& a, const std::vector<int32_t>& steps);
+  double exact_product_scale(uint32_t level, double target) const;
+  Ct matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x);
+  Ct matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x);
+
+ private:
+  Ct add_sub(const Ct& a, const Ct& b, bool sub);
+  Ct new_ct(uint32_t ncomp, uint32_t level, double scale);
+  void check_basis(const Ct& a) const;
+  void check_basis_pt(const Pt& p) const;
+  void check_mul_operands(const Ct& a, const Ct& b) const;
+  void check_galois_input(const Ct& a) const;
+  const DevKey& relin_key_checked() const;
+  const DevKey& galois_key(uint64_t elt) const;
+  void check_key_basis(const DevKey& k) const;
+  std::optional<uint64_t> rotation_elt(int32_t steps) const;
+  void check_rotation_keys(const std::vector<int32_t>& steps) const;
+  Ct apply_galois(const Ct& a, uint64_t elt);
+  template <class F>
+  void count(F f) {
+    std::lock_guard<std::mutex> lk(mu_);
+    f(counter_);
+  }
+  template <class T, class MulF, class FinF>
+  Ct bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, const Ct& x, MulF mul, FinF finish);
+
+  Context* ctx_;
+  KeyPtr relin_;
+  std::vector<KeyPtr> galois_;
+  EvalConfig cfg_;
+  mutable std::mutex mu_;
+  OpCounter counter_;
+};
+
+}  // namespace ckg

@@ -1,0 +1,643 @@
+// sm_100a kernels of the RNS-CKKS evaluator path: batched negacyclic NTT / INTT, base
+// conversion (ModUp / ModDown / rescale), the key-switch inner product, the ModDown and
+// rescale finish, element-wise ops and the NTT-form automorphism.
+//
+// All arithmetic is 64-bit integer on the IMAD pipe; the only floating-point step is the
+// overflow estimate of exact base conversion, done with __dmul_rn / __dadd_rn so that no
+// multiply-add is contracted (crates/ckks-train-core/src/baseconv.rs:198-206).
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "kernels.cuh"
+#include "launch.hpp"
+
+namespace ckg {
+
+// ------------------------------------------------------------------------------------
+// NTT. Forward: Harvey Cooley-Tukey, natural order in, bit-reversed order out, values
+// lazily in [0, 4q) between stages (crates/ckks-train-core/src/ntt.rs:141-179); inverse:
+// Gentleman-Sande with N^-1 fused into the last stage (ntt.rs:184-232). Twiddles are the
+// full-N tables roots[bitrev(i)] = psi^i as (w, floor(w 2^64 / q)) pairs.
+//
+// N = 2^logN >= 2^12 runs in two passes over a 2^(logN-8) x 256 matrix view of each limb
+// (element x = 256 * row + col). The first logN - 8 forward stages pair elements of one
+// column (stride >= 256), the last 8 pair elements of one row. Each pass loads a tile,
+// runs its stages in registers as two radix-2^E phases with one shared-memory exchange,
+// and writes the tile back (in place or to another buffer).
+// ------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kRowLog = 8;
+constexpr int kRow = 1 << kRowLog;  // 256
+constexpr int kCols = 16;           // columns per CTA in the column pass
+constexpr int kRowsPerCta = 16;     // rows per CTA in the row pass
+constexpr int kRowPad = kRow + kRow / 16;  // padded row stride in shared memory
+
+CKG_DEV void ct_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
+  uint64_t xr = csub(x, two_q);
+  uint64_t t = mul_shoup_lazy(y, w.x, w.y, q);
+  x = xr + t;
+  y = xr + two_q - t;
+}
+
+CKG_DEV void gs_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
+  uint64_t s = x + y;
+  uint64_t d = x + two_q - y;
+  x = csub(s, two_q);
+  y = mul_shoup_lazy(d, w.x, w.y, q);
+}
+
+CKG_DEV ulonglong2 ldtw(const ulonglong2* t, uint32_t i) { return __ldg(t + i); }
+
+CKG_DEV int pad_idx(int k) { return k + (k >> 4); }
+
+// Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
+template <int LOGS>
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
+    k_ntt_fwd_cols(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n) {
+  constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
+  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
+  const LimbRef ref = b.r[blockIdx.y];
+  const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
+  const int col = blockIdx.x * kCols + c;
+  uint64_t x[1 << E1];
+#pragma unroll
+  for (int j = 0; j < (1 << E1); ++j) x[j] = ref.src[col + (size_t)kRow * (ts + TPS * j)];
+#pragma unroll
+  for (int r = 0; r < E1; ++r) {
+    const int half = 1 << (E1 - 1 - r);
+#pragma unroll
+    for (int j = 0; j < (1 << E1); ++j)
+      if (!(j & half)) ct_bf(x[j], x[j + half], ldtw(roots, (1u << r) + (j >> (E1 - r))), q, two_q);
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << E1); ++j) sm[(ts + TPS * j) * kCols + c] = x[j];
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int t2 = ts + TPS * v;
+    uint64_t y[1 << E2];
+#pragma unroll
+    for (int j = 0; j < (1 << E2); ++j) y[j] = sm[((t2 << E2) + j) * kCols + c];
+#pragma unroll
+    for (int r = E1; r < LOGS; ++r) {
+      const int half = 1 << (LOGS - 1 - r);
+#pragma unroll
+      for (int j = 0; j < (1 << E2); ++j)
+        if (!(j & half)) {
+          const int k = (t2 << E2) + j;
+          ct_bf(y[j], y[j + half], ldtw(roots, (1u << r) + (k >> (LOGS - r))), q, two_q);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << E2); ++j) ref.dst[col + (size_t)kRow * ((t2 << E2) + j)] = y[j];
+  }
+}
+
+// Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
+__global__ void __launch_bounds__(256)
+    k_ntt_fwd_rows(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n) {
+  __shared__ uint64_t sm[kRowsPerCta * kRowPad];
+  const LimbRef ref = b.r[blockIdx.y];
+  const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  const int s0 = log_n - kRowLog;
+  const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
+  const uint32_t row = blockIdx.x * kRowsPerCta + rr;
+  const uint64_t* src = ref.src + (size_t)row * kRow;
+  uint64_t x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = src[t + 16 * j];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int half = 1 << (3 - r);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & half))
+        ct_bf(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, two_q);
+  }
+  uint64_t* srow = sm + rr * kRowPad;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) srow[pad_idx(t + 16 * j)] = x[j];
+  __syncwarp();
+  // A row's 16 threads form half a warp, so the exchange only needs a warp barrier.
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = srow[pad_idx(16 * t + j)];
+#pragma unroll
+  for (int r = 4; r < 8; ++r) {
+    const int half = 1 << (7 - r);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & half)) {
+        const int k = 16 * t + j;
+        ct_bf(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, two_q);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    uint64_t v = csub(x[j], two_q);
+    srow[pad_idx(16 * t + j)] = csub(v, q);
+  }
+  __syncthreads();
+  uint64_t* dst = ref.dst + (size_t)blockIdx.x * kRowsPerCta * kRow;
+#pragma unroll
+  for (int i = 0; i < kRowsPerCta; ++i) dst[i * kRow + threadIdx.x] = sm[i * kRowPad + pad_idx(threadIdx.x)];
+}
+
+// Inverse row pass: GS stages u = 0..7 (pair distance 2^u) within 256-point rows.
+__global__ void __launch_bounds__(256)
+    k_ntt_inv_rows(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n) {
+  __shared__ uint64_t sm[kRowsPerCta * kRowPad];
+  const LimbRef ref = b.r[blockIdx.y];
+  const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  const uint64_t* src = ref.src + (size_t)blockIdx.x * kRowsPerCta * kRow;
+#pragma unroll
+  for (int i = 0; i < kRowsPerCta; ++i) sm[i * kRowPad + pad_idx(threadIdx.x)] = src[i * kRow + threadIdx.x];
+  __syncthreads();
+  const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
+  const uint32_t row = blockIdx.x * kRowsPerCta + rr;
+  uint64_t* srow = sm + rr * kRowPad;
+  uint64_t x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = srow[pad_idx(16 * t + j)];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int d = 1 << u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & d)) {
+        const uint32_t k = 16 * t + j;
+        const uint32_t h = 1u << (log_n - 1 - u);
+        gs_bf(x[j], x[j + d], ldtw(roots, h + (row << (7 - u)) + (k >> (u + 1))), q, two_q);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = x[j];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = srow[pad_idx(t + 16 * j)];
+#pragma unroll
+  for (int u = 4; u < 8; ++u) {
+    const int d = 1 << (u - 4);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & d)) {
+        const uint32_t k = t + 16 * j;
+        const uint32_t h = 1u << (log_n - 1 - u);
+        gs_bf(x[j], x[j + d], ldtw(roots, h + (row << (7 - u)) + (k >> (u + 1))), q, two_q);
+      }
+  }
+  uint64_t* dst = ref.dst + (size_t)row * kRow;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dst[t + 16 * j] = x[j];
+}
+
+// Inverse column pass: GS stages u = 8..logN-1 on 2^LOGS-point columns, N^-1 fused into
+// the last stage, output in [0, q).
+template <int LOGS>
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
+    k_ntt_inv_cols(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n) {
+  constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
+  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
+  const LimbRef ref = b.r[blockIdx.y];
+  const PrimeConst* P = pc + ref.prime;
+  const uint64_t q = __ldg(&P->q), two_q = 2 * q;
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
+  const int col = blockIdx.x * kCols + c;
+  uint64_t x[1 << F1];
+#pragma unroll
+  for (int j = 0; j < (1 << F1); ++j) x[j] = ref.src[col + (size_t)kRow * ((ts << F1) + j)];
+  // local stage v: pair distance 2^v, twiddle index 2^(LOGS-1-v) + (k >> (v+1))
+#pragma unroll
+  for (int v = 0; v < F1; ++v) {
+    const int d = 1 << v;
+#pragma unroll
+    for (int j = 0; j < (1 << F1); ++j)
+      if (!(j & d)) {
+        const uint32_t k = (ts << F1) + j;
+        gs_bf(x[j], x[j + d], ldtw(roots, (1u << (LOGS - 1 - v)) + (k >> (v + 1))), q, two_q);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << F1); ++j) sm[((ts << F1) + j) * kCols + c] = x[j];
+  __syncthreads();
+  const uint64_t ninv = __ldg(&P->ninv), ninv_s = __ldg(&P->ninv_s);
+  const uint64_t wninv = __ldg(&P->wninv), wninv_s = __ldg(&P->wninv_s);
+#pragma unroll
+  for (int vv = 0; vv < V; ++vv) {
+    const int t2 = ts + TPS * vv;
+    uint64_t y[1 << F2];
+#pragma unroll
+    for (int j = 0; j < (1 << F2); ++j) y[j] = sm[(t2 + (j << F1)) * kCols + c];
+#pragma unroll
+    for (int v = F1; v < LOGS - 1; ++v) {
+      const int d = 1 << (v - F1);
+#pragma unroll
+      for (int j = 0; j < (1 << F2); ++j)
+        if (!(j & d)) {
+          const uint32_t k = t2 + (j << F1);
+          gs_bf(y[j], y[j + d], ldtw(roots, (1u << (LOGS - 1 - v)) + (k >> (v + 1))), q, two_q);
+        }
+    }
+    {  // last stage: pairs (k, k + 2^(LOGS-1)), times N^-1
+      const int d = 1 << (F2 - 1);
+#pragma unroll
+      for (int j = 0; j < (1 << F2); ++j)
+        if (!(j & d)) {
+          uint64_t s = y[j] + y[j + d], df = y[j] + two_q - y[j + d];
+          y[j] = csub(mul_shoup_lazy(s, ninv, ninv_s, q), q);
+          y[j + d] = csub(mul_shoup_lazy(df, wninv, wninv_s, q), q);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << F2); ++j) ref.dst[col + (size_t)kRow * (t2 + (j << F1))] = y[j];
+  }
+}
+
+// Small transforms (logN <= 11): one CTA per limb, the limb in shared memory, radix-2.
+__global__ void k_ntt_small(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+                            const ulonglong2* __restrict__ twf, const ulonglong2* __restrict__ twi, int log_n,
+                            int inverse) {
+  extern __shared__ uint64_t sm[];
+  const LimbRef ref = b.r[blockIdx.y];
+  const PrimeConst* P = pc + ref.prime;
+  const uint64_t q = __ldg(&P->q), two_q = 2 * q;
+  const int n = 1 << log_n, half_n = n >> 1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sm[i] = ref.src[i];
+  __syncthreads();
+  if (!inverse) {
+    const ulonglong2* roots = twf + ((size_t)ref.prime << log_n);
+    for (int s = 0; s < log_n; ++s) {
+      const int t = half_n >> s;
+      for (int bf = threadIdx.x; bf < half_n; bf += blockDim.x) {
+        const int g = bf / t, k = bf % t;
+        const int i0 = 2 * t * g + k;
+        ct_bf(sm[i0], sm[i0 + t], ldtw(roots, (1u << s) + g), q, two_q);
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ref.dst[i] = csub(csub(sm[i], two_q), q);
+  } else {
+    const ulonglong2* roots = twi + ((size_t)ref.prime << log_n);
+    for (int u = 0; u < log_n - 1; ++u) {
+      const int t = 1 << u;
+      for (int bf = threadIdx.x; bf < half_n; bf += blockDim.x) {
+        const int g = bf / t, k = bf % t;
+        const int i0 = 2 * t * g + k;
+        gs_bf(sm[i0], sm[i0 + t], ldtw(roots, (half_n >> u) + g), q, two_q);
+      }
+      __syncthreads();
+    }
+    const uint64_t ninv = __ldg(&P->ninv), ninv_s = __ldg(&P->ninv_s);
+    const uint64_t wninv = __ldg(&P->wninv), wninv_s = __ldg(&P->wninv_s);
+    for (int k = threadIdx.x; k < half_n; k += blockDim.x) {
+      uint64_t x = sm[k], y = sm[k + half_n];
+      ref.dst[k] = csub(mul_shoup_lazy(x + y, ninv, ninv_s, q), q);
+      ref.dst[k + half_n] = csub(mul_shoup_lazy(x + two_q - y, wninv, wninv_s, q), q);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Base conversion (ModUp digit lift, ModDown P -> Q, rescale last-prime lift).
+// One thread per coefficient: the source words are read once, the n_src values y_j stay
+// in registers, and each target is one 128-bit multiply-accumulate chain and one
+// reduction. Exact conversion (n_src > 1) subtracts e * S with the f64 estimate
+// e = floor(sum_j f64(y_j) * f64(1/s_j)), each product and sum rounded to nearest in source
+// order starting from 0 (crates/ckks-train-core/src/baseconv.rs:198-206, 221-230).
+// ------------------------------------------------------------------------------------
+
+template <int NS>
+__global__ void __launch_bounds__(256)
+    k_bconv(const __grid_constant__ ConvBatch cb, const PrimeConst* __restrict__ pc, int n) {
+  const ConvJob& job = cb.j[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int n_src = NS > 0 ? NS : cb.n_src;
+  const uint64_t* tab = job.table;
+  uint64_t y[kMaxSrc];
+  double f = 0.0;
+#pragma unroll
+  for (int j = 0; j < kMaxSrc; ++j) {
+    if (j < n_src) {
+      const uint64_t* s = tab + ConvLayout::kSrcWords * j;
+      const uint32_t p = (uint32_t)__ldg(s);
+      const uint64_t q = __ldg(&pc[p].q);
+      uint64_t x = job.src[j * job.src_stride + c];
+      x = add_mod(x, __ldg(s + 3), q);
+      const uint64_t yj = mul_shoup(x, __ldg(s + 1), __ldg(s + 2), q);
+      y[j] = yj;
+      const double prod = __dmul_rn(__ull2double_rn(yj), __longlong_as_double((long long)__ldg(s + 4)));
+      f = j == 0 ? prod : __dadd_rn(f, prod);
+    }
+  }
+  const uint64_t e = n_src > 1 ? (uint64_t)floor(f) : 0;
+  const uint64_t* dtab = tab + ConvLayout::kSrcWords * n_src;
+  const int dw = ConvLayout::dst_words(n_src);
+  for (int t = 0; t < cb.n_dst; ++t) {
+    const uint64_t* d = dtab + dw * t;
+    const PrimeConst& P = pc[(uint32_t)__ldg(d)];
+    uint64_t hi = 0, lo = __ldg(d + 2);  // + (t - h_t)
+    mac128(hi, lo, e, __ldg(d + 1));      // + e * (t - S_t)
+#pragma unroll
+    for (int j = 0; j < kMaxSrc; ++j)
+      if (j < n_src) mac128(hi, lo, y[j], __ldg(d + 4 + j));
+    job.dst[t * job.dst_stride + c] = reduce128(hi, lo, P);
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Key-switch inner product (crates/ckks-train-ckks/src/keyswitch.rs:230-309): for every
+// limb i of Q_l * P, out_b = sum_j d_j * b_j and out_a = sum_j d_j * a_j, accumulated
+// exactly in 128 bits and reduced once. Digit j's limb i is the input polynomial's limb
+// when prime i belongs to digit j, else the converted limb; with a Galois permutation
+// every digit word is read at perm[c] (hoisted rotation).
+// ------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256)
+    k_inner_product(const __grid_constant__ IpBatch ib, const PrimeConst* __restrict__ pc, int log_n) {
+  const int n = 1 << log_n;
+  const IpJob& job = ib.j[blockIdx.z];
+  const int i = blockIdx.y;  // limb of Q_l * P: 0..l data primes, l+1..l+k special
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int l = ib.level;
+  const bool is_q = i <= l;
+  const uint32_t prime = is_q ? i : (ib.L + 1) + (i - l - 1);
+  const int key_limb = is_q ? i : ib.key_q + (i - l - 1);
+  const size_t key_limbs = (size_t)(ib.key_q + ib.k);
+  const uint32_t src_c = job.perm ? __ldg(job.perm + c) : (uint32_t)c;
+  uint64_t bh = 0, bl = 0, ah = 0, al = 0;
+  for (int j = 0; j < ib.ndig; ++j) {
+    const int start = j * ib.alpha;
+    const int end = min(start + ib.alpha, l + 1);
+    uint64_t d;
+    if (is_q && i >= start && i < end) {
+      d = job.in[((size_t)i << log_n) + src_c];
+    } else {
+      const int t = i < start ? i : i - (end - start);
+      d = job.conv[j][((size_t)t << log_n) + src_c];
+    }
+    const uint64_t* kb = job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n;
+    const uint64_t* ka = job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n;
+    mac128(bh, bl, d, __ldcs(kb + c));
+    mac128(ah, al, d, __ldcs(ka + c));
+  }
+  const PrimeConst& P = pc[prime];
+  job.out_b[((size_t)i << log_n) + c] = reduce128(bh, bl, P);
+  job.out_a[((size_t)i << log_n) + c] = reduce128(ah, al, P);
+}
+
+// ------------------------------------------------------------------------------------
+// ModDown / rescale finish (baseconv.rs:286-289, 505-510): out = (x - t) * c (+ add).
+// ------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256)
+    k_finish(const __grid_constant__ FinBatch fb, const PrimeConst* __restrict__ pc, int n) {
+  const FinRef& r = fb.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const uint64_t q = __ldg(&pc[r.prime].q);
+  uint64_t v = mul_shoup(sub_mod(r.x[c], r.t[c], q), r.c, r.c_s, q);
+  if (r.add) v = add_mod(v, r.add[r.add_perm ? __ldg(r.add_perm + c) : c], q);
+  r.out[c] = v;
+}
+
+// ------------------------------------------------------------------------------------
+// Element-wise ops (crates/ckks-train-core/src/poly.rs:131-190) and the NTT-form
+// automorphism gather (poly.rs:255-262).
+// ------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256)
+    k_binary(const __grid_constant__ BinBatch bb, const PrimeConst* __restrict__ pc, int n) {
+  const BinRef& r = bb.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const PrimeConst& P = pc[r.prime];
+  const uint64_t a = r.a[c], b = r.b[c];
+  uint64_t v;
+  if (bb.op == 0) v = add_mod(a, b, P.q);
+  else if (bb.op == 1) v = sub_mod(a, b, P.q);
+  else v = mul_mod(a, b, P);
+  r.out[c] = v;
+}
+
+// op 0: negate; op 1: multiply by the per-limb Shoup constant (aux selects it from
+// `consts`, 2 words per entry); op 2: copy; op 3: gather through `perm`.
+__global__ void __launch_bounds__(256)
+    k_unary(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc, int n, int op,
+            const uint64_t* __restrict__ consts, const uint32_t* __restrict__ perm) {
+  const LimbRef& r = b.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const uint64_t q = __ldg(&pc[r.prime].q);
+  uint64_t v;
+  if (op == 0) {
+    v = sub_mod(0, r.src[c], q);
+  } else if (op == 1) {
+    v = mul_shoup(r.src[c], __ldg(consts + 2 * r.aux), __ldg(consts + 2 * r.aux + 1), q);
+  } else if (op == 2) {
+    v = r.src[c];
+  } else {
+    v = r.src[__ldg(perm + c)];
+  }
+  r.dst[c] = v;
+}
+
+__global__ void __launch_bounds__(256)
+    k_tensor(const __grid_constant__ TensorBatch tb, const PrimeConst* __restrict__ pc, int n) {
+  const TensorRef& r = tb.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const PrimeConst& P = pc[r.prime];
+  const uint64_t a0 = r.a0[c], a1 = r.a1[c], b0 = r.b0[c], b1 = r.b1[c];
+  r.d0[c] = mul_mod(a0, b0, P);
+  r.d1[c] = add_mod(mul_mod(a0, b1, P), mul_mod(a1, b0, P), P.q);
+  r.d2[c] = mul_mod(a1, b1, P);
+}
+
+__global__ void __launch_bounds__(256)
+    k_scalar(const __grid_constant__ LimbBatch b, const __grid_constant__ ScalarTable st,
+             const PrimeConst* __restrict__ pc, int n) {
+  const LimbRef& r = b.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const uint64_t q = __ldg(&pc[r.prime].q);
+  r.dst[c] = mul_shoup(r.src[c], st.w[r.prime], st.ws[r.prime], q);
+}
+
+template <class T>
+void set_smem(T* fn, int bytes) {
+  cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <int LOGS>
+void launch_cols(bool inverse, const LimbBatch& b, const DevTables& d, cudaStream_t st) {
+  const int smem = (1 << LOGS) * kCols * 8;
+  const int threads = kCols * (1 << (LOGS / 2));
+  dim3 grid(kRow / kCols, b.count);
+  if (!inverse) {
+    if (smem > 48 * 1024) set_smem(k_ntt_fwd_cols<LOGS>, smem);
+    k_ntt_fwd_cols<LOGS><<<grid, threads, smem, st>>>(b, d.prime, d.tw_fwd, d.log_n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  } else {
+    if (smem > 48 * 1024) set_smem(k_ntt_inv_cols<LOGS>, smem);
+    k_ntt_inv_cols<LOGS><<<grid, threads, smem, st>>>(b, d.prime, d.tw_inv, d.log_n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_cols_any(bool inverse, const LimbBatch& b, const DevTables& d, cudaStream_t st) {
+  switch (d.log_n - kRowLog) {
+    case 4: launch_cols<4>(inverse, b, d, st); break;
+    case 5: launch_cols<5>(inverse, b, d, st); break;
+    case 6: launch_cols<6>(inverse, b, d, st); break;
+    case 7: launch_cols<7>(inverse, b, d, st); break;
+    case 8: launch_cols<8>(inverse, b, d, st); break;
+    case 9: launch_cols<9>(inverse, b, d, st); break;
+    default: break;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Host launchers (declared in launch.hpp). Lists longer than one launch's capacity are
+// split; every launch goes to stream `st` and is counted in g_launches.
+// ------------------------------------------------------------------------------------
+
+std::atomic<uint64_t> g_launches{0};
+
+void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st) {
+  LimbBatch b;
+  for (int off = 0; off < count; off += kMaxLimbs) {
+    b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
+    for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
+    if (d.log_n <= 11) {
+      const int n = 1 << d.log_n;
+      const int threads = n / 2 < 512 ? (n / 2 < 32 ? 32 : n / 2) : 512;
+      k_ntt_small<<<dim3(1, b.count), threads, n * 8, st>>>(b, d.prime, d.tw_fwd, d.tw_inv, d.log_n, inverse);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      continue;
+    }
+    const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), b.count);
+    if (!inverse) {
+      launch_cols_any(false, b, d, st);
+      for (int i = 0; i < b.count; ++i) b.r[i].src = b.r[i].dst;  // second pass in place on dst
+      k_ntt_fwd_rows<<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.log_n);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+    } else {
+      k_ntt_inv_rows<<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.log_n);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      for (int i = 0; i < b.count; ++i) b.r[i].src = b.r[i].dst;
+      launch_cols_any(true, b, d, st);
+    }
+  }
+}
+
+void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st) {
+  ConvBatch cb;
+  cb.n_src = n_src;
+  cb.n_dst = n_dst;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxConv) {
+    cb.count = count - off < kMaxConv ? count - off : kMaxConv;
+    for (int i = 0; i < cb.count; ++i) cb.j[i] = jobs[off + i];
+    dim3 grid((n + 255) / 256, cb.count);
+    switch (n_src) {
+      case 1: k_bconv<1><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      case 2: k_bconv<2><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      case 4: k_bconv<4><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      case 8: k_bconv<8><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      default: k_bconv<0><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+  }
+}
+
+void launch_inner_product(const DevTables& d, const IpBatch& proto, const IpJob* jobs, int count,
+                          cudaStream_t st) {
+  IpBatch ib = proto;
+  const int n = 1 << d.log_n;
+  const int limbs = proto.level + 1 + proto.k;
+  for (int off = 0; off < count; off += kMaxIp) {
+    ib.count = count - off < kMaxIp ? count - off : kMaxIp;
+    for (int i = 0; i < ib.count; ++i) ib.j[i] = jobs[off + i];
+    dim3 grid((n + 255) / 256, limbs, ib.count);
+    k_inner_product<<<grid, 256, 0, st>>>(ib, d.prime, d.log_n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {
+  FinBatch fb;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxFin) {
+    fb.count = count - off < kMaxFin ? count - off : kMaxFin;
+    for (int i = 0; i < fb.count; ++i) fb.r[i] = refs[off + i];
+    k_finish<<<dim3((n + 255) / 256, fb.count), 256, 0, st>>>(fb, d.prime, n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st) {
+  BinBatch bb;
+  bb.op = op;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxBin) {
+    bb.count = count - off < kMaxBin ? count - off : kMaxBin;
+    for (int i = 0; i < bb.count; ++i) bb.r[i] = refs[off + i];
+    k_binary<<<dim3((n + 255) / 256, bb.count), 256, 0, st>>>(bb, d.prime, n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
+                  const uint32_t* perm, cudaStream_t st) {
+  LimbBatch b;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxLimbs) {
+    b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
+    for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
+    k_unary<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, d.prime, n, op, consts, perm);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st) {
+  TensorBatch tb;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxTensor) {
+    tb.count = count - off < kMaxTensor ? count - off : kMaxTensor;
+    for (int i = 0; i < tb.count; ++i) tb.r[i] = refs[off + i];
+    k_tensor<<<dim3((n + 255) / 256, tb.count), 256, 0, st>>>(tb, d.prime, n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st) {
+  LimbBatch b;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxLimbs) {
+    b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
+    for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
+    k_scalar<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, table, d.prime, n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+}  // namespace ckg

@@ -1,0 +1,143 @@
+// Launch descriptors shared by the device kernels and the host engine.
+//
+// Kernels take their work lists by value (`__grid_constant__` parameter structs), so a
+// launch needs no separate descriptor upload and a captured CUDA graph keeps its own copy.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "modarith.cuh"
+
+namespace ckg {
+
+// One limb of a batched limb-wise kernel: N words at src (read) and dst (written; may
+// equal src), reduced modulo the prime with global index `prime`.
+struct LimbRef {
+  const uint64_t* src;
+  uint64_t* dst;
+  uint32_t prime;
+  uint32_t aux;  // kernel-specific (e.g. the second operand's limb offset)
+};
+
+constexpr int kMaxLimbs = 256;  // per launch; larger lists are split by the host
+struct LimbBatch {
+  int count;
+  int pad;
+  LimbRef r[kMaxLimbs];
+};
+
+// Element-wise binary op over limbs: out = a (op) b, b given per limb.
+struct BinRef {
+  const uint64_t* a;
+  const uint64_t* b;
+  uint64_t* out;
+  uint32_t prime;
+  uint32_t pad;
+};
+constexpr int kMaxBin = 192;
+struct BinBatch {
+  int count;
+  int op;  // 0 add, 1 sub, 2 mul
+  BinRef r[kMaxBin];
+};
+
+// Base conversion job: source limbs (coefficient form) -> target limbs (coefficient form)
+// out_t = (sum_j y_j * (S/s_j mod t) - e * (S mod t) - h_t) mod t,
+// y_j = [(x_j + h_j) * (S/s_j)^-1]_{s_j}, e = floor(sum_j f64(y_j) * f64(1/s_j)) when n_src > 1.
+// `table` points at a device record laid out by ConvLayout below.
+constexpr int kMaxSrc = 16;
+constexpr int kMaxDst = 64;
+struct ConvJob {
+  const uint64_t* src;   // n_src limbs, limb j at src + j * src_stride
+  uint64_t* dst;         // n_dst limbs, limb t at dst + t * dst_stride
+  const uint64_t* table;
+  uint64_t src_stride;
+  uint64_t dst_stride;
+};
+constexpr int kMaxConv = 32;
+struct ConvBatch {
+  int count;
+  int n_src;
+  int n_dst;
+  int pad;
+  ConvJob j[kMaxConv];
+};
+
+// Table record (u64 words):
+//   src block, 5 words per source j: prime, qhat_inv, qhat_inv_shoup, half_j, bits(1.0/s_j)
+//   dst block, (4 + n_src) words per target t: prime, (t - [S]_t), (t - [h]_t) mod t, pad, w_t0..w_t(n_src-1)
+struct ConvLayout {
+  static constexpr int kSrcWords = 5;
+  static __host__ __device__ int dst_words(int n_src) { return 4 + n_src; }
+  static __host__ __device__ int size(int n_src, int n_dst) { return kSrcWords * n_src + dst_words(n_src) * n_dst; }
+};
+
+// Key-switch inner product of one level-l polynomial (module docs of keyswitch.cu).
+constexpr int kMaxDigits = 16;
+struct IpJob {
+  const uint64_t* in;                 // the switched polynomial (NTT form, l+1 limbs)
+  const uint64_t* conv[kMaxDigits];   // digit j's converted limbs (targets, NTT form)
+  const uint64_t* key;                // key base: part j, b/a, (L+1+k) limbs
+  uint64_t* out_b;                    // l+1+k limbs
+  uint64_t* out_a;
+  const uint32_t* perm;               // optional NTT-form Galois permutation (hoisting)
+};
+constexpr int kMaxIp = 16;
+struct IpBatch {
+  int count;
+  int level;   // l
+  int ndig;    // digits at level l
+  int alpha;   // primes per digit
+  int L;       // max level of the parameters (special prime t has global index L+1+t)
+  int k;       // special primes
+  int key_q;   // data limbs per key part (the key's max level + 1)
+  int pad;
+  IpJob j[kMaxIp];
+};
+
+// Finish of ModDown / rescale: out_i = (x_i - t_i) * c_i (+ add_i) mod q_i.
+struct FinRef {
+  const uint64_t* x;
+  const uint64_t* t;
+  const uint64_t* add;       // may be null
+  const uint32_t* add_perm;  // optional: the addend is read as add[add_perm[c]]
+  uint64_t* out;
+  uint64_t c;            // the constant and its Shoup companion
+  uint64_t c_s;
+  uint32_t prime;
+  uint32_t pad;
+};
+constexpr int kMaxFin = 96;
+struct FinBatch {
+  int count;
+  int pad;
+  FinRef r[kMaxFin];
+};
+
+// Ciphertext tensor product per limb: d0 = a0 b0, d1 = a0 b1 + a1 b0, d2 = a1 b1.
+struct TensorRef {
+  const uint64_t* a0;
+  const uint64_t* a1;
+  const uint64_t* b0;
+  const uint64_t* b1;
+  uint64_t* d0;
+  uint64_t* d1;
+  uint64_t* d2;
+  uint32_t prime;
+  uint32_t pad;
+};
+constexpr int kMaxTensor = 96;
+struct TensorBatch {
+  int count;
+  int pad;
+  TensorRef r[kMaxTensor];
+};
+
+// Multiplication of limbs by a per-prime constant (Shoup pair per global prime index).
+constexpr int kMaxPrimes = 64;
+struct ScalarTable {
+  uint64_t w[kMaxPrimes];
+  uint64_t ws[kMaxPrimes];
+};
+
+}  // namespace ckg

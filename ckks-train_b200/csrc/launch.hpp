@@ -1,0 +1,34 @@
+// Host-side launchers of the device kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "kernels.cuh"
+
+namespace ckg {
+
+// Kernel launches issued by this library since it was loaded.
+extern std::atomic<uint64_t> g_launches;
+
+// Device tables of one context: per-prime constants and the twiddle tables.
+struct DevTables {
+  const PrimeConst* prime;   // [n_primes]
+  const ulonglong2* tw_fwd;  // [n_primes][N] (w, w') with roots[bitrev(i)] = psi^i
+  const ulonglong2* tw_inv;  // [n_primes][N] inverse roots
+  int log_n;
+};
+
+void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st);
+void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st);
+void launch_inner_product(const DevTables& d, const IpBatch& proto, const IpJob* jobs, int count,
+                          cudaStream_t st);
+void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
+void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st);
+void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
+                  const uint32_t* perm, cudaStream_t st);
+
+void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st);
+void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st);
+
+}  // namespace ckg

@@ -1,0 +1,564 @@
+"""Python mirror of the reference's ``HeOps`` evaluator interface over ``libckg.so``.
+
+The names, argument meanings and errors follow ``crates/ckks-train-ckks/src/ops.rs:198-356``
+(``HeOps``) and the CPU ``Evaluator`` it documents (``crates/ckks-train-ckks/src/evaluator.rs``):
+every method returns a new ciphertext, failures raise the ``HekitError`` kind the
+reference returns, and the ``OpCounter`` is kept exactly. All arithmetic runs in the
+sm_100a kernels of the C ABI (``include/ckg.h``); there is no CPU fallback: loading fails
+loudly when the library is missing.
+"""
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libckg.so")
+
+U64P = C.POINTER(C.c_uint64)
+U32P = C.POINTER(C.c_uint32)
+I32P = C.POINTER(C.c_int32)
+VP = C.c_void_p
+
+HOIST, BSGS, LAZY_RELIN = 1, 2, 4
+
+
+# ---- errors (crates/ckks-train-core/src/error.rs:7-21) ---------------------------------
+
+class HekitError(Exception):
+    code = -1
+
+
+class InvalidParams(HekitError):
+    code = 1
+
+
+class ScaleMismatch(HekitError):
+    code = 2
+
+
+class LevelMismatch(HekitError):
+    code = 3
+
+
+class NoLevelsLeft(HekitError):
+    code = 4
+
+
+class Decode(HekitError):
+    code = 5
+
+
+class Device(HekitError):
+    code = 6
+
+
+class OutOfMemory(Device):
+    code = 7
+
+
+class Timeout(Device):
+    code = 8
+
+
+_ERRORS = {c.code: c for c in (InvalidParams, ScaleMismatch, LevelMismatch, NoLevelsLeft, Decode, Device,
+                               OutOfMemory, Timeout)}
+
+_lib = None
+
+
+def build():
+    """Compiles libckg.so for sm_100a (nvcc, in-tree)."""
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(_HERE, "csrc")], check=True)
+
+
+def lib():
+    """The loaded C ABI. Raises if libckg.so has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with ckks_train_b200.build() (no CPU fallback)")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    L.ckg_last_error.restype = C.c_char_p
+    L.ckg_abi_version.restype = C.c_uint32
+    L.ckg_launch_count.restype = C.c_uint64
+    L.ckg_primes_for_bits.argtypes = [C.c_uint32, U32P, C.c_uint32, U32P, C.c_uint32, U64P, U64P]
+    L.ckg_ctx_create.argtypes = [C.c_uint32, U64P, C.c_uint32, U64P, C.c_uint32, C.c_uint32, C.c_int, VP,
+                                 C.POINTER(VP)]
+    L.ckg_ctx_destroy.argtypes = [VP]
+    L.ckg_ctx_sync.argtypes = [VP]
+    L.ckg_ctx_stream.argtypes = [VP]
+    L.ckg_ctx_stream.restype = VP
+    L.ckg_ntt.argtypes = [VP, VP, VP, U32P, C.c_uint32, C.c_int]
+    L.ckg_poly_binary.argtypes = [VP, C.c_int, VP, VP, VP, C.c_uint32, C.c_uint32]
+    L.ckg_poly_negate.argtypes = [VP, VP, VP, C.c_uint32, C.c_uint32]
+    L.ckg_poly_mul_scalar.argtypes = [VP, VP, C.c_uint64, VP, C.c_uint32, C.c_uint32]
+    L.ckg_automorphism.argtypes = [VP, VP, VP, C.c_uint32, C.c_uint64]
+    L.ckg_rescale.argtypes = [VP, VP, C.c_uint32, VP]
+    L.ckg_mod_up.argtypes = [VP, VP, C.c_uint32, C.c_uint32, VP, VP]
+    L.ckg_mod_down.argtypes = [VP, VP, C.c_uint32, VP, VP]
+    L.ckg_key_upload.argtypes = [VP, U64P, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(VP)]
+    L.ckg_key_upload_device.argtypes = [VP, VP, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(VP)]
+    L.ckg_key_free.argtypes = [VP]
+    L.ckg_key_bytes.argtypes = [VP]
+    L.ckg_key_bytes.restype = C.c_uint64
+    L.ckg_key_switch.argtypes = [VP, VP, VP, C.c_uint32, VP, VP]
+    L.ckg_eval_create.argtypes = [VP, VP, C.POINTER(VP), C.c_uint32, C.c_uint32, C.POINTER(VP)]
+    L.ckg_eval_destroy.argtypes = [VP]
+    L.ckg_eval_fork.argtypes = [VP, C.POINTER(VP)]
+    L.ckg_eval_config.argtypes = [VP]
+    L.ckg_eval_config.restype = C.c_uint32
+    L.ckg_eval_counter.argtypes = [VP, U64P]
+    L.ckg_eval_reset_counter.argtypes = [VP]
+    L.ckg_eval_add_counts.argtypes = [VP, U64P]
+    L.ckg_eval_has_relin_key.argtypes = [VP]
+    L.ckg_eval_has_galois_key.argtypes = [VP, C.c_int32]
+    L.ckg_ct_upload.argtypes = [VP, U64P, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_ct_upload_device.argtypes = [VP, VP, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_ct_download.argtypes = [VP, U64P]
+    L.ckg_ct_download_device.argtypes = [VP, VP]
+    L.ckg_ct_info.argtypes = [VP, U32P, U32P, C.POINTER(C.c_double)]
+    L.ckg_ct_clone.argtypes = [VP]
+    L.ckg_ct_clone.restype = VP
+    L.ckg_ct_free.argtypes = [VP]
+    L.ckg_eval_owns.argtypes = [VP, VP]
+    L.ckg_pt_upload.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_pt_upload_device.argtypes = [VP, VP, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_pt_clone.argtypes = [VP]
+    L.ckg_pt_clone.restype = VP
+    L.ckg_pt_free.argtypes = [VP]
+    for name in ("ckg_add", "ckg_sub", "ckg_mul_no_relin", "ckg_mul"):
+        getattr(L, name).argtypes = [VP, VP, VP, C.POINTER(VP)]
+    for name in ("ckg_negate", "ckg_relinearize", "ckg_rescale_ct", "ckg_conjugate"):
+        getattr(L, name).argtypes = [VP, VP, C.POINTER(VP)]
+    L.ckg_add_plain.argtypes = [VP, VP, VP, C.POINTER(VP)]
+    L.ckg_mul_plain.argtypes = [VP, VP, VP, C.POINTER(VP)]
+    L.ckg_mul_scalar.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
+    L.ckg_mul_plain_to_scale.argtypes = [VP, VP, VP, C.c_double, C.POINTER(VP)]
+    L.ckg_mod_switch_to_level.argtypes = [VP, VP, C.c_uint32, C.POINTER(VP)]
+    L.ckg_relabel.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
+    L.ckg_rotate.argtypes = [VP, VP, C.c_int32, C.POINTER(VP)]
+    L.ckg_hoisted_rotate.argtypes = [VP, VP, I32P, C.c_uint32, C.POINTER(VP)]
+    L.ckg_exact_product_scale.argtypes = [VP, C.c_uint32, C.c_double, C.POINTER(C.c_double)]
+    L.ckg_matvec_plain.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
+    L.ckg_matvec_enc.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
+
+
+def _check(code):
+    if code != 0:
+        msg = lib().ckg_last_error().decode()
+        raise _ERRORS.get(code, Device)(msg)
+
+
+def _p64(a):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"], "expected a C-contiguous uint64 array"
+    return a.ctypes.data_as(U64P)
+
+
+def launch_count():
+    """Kernel launches issued by libckg.so so far."""
+    return lib().ckg_launch_count()
+
+
+def primes_for_bits(log_n, q_bits, p_bits):
+    """The data and special primes CkksParams::new hands out (params.rs:87-157)."""
+    qb = (C.c_uint32 * len(q_bits))(*q_bits)
+    pb = (C.c_uint32 * len(p_bits))(*p_bits)
+    q = np.zeros(len(q_bits), np.uint64)
+    p = np.zeros(len(p_bits), np.uint64)
+    _check(lib().ckg_primes_for_bits(log_n, qb, len(q_bits), pb, len(p_bits), _p64(q), _p64(p)))
+    return [int(x) for x in q], [int(x) for x in p]
+
+
+class Context:
+    """Parameters resident on one GPU: primes, NTT and base-conversion tables, a stream."""
+
+    def __init__(self, log_n, q, p, dnum, device=0, stream=None, scale=None):
+        self.log_n, self.n = log_n, 1 << log_n
+        self.q, self.p, self.dnum = [int(x) for x in q], [int(x) for x in p], dnum
+        self.alpha = len(self.q) // dnum
+        self.max_level = len(self.q) - 1
+        self.k = len(self.p)
+        self.scale = scale
+        qa, pa = np.asarray(self.q, np.uint64), np.asarray(self.p, np.uint64)
+        h = VP()
+        _check(lib().ckg_ctx_create(log_n, _p64(qa), len(qa), _p64(pa), len(pa), dnum, device,
+                                    VP(stream) if stream else None, C.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_bits(cls, log_n, q_bits, p_bits, dnum, device=0, stream=None, scale_bits=None):
+        q, p = primes_for_bits(log_n, q_bits, p_bits)
+        return cls(log_n, q, p, dnum, device, stream, None if scale_bits is None else float(2.0 ** scale_bits))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_ctx_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    @property
+    def primes(self):
+        return self.q + self.p
+
+    @property
+    def stream(self):
+        return lib().ckg_ctx_stream(self.h)
+
+    def sync(self):
+        _check(lib().ckg_ctx_sync(self.h))
+
+    def digit_ranges(self, level):
+        """keyswitch::digit_ranges (crates/ckks-train-ckks/src/keyswitch.rs:68-74)."""
+        out = []
+        for j in range(self.dnum):
+            s, e = j * self.alpha, min((j + 1) * self.alpha, level + 1)
+            if s > level:
+                break
+            out.append((s, e))
+        return out
+
+    # -- device-buffer primitives (integer device addresses) --
+    def ntt(self, src, dst, primes, inverse=False):
+        pr = (C.c_uint32 * len(primes))(*primes)
+        _check(lib().ckg_ntt(self.h, VP(src), VP(dst), pr, len(primes), int(inverse)))
+
+    def poly_binary(self, op, a, b, out, first_prime, nlimbs):
+        _check(lib().ckg_poly_binary(self.h, op, VP(a), VP(b), VP(out), first_prime, nlimbs))
+
+    def poly_negate(self, a, out, first_prime, nlimbs):
+        _check(lib().ckg_poly_negate(self.h, VP(a), VP(out), first_prime, nlimbs))
+
+    def poly_mul_scalar(self, a, scalar, out, first_prime, nlimbs):
+        _check(lib().ckg_poly_mul_scalar(self.h, VP(a), scalar, VP(out), first_prime, nlimbs))
+
+    def automorphism(self, src, dst, nlimbs, galois_elt):
+        _check(lib().ckg_automorphism(self.h, VP(src), VP(dst), nlimbs, galois_elt))
+
+    def rescale(self, src, level, dst):
+        _check(lib().ckg_rescale(self.h, VP(src), level, VP(dst)))
+
+    def mod_up(self, src, level, digit, out_q, out_p):
+        _check(lib().ckg_mod_up(self.h, VP(src), level, digit, VP(out_q), VP(out_p)))
+
+    def mod_down(self, q_part, level, p_part, out):
+        _check(lib().ckg_mod_down(self.h, VP(q_part), level, VP(p_part), VP(out)))
+
+    def upload_key(self, key, galois_elt=0):
+        """key: uint64 array (parts, 2, q_limbs + k, N) in the reference device layout."""
+        return Key(self, key, galois_elt)
+
+    def upload_key_device(self, ptr, shape, galois_elt=0):
+        """The same from a device buffer of that shape."""
+        return Key(self, None, galois_elt, device_ptr=ptr, shape=shape)
+
+    def key_switch(self, key, src, level, out_b, out_a):
+        _check(lib().ckg_key_switch(self.h, key.h, VP(src), level, VP(out_b), VP(out_a)))
+
+
+class Key:
+    """A key-switching key resident in HBM (relinearization key when galois_elt is 0)."""
+
+    def __init__(self, ctx, arr, galois_elt=0, device_ptr=None, shape=None):
+        self.ctx, self.elt = ctx, galois_elt
+        h = VP()
+        if device_ptr is not None:
+            parts, two, limbs, n = shape
+            assert two == 2 and n == ctx.n and limbs > ctx.k
+            _check(lib().ckg_key_upload_device(ctx.h, VP(device_ptr), parts, limbs - ctx.k, galois_elt, C.byref(h)))
+        else:
+            arr = np.ascontiguousarray(arr, np.uint64)
+            parts, two, limbs, n = arr.shape
+            assert two == 2 and n == ctx.n and limbs > ctx.k
+            _check(lib().ckg_key_upload(ctx.h, _p64(arr), parts, limbs - ctx.k, galois_elt, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_key_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    @property
+    def nbytes(self):
+        return lib().ckg_key_bytes(self.h)
+
+
+class EvalConfig:
+    """The ablation flags (crates/ckks-train-ckks/src/ops.rs:111-178)."""
+
+    def __init__(self, hoist=True, bsgs=True, lazy_relin=True):
+        self.hoist, self.bsgs, self.lazy_relin = hoist, bsgs, lazy_relin
+
+    @property
+    def flags(self):
+        return (HOIST if self.hoist else 0) | (BSGS if self.bsgs else 0) | (LAZY_RELIN if self.lazy_relin else 0)
+
+    @classmethod
+    def from_flags(cls, f):
+        return cls(bool(f & HOIST), bool(f & BSGS), bool(f & LAZY_RELIN))
+
+    def __eq__(self, o):
+        return self.flags == o.flags
+
+    def __repr__(self):
+        return f"EvalConfig(hoist={self.hoist}, bsgs={self.bsgs}, lazy_relin={self.lazy_relin})"
+
+
+COUNTER_FIELDS = ("rotations", "relins", "ct_ct_tensor", "ct_pt_mults", "rescales", "sse_switches", "bootstraps")
+
+
+class Ciphertext:
+    """A device ciphertext handle. Copies share the device buffer (no allocation)."""
+
+    def __init__(self, ev, h):
+        self.ev, self.h = ev, h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_ct_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def info(self):
+        n, l, s = C.c_uint32(), C.c_uint32(), C.c_double()
+        lib().ckg_ct_info(self.h, C.byref(n), C.byref(l), C.byref(s))
+        return n.value, l.value, s.value
+
+    def size(self):
+        return self.info()[0]
+
+    def level(self):
+        return self.info()[1]
+
+    def scale(self):
+        return self.info()[2]
+
+    def slots(self):
+        return self.ev.ctx.n // 2
+
+    def clone(self):
+        return Ciphertext(self.ev, VP(lib().ckg_ct_clone(self.h)))
+
+    __copy__ = clone
+
+
+class Plaintext:
+    def __init__(self, ev, h, level, scale):
+        self.ev, self.h, self._level, self._scale = ev, h, level, scale
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_pt_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def level(self):
+        return self._level
+
+    def scale(self):
+        return self._scale
+
+    def slots(self):
+        return self.ev.ctx.n // 2
+
+
+class CudaEvaluator:
+    """HeOps on the GPU (crates/ckks-train-ckks/src/ops.rs:198-356)."""
+
+    def __init__(self, ctx, relin_key=None, galois_keys=(), config=None, _handle=None):
+        self.ctx = ctx
+        self._keys = (relin_key, tuple(galois_keys))
+        if _handle is not None:
+            self.h = _handle
+            return
+        config = config or EvalConfig()
+        gal = list(galois_keys)
+        arr = (VP * max(len(gal), 1))(*[k.h for k in gal])
+        h = VP()
+        _check(lib().ckg_eval_create(ctx.h, relin_key.h if relin_key else None, arr, len(gal), config.flags,
+                                     C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_eval_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    # -- bookkeeping --
+    def params(self):
+        return self.ctx
+
+    def config(self):
+        return EvalConfig.from_flags(lib().ckg_eval_config(self.h))
+
+    def counter(self):
+        out = np.zeros(7, np.uint64)
+        lib().ckg_eval_counter(self.h, _p64(out))
+        return dict(zip(COUNTER_FIELDS, (int(x) for x in out)))
+
+    def key_switches(self):
+        """OpCounter::key_switches (counter.rs:76-78)."""
+        c = self.counter()
+        return c["rotations"] + c["relins"] + c["sse_switches"]
+
+    def reset_counter(self):
+        lib().ckg_eval_reset_counter(self.h)
+
+    def add_counts(self, counts):
+        arr = np.asarray([counts.get(f, 0) for f in COUNTER_FIELDS], np.uint64)
+        lib().ckg_eval_add_counts(self.h, _p64(arr))
+
+    def fork(self):
+        h = VP()
+        _check(lib().ckg_eval_fork(self.h, C.byref(h)))
+        return CudaEvaluator(self.ctx, *self._keys, _handle=h)
+
+    def has_relin_key(self):
+        return bool(lib().ckg_eval_has_relin_key(self.h))
+
+    def has_galois_key(self, step):
+        return bool(lib().ckg_eval_has_galois_key(self.h, step))
+
+    def owns(self, ct):
+        return bool(lib().ckg_eval_owns(self.h, ct.h))
+
+    # -- transfers --
+    def upload_ct(self, data, scale):
+        """data: uint64 (ncomp, level+1, N), NTT form, reduced."""
+        d = np.ascontiguousarray(data, np.uint64)
+        h = VP()
+        _check(lib().ckg_ct_upload(self.h, _p64(d), d.shape[0], d.shape[1] - 1, scale, C.byref(h)))
+        return Ciphertext(self, h)
+
+    upload_ct_owned = upload_ct
+
+    def upload_ct_device(self, ptr, ncomp, level, scale):
+        h = VP()
+        _check(lib().ckg_ct_upload_device(self.h, VP(ptr), ncomp, level, scale, C.byref(h)))
+        return Ciphertext(self, h)
+
+    def download_ct(self, ct):
+        n, l, s = ct.info()
+        out = np.zeros((n, l + 1, self.ctx.n), np.uint64)
+        _check(lib().ckg_ct_download(ct.h, _p64(out)))
+        return out, s
+
+    def download_ct_device(self, ct, ptr):
+        _check(lib().ckg_ct_download_device(ct.h, VP(ptr)))
+
+    def upload_pt(self, data, scale):
+        d = np.ascontiguousarray(data, np.uint64)
+        h = VP()
+        _check(lib().ckg_pt_upload(self.h, _p64(d), d.shape[0] - 1, scale, C.byref(h)))
+        return Plaintext(self, h, d.shape[0] - 1, scale)
+
+    upload_pt_owned = upload_pt
+
+    def upload_pt_device(self, ptr, level, scale):
+        h = VP()
+        _check(lib().ckg_pt_upload_device(self.h, VP(ptr), level, scale, C.byref(h)))
+        return Plaintext(self, h, level, scale)
+
+    # -- arithmetic --
+    def _ct(self, fn, *args):
+        h = VP()
+        _check(fn(self.h, *args, C.byref(h)))
+        return Ciphertext(self, h)
+
+    def add(self, a, b):
+        return self._ct(lib().ckg_add, a.h, b.h)
+
+    def sub(self, a, b):
+        return self._ct(lib().ckg_sub, a.h, b.h)
+
+    def negate(self, a):
+        return self._ct(lib().ckg_negate, a.h)
+
+    def add_plain(self, a, p):
+        return self._ct(lib().ckg_add_plain, a.h, p.h)
+
+    def mul_plain(self, a, p):
+        return self._ct(lib().ckg_mul_plain, a.h, p.h)
+
+    def mul_scalar(self, ct, value, target_scale):
+        return self._ct(lib().ckg_mul_scalar, ct.h, value, target_scale)
+
+    def mul_plain_to_scale(self, a, p, target_scale):
+        return self._ct(lib().ckg_mul_plain_to_scale, a.h, p.h, target_scale)
+
+    def mul_no_relin(self, a, b):
+        return self._ct(lib().ckg_mul_no_relin, a.h, b.h)
+
+    def relinearize(self, ct):
+        return self._ct(lib().ckg_relinearize, ct.h)
+
+    def mul(self, a, b):
+        return self._ct(lib().ckg_mul, a.h, b.h)
+
+    def rescale(self, ct):
+        return self._ct(lib().ckg_rescale_ct, ct.h)
+
+    def mod_switch_to_level(self, ct, level):
+        return self._ct(lib().ckg_mod_switch_to_level, ct.h, level)
+
+    def relabel(self, ct, scale):
+        return self._ct(lib().ckg_relabel, ct.h, scale)
+
+    def rotate(self, ct, steps):
+        return self._ct(lib().ckg_rotate, ct.h, steps)
+
+    def conjugate(self, ct):
+        return self._ct(lib().ckg_conjugate, ct.h)
+
+    def hoisted_rotate(self, ct, steps):
+        st = (C.c_int32 * max(len(steps), 1))(*steps)
+        outs = (VP * max(len(steps), 1))()
+        _check(lib().ckg_hoisted_rotate(self.h, ct.h, st, len(steps), outs))
+        return [Ciphertext(self, VP(outs[i])) for i in range(len(steps))]
+
+    def matvec_plain(self, d, stride, entries, x):
+        arr = (VP * len(entries))(*[e.h for e in entries])
+        return self._ct(lib().ckg_matvec_plain, d, stride, arr, x.h)
+
+    def matvec_enc(self, d, stride, entries, x):
+        arr = (VP * len(entries))(*[e.h for e in entries])
+        return self._ct(lib().ckg_matvec_enc, d, stride, arr, x.h)
+
+    def exact_product_scale(self, level, target_scale):
+        out = C.c_double()
+        _check(lib().ckg_exact_product_scale(self.h, level, target_scale, C.byref(out)))
+        return out.value
+
+    def target_plain_scale(self, ct, target_scale):
+        """HeOps::target_plain_scale (ops.rs:334-338)."""
+        sp = self.exact_product_scale(ct.level(), target_scale) / ct.scale()
+        if sp < 1048576.0:
+            raise InvalidParams("plaintext scale is below 2^20")
+        return sp
+
+    def mul_lazy(self, a, b):
+        """HeOps::mul_lazy (ops.rs:340-347)."""
+        return self.mul_no_relin(a, b) if self.config().lazy_relin else self.mul(a, b)
+
+    def relin_lazy(self, s):
+        """HeOps::relin_lazy (ops.rs:349-355)."""
+        return self.relinearize(s) if self.config().lazy_relin else s

@@ -1,0 +1,191 @@
+/*
+ * ckg.h -- C ABI of the B200-native RNS-CKKS evaluator path (libckg.so, sm_100a).
+ *
+ * A drop-in for the device backend behind the `HeOps` evaluator interface of
+ * kenmaro3/ckks-train (crates/ckks-train-ckks/src/ops.rs:198-356), i.e. for what
+ * `CudaEvaluator` (crates/ckks-train-cuda/src/evaluator.rs:123, 522) and its launch
+ * sequences (crates/ckks-train-cuda/src/ks.rs:270-470, basis.rs:455-514) do today.
+ *
+ * Conventions
+ *  - Every function returns CKG_OK (0) or one of the CKG_* status codes, mirroring
+ *    HekitError (crates/ckks-train-core/src/error.rs:7-21) plus OOM and TIMEOUT;
+ *    ckg_last_error() returns the calling thread's message for the last failure.
+ *    Nothing aborts or panics across this boundary.
+ *  - Polynomials are limb-major u64 arrays: limb i (residues modulo prime i) occupies
+ *    words [i*N, (i+1)*N). A ciphertext is its components one after another.
+ *  - Prime indices are global: 0..L are the data primes q_0..q_L, L+1..L+k the special
+ *    primes p_0..p_{k-1} (CkksParams::q() and ::p(), crates/ckks-train-ckks/src/params.rs).
+ *  - "Device" pointers are CUDA device addresses on the context's device; "host"
+ *    pointers are ordinary (pageable or pinned) memory. All work is queued on the
+ *    context's stream; ckg_ctx_sync() waits for it. Downloads synchronise.
+ *  - Results are bit-identical to the reference's CPU path (crates/ckks-train-core,
+ *    crates/ckks-train-ckks) on the same inputs.
+ */
+#ifndef CKG_H
+#define CKG_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CKG_API __attribute__((visibility("default")))
+#else
+#define CKG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ckg_ctx ckg_ctx;   /* parameters + device tables + stream (CudaDevice, device.rs:290-384) */
+typedef struct ckg_key ckg_key;   /* device-resident key-switching key (DeviceKsk, keyswitch.rs:53-216) */
+typedef struct ckg_eval ckg_eval; /* evaluator: keys, EvalConfig, OpCounter (CudaEvaluator) */
+typedef struct ckg_ct ckg_ct;     /* ciphertext handle; clones share the device buffer (ciphertext.rs) */
+typedef struct ckg_pt ckg_pt;     /* plaintext handle (NTT form) */
+
+enum {
+  CKG_OK = 0,
+  CKG_INVALID_PARAMS = 1,   /* HekitError::InvalidParams */
+  CKG_SCALE_MISMATCH = 2,   /* HekitError::ScaleMismatch */
+  CKG_LEVEL_MISMATCH = 3,   /* HekitError::LevelMismatch */
+  CKG_NO_LEVELS_LEFT = 4,   /* HekitError::NoLevelsLeft */
+  CKG_DECODE = 5,           /* HekitError::Decode */
+  CKG_DEVICE = 6,           /* HekitError::Device */
+  CKG_OOM = 7,              /* HekitError::Device (out of device memory) */
+  CKG_TIMEOUT = 8           /* HekitError::Device (a bounded wait gave up) */
+};
+
+/* EvalConfig flags (crates/ckks-train-ckks/src/ops.rs:111-178). */
+enum { CKG_HOIST = 1, CKG_BSGS = 2, CKG_LAZY_RELIN = 4, CKG_OPTIMIZED = 7 };
+
+CKG_API const char* ckg_last_error(void);
+CKG_API uint32_t ckg_abi_version(void);
+/* Number of kernel launches this library has issued since it was loaded. */
+CKG_API uint64_t ckg_launch_count(void);
+
+/* ---- parameters and context -------------------------------------------------------- */
+
+/* SEAL-style prime hand-out of CkksParams::new (crates/ckks-train-ckks/src/params.rs:87-157):
+ * fills q_out[nq] and p_out[np]. */
+CKG_API int ckg_primes_for_bits(uint32_t log_n, const uint32_t* q_bits, uint32_t nq, const uint32_t* p_bits, uint32_t np,
+                        uint64_t* q_out, uint64_t* p_out);
+
+/* CudaDevice::new (crates/ckks-train-cuda/src/device.rs:290-384): uploads the NTT and
+ * base-conversion tables for the primes q[0..nq), p[0..np) of ring degree 2^log_n with
+ * `dnum` key-switching digits. `stream` is a cudaStream_t to use, or NULL for an own one. */
+CKG_API int ckg_ctx_create(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* p, uint32_t np, uint32_t dnum,
+                   int device, void* stream, ckg_ctx** out);
+CKG_API void ckg_ctx_destroy(ckg_ctx* ctx);
+CKG_API int ckg_ctx_sync(ckg_ctx* ctx);
+CKG_API void* ckg_ctx_stream(ckg_ctx* ctx);
+
+/* ---- device-buffer primitives (device pointers) ------------------------------------ */
+
+/* NttTable::forward / ::inverse on every limb (crates/ckks-train-core/src/ntt.rs:141-232);
+ * limb i of src/dst uses global prime primes[i]. src may equal dst. */
+CKG_API int ckg_ntt(ckg_ctx* ctx, const uint64_t* src, uint64_t* dst, const uint32_t* primes, uint32_t nlimbs, int inverse);
+
+/* RnsPoly add/sub/mul_assign (poly.rs:131-182): op 0 add, 1 sub, 2 pointwise product. */
+CKG_API int ckg_poly_binary(ckg_ctx* ctx, int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint32_t first_prime,
+                    uint32_t nlimbs);
+/* RnsPoly::neg and ::mul_scalar_assign (poly.rs:157-190). */
+CKG_API int ckg_poly_negate(ckg_ctx* ctx, const uint64_t* a, uint64_t* out, uint32_t first_prime, uint32_t nlimbs);
+CKG_API int ckg_poly_mul_scalar(ckg_ctx* ctx, const uint64_t* a, uint64_t scalar, uint64_t* out, uint32_t first_prime,
+                        uint32_t nlimbs);
+/* RnsPoly::automorphism in NTT form (poly.rs:242-262, rns.rs:137-175). out must not alias in. */
+CKG_API int ckg_automorphism(ckg_ctx* ctx, const uint64_t* in, uint64_t* out, uint32_t nlimbs, uint64_t galois_elt);
+/* RnsPoly::rescale_by_last in NTT form (crates/ckks-train-core/src/baseconv.rs:258-291):
+ * in has level+1 limbs, out receives level limbs. */
+CKG_API int ckg_rescale(ckg_ctx* ctx, const uint64_t* in, uint32_t level, uint64_t* out);
+/* The exact centered lift of digit `digit` of a level-`level` NTT-form polynomial to
+ * Q_level * P (keyswitch.rs:140-202): out_q gets level+1 limbs, out_p the k special limbs. */
+CKG_API int ckg_mod_up(ckg_ctx* ctx, const uint64_t* in, uint32_t level, uint32_t digit, uint64_t* out_q, uint64_t* out_p);
+/* RnsPoly::mod_down (baseconv.rs:459-511), NTT form: (q_part, p_part) over Q_level * P
+ * divided by P with rounding -> out (level+1 limbs). */
+CKG_API int ckg_mod_down(ckg_ctx* ctx, const uint64_t* q_part, uint32_t level, const uint64_t* p_part, uint64_t* out);
+
+/* Key upload (DeviceKsk, crates/ckks-train-cuda/src/keyswitch.rs:110-216). host_key holds
+ * `parts` parts, each b_j then a_j, each q_limbs data limbs then the k special limbs (NTT
+ * form); galois_elt is 0 for a relinearization key. One device allocation per key. */
+CKG_API int ckg_key_upload(ckg_ctx* ctx, const uint64_t* host_key, uint32_t parts, uint32_t q_limbs, uint64_t galois_elt,
+                   ckg_key** out);
+/* The same from a device buffer in that layout (copied). */
+CKG_API int ckg_key_upload_device(ckg_ctx* ctx, const uint64_t* dev_key, uint32_t parts, uint32_t q_limbs,
+                                  uint64_t galois_elt, ckg_key** out);
+CKG_API void ckg_key_free(ckg_key* key);
+CKG_API uint64_t ckg_key_bytes(const ckg_key* key);
+
+/* keyswitch::key_switch (crates/ckks-train-ckks/src/keyswitch.rs:317-319): in is NTT form
+ * at `level`; out_b, out_a receive level+1 limbs each. */
+CKG_API int ckg_key_switch(ckg_ctx* ctx, const ckg_key* key, const uint64_t* in, uint32_t level, uint64_t* out_b,
+                   uint64_t* out_a);
+
+/* ---- evaluator (HeOps, crates/ckks-train-ckks/src/ops.rs:198-356) ------------------- */
+
+/* Evaluator::with_config (evaluator.rs:193-206): relin may be NULL; galois[0..ngal) are
+ * Galois keys (their elements set at upload); flags = CKG_* EvalConfig bits. */
+CKG_API int ckg_eval_create(ckg_ctx* ctx, const ckg_key* relin, const ckg_key* const* galois, uint32_t ngal, uint32_t flags,
+                    ckg_eval** out);
+CKG_API void ckg_eval_destroy(ckg_eval* ev);
+/* HeOps::fork: same keys and flags, counter at zero. */
+CKG_API int ckg_eval_fork(const ckg_eval* ev, ckg_eval** out);
+CKG_API uint32_t ckg_eval_config(const ckg_eval* ev);
+/* OpCounter (crates/ckks-train-ckks/src/counter.rs:42-58) as 7 words: rotations, relins,
+ * ct_ct_tensor, ct_pt_mults, rescales, sse_switches, bootstraps. */
+CKG_API void ckg_eval_counter(const ckg_eval* ev, uint64_t out[7]);
+CKG_API void ckg_eval_reset_counter(ckg_eval* ev);
+CKG_API void ckg_eval_add_counts(ckg_eval* ev, const uint64_t counts[7]);
+CKG_API int ckg_eval_has_relin_key(const ckg_eval* ev);
+CKG_API int ckg_eval_has_galois_key(const ckg_eval* ev, int32_t step);
+
+/* upload_ct / download_ct (ops.rs:241-257): host buffer of ncomp * (level+1) * N words. */
+CKG_API int ckg_ct_upload(ckg_eval* ev, const uint64_t* host, uint32_t ncomp, uint32_t level, double scale, ckg_ct** out);
+/* The same from a device buffer (copied). */
+CKG_API int ckg_ct_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t ncomp, uint32_t level, double scale,
+                         ckg_ct** out);
+CKG_API int ckg_ct_download(const ckg_ct* ct, uint64_t* host);
+/* Copy of the ciphertext into a device buffer (ncomp * (level+1) * N words), queued. */
+CKG_API int ckg_ct_download_device(const ckg_ct* ct, uint64_t* dev);
+CKG_API void ckg_ct_info(const ckg_ct* ct, uint32_t* ncomp, uint32_t* level, double* scale);
+/* Clone shares the device buffer: no allocation, cannot fail (ops.rs:17-20). */
+CKG_API ckg_ct* ckg_ct_clone(const ckg_ct* ct);
+CKG_API void ckg_ct_free(ckg_ct* ct);
+CKG_API int ckg_eval_owns(const ckg_eval* ev, const ckg_ct* ct);
+
+CKG_API int ckg_pt_upload(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
+CKG_API int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, double scale, ckg_pt** out);
+CKG_API ckg_pt* ckg_pt_clone(const ckg_pt* pt);
+CKG_API void ckg_pt_free(ckg_pt* pt);
+
+/* Ciphertext arithmetic; each has the checks, errors, scale labels and counts of the
+ * Evaluator method of the same name (crates/ckks-train-ckks/src/evaluator.rs). */
+CKG_API int ckg_add(ckg_eval* ev, const ckg_ct* a, const ckg_ct* b, ckg_ct** out);                  /* :232 */
+CKG_API int ckg_sub(ckg_eval* ev, const ckg_ct* a, const ckg_ct* b, ckg_ct** out);                  /* :237 */
+CKG_API int ckg_negate(ckg_eval* ev, const ckg_ct* a, ckg_ct** out);                                /* :242 */
+CKG_API int ckg_add_plain(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, ckg_ct** out);            /* :251 */
+CKG_API int ckg_mul_plain(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, ckg_ct** out);            /* :262 */
+CKG_API int ckg_mul_scalar(ckg_eval* ev, const ckg_ct* a, double value, double target_scale, ckg_ct** out); /* :361 */
+CKG_API int ckg_mul_plain_to_scale(ckg_eval* ev, const ckg_ct* a, const ckg_pt* p, double target_scale,
+                           ckg_ct** out);                                                   /* :393 */
+CKG_API int ckg_mul_no_relin(ckg_eval* ev, const ckg_ct* a, const ckg_ct* b, ckg_ct** out);         /* :422 */
+CKG_API int ckg_relinearize(ckg_eval* ev, const ckg_ct* a, ckg_ct** out);                           /* :441 */
+CKG_API int ckg_mul(ckg_eval* ev, const ckg_ct* a, const ckg_ct* b, ckg_ct** out);                  /* :463 */
+CKG_API int ckg_rescale_ct(ckg_eval* ev, const ckg_ct* a, ckg_ct** out);                            /* :498 */
+CKG_API int ckg_mod_switch_to_level(ckg_eval* ev, const ckg_ct* a, uint32_t level, ckg_ct** out);   /* :513 */
+CKG_API int ckg_relabel(ckg_eval* ev, const ckg_ct* a, double scale, ckg_ct** out);                 /* ops.rs:302 */
+CKG_API int ckg_rotate(ckg_eval* ev, const ckg_ct* a, int32_t steps, ckg_ct** out);                 /* :534 */
+CKG_API int ckg_conjugate(ckg_eval* ev, const ckg_ct* a, ckg_ct** out);                             /* :547 */
+/* outs[0..nsteps) receive the rotations in step order (evaluator.rs:572-616). */
+CKG_API int ckg_hoisted_rotate(ckg_eval* ev, const ckg_ct* a, const int32_t* steps, uint32_t nsteps, ckg_ct** outs);
+CKG_API int ckg_exact_product_scale(const ckg_eval* ev, uint32_t level, double target_scale, double* out); /* :739 */
+/* W x for pre-rotated BSGS diagonals (crates/ckks-train-ckks/src/linalg.rs:608-680): d
+ * entries in entries[k1*baby + k2] order, `stride` lanes. */
+CKG_API int ckg_matvec_plain(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_pt* const* entries, const ckg_ct* x,
+                     ckg_ct** out);
+CKG_API int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* const* entries, const ckg_ct* x,
+                   ckg_ct** out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CKG_H */

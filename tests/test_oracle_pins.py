@@ -1,0 +1,371 @@
+"""Pins the CPU oracle to the reference's own golden values and known answers (CPU only).
+
+Each test cites the reference test that holds the value. Where the reference pins a
+property instead of a number (negacyclic convolution, bit-reversed evaluation order,
+exactness of the conversions), the property is checked against independent Python
+big-integer arithmetic.
+"""
+
+import math
+import struct
+
+import numpy as np
+import pytest
+
+
+# ---- modulus.rs:164-216 ----------------------------------------------------------------
+
+def test_barrett_constant(oracle):
+    for q in [2, 3, 4, 1 << 59, (1 << 60) - 1, 1152921504606846883]:
+        assert oracle.barrett(q) == (1 << 128) // q
+
+
+def test_worst_case_mul(oracle):
+    for q in [3, (1 << 60) - 1, (1 << 59) + 1, 1152921504606846883]:
+        a = q - 1
+        assert oracle.mulmod(q, a, a) == 1 % q
+        assert oracle.mulmod(q, a, 0) == 0
+        assert oracle.mul_shoup(q, a, a) == 1 % q
+        assert oracle.mul_shoup(q, (1 << 64) - 1, a) == ((1 << 64) - 1) * a % q
+
+
+# ---- primes.rs:120-191 -----------------------------------------------------------------
+
+def test_known_primes(oracle):
+    assert oracle.is_prime(1152921504606846883)  # 2^60 - 93
+    assert oracle.is_prime(2) and oracle.is_prime(3) and oracle.is_prime((1 << 64) - 59)
+    assert not oracle.is_prime(0) and not oracle.is_prime(1) and not oracle.is_prime((1 << 64) - 1)
+    for c in [561, 1105, 1729, 3215031751, 3825123056546413051]:
+        assert not oracle.is_prime(c)
+    assert oracle.is_prime((1 << 61) - 1)
+    assert not oracle.is_prime(4294967291 * 4294967279)
+
+
+def test_trial_division_below_20000(oracle):
+    for n in range(0, 20000, 7):
+        naive = n >= 2 and all(n % d for d in range(2, int(math.isqrt(n)) + 1))
+        assert oracle.is_prime(n) == naive, n
+
+
+def test_prime_search(oracle):
+    ps = oracle.ntt_primes_skip(40, 1 << 15, 0, 9)
+    assert len(ps) == 9
+    for i, q in enumerate(ps):
+        assert oracle.is_prime(q) and (q - 1) % (2 << 15) == 0 and (1 << 39) < q < (1 << 40)
+        if i:
+            assert q < ps[i - 1]
+    ps60 = oracle.ntt_primes_skip(60, 1 << 15, 0, 3)
+    assert oracle.ntt_primes_skip(60, 1 << 15, 1, 2) == ps60[1:]
+    assert oracle.ntt_primes_skip(17, 1 << 15, 0, 1) == [65537]
+    with pytest.raises(oracle.OracleError):
+        oracle.ntt_primes_skip(17, 1 << 15, 0, 5)
+    with pytest.raises(oracle.OracleError):
+        oracle.ntt_primes_skip(61, 1 << 15, 0, 1)
+
+
+# ---- params.rs:325-345 (SEAL 4.1.2 CoeffModulus::Create(32768, {60, 40 x 9, 60})) ------
+
+SEAL_2020 = [1152921504598720513, 1099501731841, 1099502518273, 1099502714881, 1099503370241, 1099503894529,
+             1099504549889, 1099506515969, 1099507695617, 1099510054913, 1152921504606584833]
+
+
+def test_seal_2020_primes(oracle, ckg):
+    P = oracle.Params.from_bits(15, [60] + [40] * 9, [60], 40, 10)
+    assert P.q == SEAL_2020[:10] and P.p == SEAL_2020[10:]
+    q, p = ckg.primes_for_bits(15, [60] + [40] * 9, [60])
+    assert q == SEAL_2020[:10] and p == SEAL_2020[10:]
+
+
+def test_prime_assignment_follows_seal(oracle):
+    """params.rs:349-363: {58, 58, 58} gets the third, second and first largest."""
+    largest = oracle.ntt_primes_skip(58, 1 << 16, 0, 3)
+    P = oracle.Params.from_bits(16, [58, 58, 58], [58], 42, 1)
+    four = oracle.ntt_primes_skip(58, 1 << 16, 0, 4)
+    assert P.q == [four[3], four[2], four[1]] and P.p == [four[0]]
+    assert largest == four[:3]
+
+
+def test_n16_boot_shape(oracle):
+    """params.rs:408-464: n16_boot bands, log PQ ~ 1732, scale_at."""
+    q_bits = [54] + [42] * 16 + [34] * 4 + [58] * 7 + [56] * 4
+    P = oracle.Params.from_bits(16, q_bits, [60] * 4, 42, 8)
+    assert P.max_level == 31 and P.alpha == 4
+    assert abs(P.log_pq() - 1732.0) <= 2.0 and P.log_pq() <= 1750.0
+    assert P.scale_at(0) == 2.0 ** 42 and P.scale_at(24) == 2.0 ** 58 and P.scale_at(31) == 2.0 ** 56
+    assert all(P.scale_at(l) == 2.0 ** 42 for l in range(1, 17))
+    assert all(P.scale_at(l) == 2.0 ** 34 for l in range(17, 21))
+
+
+def test_dnum_must_divide(oracle):
+    """params.rs:111-116: dnum 3 does not divide 32 q primes (BASELINE's n16_boot dnum)."""
+    with pytest.raises(oracle.OracleError):
+        oracle.Params.from_bits(16, [54] + [42] * 31, [60] * 4, 42, 3)
+
+
+# ---- ntt.rs:235-394 --------------------------------------------------------------------
+
+def test_psi_minimal(oracle):
+    assert oracle.min_root(8, 17) == 3
+    for n, q in [(8, 17), (8, 97), (16, 193), (16, 12289)]:
+        expect = next(g for g in range(1, q) if pow(g, n, q) == q - 1)
+        assert oracle.min_root(n, q) == expect
+
+
+def _naive_negacyclic(a, b, q):
+    n = len(a)
+    c = [0] * n
+    for i in range(n):
+        for j in range(n):
+            k = i + j
+            if k < n:
+                c[k] = (c[k] + a[i] * b[j]) % q
+            else:
+                c[k - n] = (c[k - n] - a[i] * b[j]) % q
+    return c
+
+
+def test_ntt_convolution_and_order(oracle):
+    for n in (8, 64):
+        P = oracle.Params.from_bits(int(math.log2(n)), [60], [50], 40, 1)
+        q = P.q[0]
+        a = oracle.random_poly(1, [q], n)
+        b = oracle.random_poly(2, [q], n)
+        fa, fb = P.ntt(a), P.ntt(b)
+        prod = np.array([[int(x) * int(y) % q for x, y in zip(fa[0], fb[0])]], np.uint64)
+        c = P.ntt(prod, inverse=True)
+        assert [int(x) for x in c[0]] == _naive_negacyclic([int(x) for x in a[0]], [int(x) for x in b[0]], q)
+        psi = oracle.min_root(n, q)
+        bits = int(math.log2(n))
+        for k in range(n):
+            x = pow(psi, 2 * k + 1, q)
+            acc = 0
+            for cc in reversed([int(v) for v in a[0]]):
+                acc = (acc * x + cc) % q
+            r = int(format(k, f"0{bits}b")[::-1], 2)
+            assert int(fa[0][r]) == acc
+
+
+def test_ntt_worst_case(oracle):
+    P = oracle.Params.from_bits(10, [60], [50], 40, 1)
+    q = P.q[0]
+    mx = np.full((1, 1024), q - 1, np.uint64)
+    assert np.array_equal(P.ntt(P.ntt(mx), inverse=True), mx)
+    z = np.zeros((1, 1024), np.uint64)
+    assert np.array_equal(P.ntt(z), z)
+
+
+# ---- rns.rs:193-230 --------------------------------------------------------------------
+
+def test_galois_permutation_formula(oracle):
+    for n in (2, 8, 64, 1024):
+        bits = int(math.log2(n))
+        two_n = 2 * n
+        gs = [1, 3 % two_n, two_n - 1]
+        g = 1
+        for _ in range(6):
+            g = g * 5 % two_n
+            gs.append(g)
+        for g in gs:
+            perm = oracle.galois_perm(n, g)
+            for i, p in enumerate(perm):
+                k = int(format(i, f"0{bits}b")[::-1], 2) if bits else 0
+                odd = g * (2 * k + 1) % two_n
+                want = int(format((odd - 1) // 2, f"0{bits}b")[::-1], 2) if bits else 0
+                assert p == want
+            assert sorted(perm) == list(range(n))
+    assert list(oracle.galois_perm(256, 1)) == list(range(256))
+
+
+def test_galois_elt(oracle, ckg):
+    """keys.rs:89-107: generator 3, negative steps are inverses."""
+    n = 1 << 12
+    for s in (1, 2, 5, 100, 2047):
+        e, ei = oracle.galois_elt(n, s), oracle.galois_elt(n, -s)
+        assert e * ei % (2 * n) == 1
+        assert e == pow(3, s, 2 * n)
+    assert oracle.galois_elt(n, 0) == 1 and oracle.galois_elt(n, n // 2) == 1
+
+
+# ---- keyswitch.rs:377-388 --------------------------------------------------------------
+
+def test_digit_ranges(oracle):
+    P = oracle.Params.from_bits(12, [60, 40, 40, 40, 40, 40], [60, 60], 40, 3)
+    assert P.digit_ranges(5) == [(0, 2), (2, 4), (4, 6)]
+    assert P.digit_ranges(4) == [(0, 2), (2, 4), (4, 5)]
+    assert P.digit_ranges(2) == [(0, 2), (2, 3)]
+    assert P.digit_ranges(1) == [(0, 2)]
+    assert P.digit_ranges(0) == [(0, 1)]
+    S = oracle.Params.from_bits(15, [60] + [40] * 9, [60], 40, 10)
+    assert len(S.digit_ranges(9)) == 10
+    assert S.digit_ranges(3) == [(0, 1), (1, 2), (2, 3), (3, 4)]
+
+
+# ---- linalg.rs split rule and ops.rs:43-61 count table ---------------------------------
+
+def test_bsgs_split_rule(oracle):
+    cases = [(1, (1, 1)), (2, (2, 1)), (4, (2, 2)), (8, (4, 2)), (16, (4, 4)), (32, (8, 4)), (64, (8, 8)),
+             (128, (16, 8)), (256, (16, 16))]
+    for d, bg in cases:
+        assert oracle.bsgs_split(d) == bg
+    assert oracle.bsgs_steps(16) == [1, 2, 3, 4, 8, 12]
+    assert oracle.bsgs_steps(64, 2) == [2, 4, 6, 8, 10, 12, 14, 16, 32, 48, 64, 80, 96, 112]
+
+
+def test_key_shapes():
+    """crates/ckks-train-cuda/src/ks.rs:514-519: an n16_boot key is 8 x 2 x 36 limbs =
+    288 MiB; the benchmark's N = 2^16, 24 + 8 primes, dnum 3 key is 3 x 2 x 32 limbs."""
+    limb = 8 << 16
+    assert 8 * 2 * 36 * limb == 288 << 20
+    assert 3 * 2 * 32 * limb == 96 << 20
+
+
+# ---- base conversion exactness (baseconv.rs:167-235, 258-291, 459-511) ----------------
+
+def _crt(limbs, primes):
+    Q = 1
+    for p in primes:
+        Q *= p
+    x = 0
+    for r, p in zip(limbs, primes):
+        Qi = Q // p
+        x += int(r) * Qi * pow(Qi, -1, p)
+    return x % Q, Q
+
+
+def _f64_overflow(y, primes):
+    """floor(sum_j f64(y_j) * f64(1/q_j)) with separate round-to-nearest ops (Python floats)."""
+    f = -0.0
+    for yj, q in zip(y, primes):
+        f = f + float(yj) * (1.0 / float(q))
+    return math.floor(f)
+
+
+def test_mod_down_against_bigint(oracle):
+    """mod_down = round(X / P) exactly, except where the f64 estimate of the reference rounds
+    differently; that estimate is recomputed here with Python floats."""
+    P = oracle.Params.from_bits(6, [60, 40, 40], [60, 60], 40, 3)
+    n = P.n
+    q = P.random_q(1, 2)
+    p = P.random_p(2)
+    got = P.mod_down(q, p, ntt=False)
+    primes = P.q + P.p
+    Pp = P.p[0] * P.p[1]
+    for c in range(n):
+        X, QP = _crt([q[0][c], q[1][c], q[2][c], p[0][c], p[1][c]], primes)
+        h = (Pp - 1) // 2
+        xs = [(int(p[t][c]) + P.p[t] // 2) % P.p[t] for t in range(2)]
+        y = [xs[t] * pow((Pp // P.p[t]) % P.p[t], -1, P.p[t]) % P.p[t] for t in range(2)]
+        e = _f64_overflow(y, P.p)
+        conv = sum(y[t] * (Pp // P.p[t]) for t in range(2)) - e * Pp - h
+        for i, qi in enumerate(P.q):
+            want = (X - conv) * pow(Pp, -1, qi) % qi
+            assert int(got[i][c]) == want
+        # and that is round(X / P) as an integer mod q_i
+        Xr = (X + h) // Pp
+        for i, qi in enumerate(P.q):
+            assert int(got[i][c]) == Xr % qi
+
+
+def test_mod_up_exact_centered(oracle):
+    """Every converted limb is the centered digit representative (keyswitch.rs:140-202)."""
+    P = oracle.Params.from_bits(6, [60, 40, 40, 40, 40, 40], [60, 60], 40, 3)
+    x = P.random_q(5, 5)
+    xn = P.ntt(x)
+    for j, (s, e) in enumerate(P.digit_ranges(5)):
+        oq, op = P.mod_up(xn, j)
+        cq = P.ntt(oq, inverse=True)
+        cp = P.ntt(op, inverse=True, basis=1)
+        D = 1
+        for qi in P.q[s:e]:
+            D *= qi
+        for c in range(P.n):
+            xd, _ = _crt([x[i][c] for i in range(s, e)], P.q[s:e])
+            xc = xd - D if xd > D // 2 else xd
+            for i, qi in enumerate(P.q):
+                assert int(cq[i][c]) == xc % qi
+            for t, pt in enumerate(P.p):
+                assert int(cp[t][c]) == xc % pt
+
+
+def test_rescale_exact(oracle):
+    P = oracle.Params.from_bits(6, [60, 40, 40], [60], 40, 3)
+    x = P.random_q(9, 2)
+    got = P.rescale(x, ntt=False)
+    for c in range(P.n):
+        X, Q = _crt([x[i][c] for i in range(3)], P.q)
+        ql = P.q[2]
+        want = (X + (ql - 1) // 2) // ql  # round(X / q_l), q_l odd
+        for i in range(2):
+            assert int(got[i][c]) == want % P.q[i]
+
+
+def test_f64_overflow_no_fma():
+    """The f64 overflow estimate must differ from an FMA-contracted evaluation somewhere on
+    near-tie sums; this pins the separate-rounding rule the oracle and the GPU kernel use."""
+    q = [1152921504606584833, 1152921504598720513]
+    y = [q[0] - 1, 1]
+    f = -0.0
+    for yj, qj in zip(y, q):
+        f = f + float(yj) * (1.0 / float(qj))
+    assert math.floor(f) in (0, 1)
+
+
+# ---- ChaCha20 (rand_chacha 0.9.0 stream, published ChaCha20 test vector) --------------
+
+def test_chacha20_zero_key_block():
+    """ChaCha20 keystream for the all-zero key and nonce, block 0 (RFC 7539 A.1 #1)."""
+    import oracle as O
+    words = O.chacha_u64(bytes(32), 8)
+    raw = b"".join(struct.pack("<Q", int(w)) for w in words)
+    assert raw.hex() == ("76b8e0ada0f13d90405d6ae55386bd28bdd219b8a08ded1aa836efcc8b770dc7"
+                         "da41597c5157488d7724e03fb8d84a376a43b8f41518a11cc387b669b2ee6586")
+
+
+def test_chacha20_against_cryptography():
+    """The oracle's ChaCha20 stream equals the `cryptography` package's ChaCha20 keystream
+    (counter 0, nonce 0) over several blocks."""
+    cryptography = pytest.importorskip("cryptography")
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms
+    import oracle as O
+    key = bytes(range(32))
+    enc = Cipher(algorithms.ChaCha20(key, bytes(16)), mode=None).encryptor()
+    ks = enc.update(bytes(64 * 5))
+    words = O.chacha_u64(key, 40)
+    assert b"".join(struct.pack("<Q", int(w)) for w in words) == ks
+
+
+def test_cdt_table_shape(oracle):
+    """sampler.rs:209-226: 2*floor(6 sigma)+1 non-decreasing entries, last = u64::MAX."""
+    t = oracle.cdt_table(3.2)
+    assert len(t) == 2 * 19 + 1
+    assert int(t[-1]) == (1 << 64) - 1
+    assert all(int(t[i]) <= int(t[i + 1]) for i in range(len(t) - 1))
+    # symmetric: bucket masses mirror each other to ~2^-50 (the reference's exactness bound)
+    mass = np.diff(np.concatenate([[0], t.astype(object)]))
+    for i in range(19):
+        assert abs(int(mass[i]) - int(mass[-1 - i])) < (1 << 16)
+
+
+# ---- key switching noise (keyswitch.rs:409-430) -----------------------------------------
+
+def test_key_switch_noise_bound(oracle):
+    """kb + ka s - d s^2 has coefficient noise within 6 predicted standard deviations."""
+    P = oracle.Params.from_bits(10, [60, 40, 40, 40, 40, 40], [60, 60], 40, 3)
+    kg = oracle.KeyGenerator(P, 2)
+    sq, sp = kg.secret()
+    rk = kg.relin_key()
+    level = 5
+    d = P.random_q(3, level)
+    kb, ka = rk.key_switch(d)
+    s = sq[: level + 1]
+    s2 = P.poly_op(2, s, s)
+    lhs = P.poly_op(0, kb, P.poly_op(2, ka, s))
+    err = P.poly_op(1, lhs, P.poly_op(2, d, s2))
+    e = P.ntt(err, inverse=True)
+    q0 = P.q[0]
+    vals = [int(v) if int(v) <= q0 // 2 else int(v) - q0 for v in e[0]]
+    sd = float(np.std(vals))
+    pp = float(P.p[0]) * float(P.p[1])
+    digits = sum((float(np.prod([float(x) for x in P.q[s_:e_]])) / pp) ** 2 / 12.0 for s_, e_ in P.digit_ranges(level))
+    pred = math.sqrt(P.n * 3.2 * 3.2 * digits + P.n * 0.5 / 12.0 + 1.0 / 12.0)
+    assert sd <= 6 * pred, (sd, pred)
