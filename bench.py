@@ -141,9 +141,8 @@ class Workload:
         self.ct_words = 2 * (LEVEL + 1) * self.n
         self.cts = [self.ev.upload_ct_device(self.inputs[i].data_ptr(), 2, LEVEL, SCALE) for i in range(ncts)]
         self.ctx.sync()
-        # output staging for e2e (largest result: 2 x 24 limbs)
+        # pinned host staging of the results (largest result: 2 x 24 limbs)
         self.host_out = torch.empty((2 * ncts, 2, LEVEL + 1, self.n), dtype=torch.int64, pin_memory=True)
-        self.dev_out = torch.empty((2 * ncts, 2, LEVEL + 1, self.n), dtype=torch.int64, device=q_all.device)
 
     def step_ops(self, cts):
         """128 x (mul + relin + rescale), 128 rotations by +-2^k; returns the results."""
@@ -155,26 +154,34 @@ class Workload:
             out.append(ev.rotate(cts[i], ROT_STEPS[i % len(ROT_STEPS)]))
         return out
 
-    KS_PER_STEP = 2 * NCT
-
     def step_resident(self):
         return self.step_ops(self.cts)
 
     def step_e2e(self):
-        """Host -> device upload of the step's inputs, the ops, device -> host of the results."""
-        torch, ev = self.torch, self.ev
-        stream = torch.cuda.ExternalStream(self.ctx.stream)
-        with torch.cuda.stream(stream):
-            self.inputs.copy_(self.host_in, non_blocking=True)
-        cts = [ev.upload_ct_device(self.inputs[i].data_ptr(), 2, LEVEL, SCALE) for i in range(self.ncts)]
+        """Through the C ABI with host buffers: upload_ct of the step's inputs from pinned
+        host memory, the ops, and an asynchronous download of every result to pinned host
+        memory; the caller's timing ends after the stream has drained."""
+        ev = self.ev
+        stride = self.ct_words * 8
+        base_in = self.host_in.data_ptr()
+        cts = [ev.upload_ct_host_ptr(base_in + i * stride, 2, LEVEL, SCALE) for i in range(self.ncts)]
         res = self.step_ops(cts)
+        base_out = self.host_out.data_ptr()
         for i, r in enumerate(res):
-            ev.download_ct_device(r, self.dev_out[i].data_ptr())
-        with torch.cuda.stream(stream):
-            self.host_out.copy_(self.dev_out, non_blocking=True)
+            ev.download_ct_async(r, base_out + i * stride)
         h2d = self.ncts * self.ct_words * 8
         d2h = sum(2 * (r.level() + 1) * self.n * 8 for r in res)
         return h2d, d2h
+
+    def close(self):
+        self.ctx.sync()
+        self.cts = None
+        self.ev = None
+        self.galois = None
+        self.relin = None
+        self.inputs = None
+        self.host_in = None
+        self.host_out = None
 
 
 def galois_elt(n, step):
@@ -276,6 +283,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncts", type=int, default=NCT, help="ciphertexts per step (smaller for profiling)")
+    ap.add_argument("--profile", action="store_true", help="run `warmup` + one step and exit (for ncu)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -323,15 +332,20 @@ def main():
     except Exception:
         pass
 
-    w = Workload(ckg, torch, local)
+    w = Workload(ckg, torch, local, args.ncts)
+    if args.profile:
+        for _ in range(args.warmup + 1):
+            w.step_resident()
+        w.close()
+        return
     l0 = ckg.launch_count()
     with ClockSampler(local) as clk:
         ms, _ = timed(torch, w.ctx, w.step_resident, args.steps, args.warmup, dist)
     launches = (ckg.launch_count() - l0) // (args.steps + args.warmup) * args.steps
-    ks = w.KS_PER_STEP * args.steps * world
+    ks = 2 * w.ncts * args.steps * world
     value = ks / (ms * 1e-3)
     ms_e2e, bytes_e2e = timed(torch, w.ctx, w.step_e2e, args.steps, max(args.warmup, 1), dist)
-    e2e = w.KS_PER_STEP * args.steps * world / (ms_e2e * 1e-3)
+    e2e = 2 * w.ncts * args.steps * world / (ms_e2e * 1e-3)
     roof = ntt_roofline(ckg, torch, w, peaks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -347,6 +361,7 @@ def main():
                         "d2h_bytes_per_step": bytes_e2e[1]},
                 "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
         print(json.dumps(line))
+    w.close()
     if dist:
         dist.destroy_process_group()
 

@@ -379,6 +379,12 @@ int ckg_ct_download(const ckg_ct* ct, uint64_t* host) {
   CKG_API_END
 }
 
+int ckg_ct_download_async(const ckg_ct* ct, uint64_t* host) {
+  CKG_API_BEGIN
+  copy_out(ct_of(ct), host, cudaMemcpyDeviceToHost);
+  CKG_API_END
+}
+
 int ckg_ct_download_device(const ckg_ct* ct, uint64_t* dev) {
   CKG_API_BEGIN
   copy_out(ct_of(ct), dev, cudaMemcpyDeviceToDevice);

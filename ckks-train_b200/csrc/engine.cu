@@ -14,12 +14,19 @@ namespace ckg {
   throw Error(ST_DEVICE, std::string(cudaGetErrorName(e)) + " (" + cudaGetErrorString(e) + ") at " + what);
 }
 
+StreamRes::~StreamRes() {
+  if (!own || !s) return;
+  cudaSetDevice(device);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+}
+
 DevBuf::~DevBuf() {
   if (!p) return;
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
-  if (pooled) cudaFreeAsync(p, st);
+  if (pooled) cudaFreeAsync(p, sres->s);
   else cudaFree(p);
   if (cur != device) cudaSetDevice(cur);
 }
@@ -28,7 +35,7 @@ void Context::activate() const { CKG_CUDA(cudaSetDevice(device)); }
 
 DevBufPtr Context::alloc(size_t words) {
   auto b = std::make_shared<DevBuf>();
-  b->st = stream;
+  b->sres = sres;
   b->device = device;
   b->words = words;
   if (words) CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, stream));
@@ -107,12 +114,15 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
     mods.emplace_back(v);
   }
   CKG_CUDA(cudaSetDevice(device));
+  sres = std::make_shared<StreamRes>();
+  sres->device = device;
   if (st) {
-    stream = st;
+    sres->s = st;
   } else {
-    CKG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    own_stream = true;
+    CKG_CUDA(cudaStreamCreateWithFlags(&sres->s, cudaStreamNonBlocking));
+    sres->own = true;
   }
+  stream = sres->s;
   {  // keep freed pool memory cached: steady-state ops allocate without driver calls
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -213,7 +223,6 @@ Context::~Context() {
   cudaFree(d_tw_fwd);
   cudaFree(d_tw_inv);
   cudaFree(d_conv);
-  if (own_stream) cudaStreamDestroy(stream);
 }
 
 const uint32_t* Context::perm(uint64_t elt) {

@@ -48,11 +48,21 @@ struct Error : std::runtime_error {
     if (e_ != cudaSuccess) ::ckg::throw_cuda(e_, #x); \
   } while (0)
 
+// The context's stream, shared by the context and every allocation made on it, so the
+// stream outlives the last stream-ordered free whatever order handles are released in.
+struct StreamRes {
+  cudaStream_t s = nullptr;
+  int device = 0;
+  bool own = false;
+  ~StreamRes();
+};
+typedef std::shared_ptr<StreamRes> StreamPtr;
+
 // A stream-ordered device allocation of `words` u64.
 struct DevBuf {
   uint64_t* p = nullptr;
   size_t words = 0;
-  cudaStream_t st = nullptr;
+  StreamPtr sres;
   int device = 0;
   bool pooled = true;
   DevBuf() = default;
@@ -75,8 +85,8 @@ struct DevKey {
 
 struct Context {
   int device = 0;
+  StreamPtr sres;
   cudaStream_t stream = nullptr;
-  bool own_stream = false;
   uint32_t log_n = 0;
   uint64_t n = 0;
   uint32_t nq = 0, k = 0, dnum = 0, alpha = 0, L = 0;

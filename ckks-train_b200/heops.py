@@ -124,6 +124,7 @@ def _declare(L):
     L.ckg_ct_upload_device.argtypes = [VP, VP, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_ct_download.argtypes = [VP, U64P]
     L.ckg_ct_download_device.argtypes = [VP, VP]
+    L.ckg_ct_download_async.argtypes = [VP, VP]
     L.ckg_ct_info.argtypes = [VP, U32P, U32P, C.POINTER(C.c_double)]
     L.ckg_ct_clone.argtypes = [VP]
     L.ckg_ct_clone.restype = VP
@@ -464,6 +465,16 @@ class CudaEvaluator:
 
     def download_ct_device(self, ct, ptr):
         _check(lib().ckg_ct_download_device(ct.h, VP(ptr)))
+
+    def upload_ct_host_ptr(self, ptr, ncomp, level, scale):
+        """upload_ct from a raw host address (pinned memory makes the copy asynchronous)."""
+        h = VP()
+        _check(lib().ckg_ct_upload(self.h, C.cast(VP(ptr), U64P), ncomp, level, scale, C.byref(h)))
+        return Ciphertext(self, h)
+
+    def download_ct_async(self, ct, ptr):
+        """Queues the copy of `ct` to the host address `ptr`; complete after ctx.sync()."""
+        _check(lib().ckg_ct_download_async(ct.h, VP(ptr)))
 
     def upload_pt(self, data, scale):
         d = np.ascontiguousarray(data, np.uint64)

@@ -143,6 +143,9 @@ CKG_API int ckg_ct_upload(ckg_eval* ev, const uint64_t* host, uint32_t ncomp, ui
 CKG_API int ckg_ct_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t ncomp, uint32_t level, double scale,
                          ckg_ct** out);
 CKG_API int ckg_ct_download(const ckg_ct* ct, uint64_t* host);
+/* The same without waiting: queued on the context's stream (host should be pinned);
+ * the data is in place after ckg_ctx_sync(). */
+CKG_API int ckg_ct_download_async(const ckg_ct* ct, uint64_t* host);
 /* Copy of the ciphertext into a device buffer (ncomp * (level+1) * N words), queued. */
 CKG_API int ckg_ct_download_device(const ckg_ct* ct, uint64_t* dev);
 CKG_API void ckg_ct_info(const ckg_ct* ct, uint32_t* ncomp, uint32_t* level, double* scale);

@@ -81,9 +81,10 @@ def test_arithmetic_ops(env):
     env.check(env.cpu.negate(a_cpu), env.gpu.negate(a_gpu), "negate")
     t_cpu, t_gpu = env.cpu.mul_no_relin(a_cpu, b_cpu), env.gpu.mul_no_relin(a_gpu, b_gpu)
     env.check(t_cpu, t_gpu, "mul_no_relin")
-    # 3 + 2 component add / sub (lazy relinearization pattern)
-    env.check(env.cpu.add(t_cpu, a_cpu), env.gpu.add(t_gpu, a_gpu), "add 3+2")
-    env.check(env.cpu.sub(a_cpu, t_cpu), env.gpu.sub(a_gpu, t_gpu), "sub 2-3")
+    # 3 + 2 component add / sub (lazy relinearization pattern), at the product's scale
+    ar_cpu, ar_gpu = env.cpu.relabel(a_cpu, t_cpu.scale), env.gpu.relabel(a_gpu, t_gpu.scale())
+    env.check(env.cpu.add(t_cpu, ar_cpu), env.gpu.add(t_gpu, ar_gpu), "add 3+2")
+    env.check(env.cpu.sub(ar_cpu, t_cpu), env.gpu.sub(ar_gpu, t_gpu), "sub 2-3")
     r_cpu, r_gpu = env.cpu.relinearize(t_cpu), env.gpu.relinearize(t_gpu)
     env.check(r_cpu, r_gpu, "relinearize")
     m_cpu, m_gpu = env.cpu.mul(a_cpu, b_cpu), env.gpu.mul(a_gpu, b_gpu)
