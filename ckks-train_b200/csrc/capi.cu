@@ -5,27 +5,13 @@
 #include <string>
 
 #include "../../include/ckg.h"
-#include "evaluator.hpp"
+#include "handles.hpp"
 
 using namespace ckg;
 
-struct ckg_ctx {
-  std::unique_ptr<Context> c;
-};
-struct ckg_key {
-  KeyPtr k;
-};
-struct ckg_eval {
-  std::unique_ptr<Evaluator> e;
-};
-struct ckg_ct {
-  Ct c;
-};
-struct ckg_pt {
-  Pt p;
-};
-
 static thread_local std::string g_last_error;
+
+void ckg_set_last_error(const char* msg) { g_last_error = msg; }
 
 static int fail(int code, const std::string& msg) {
   g_last_error = msg;

@@ -1,0 +1,24 @@
+// Definitions of the opaque C ABI handles (include/ckg.h), shared by the C ABI sources.
+#pragma once
+#include <memory>
+
+#include "evaluator.hpp"
+
+struct ckg_ctx {
+  std::unique_ptr<ckg::Context> c;
+};
+struct ckg_key {
+  ckg::KeyPtr k;
+};
+struct ckg_eval {
+  std::unique_ptr<ckg::Evaluator> e;
+};
+struct ckg_ct {
+  ckg::Ct c;
+};
+struct ckg_pt {
+  ckg::Pt p;
+};
+
+// Sets the calling thread's message returned by ckg_last_error().
+void ckg_set_last_error(const char* msg);

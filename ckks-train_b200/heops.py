@@ -110,6 +110,7 @@ def _declare(L):
     L.ckg_key_bytes.argtypes = [VP]
     L.ckg_key_bytes.restype = C.c_uint64
     L.ckg_key_switch.argtypes = [VP, VP, VP, C.c_uint32, VP, VP]
+    L.ckg_key_switch_noalloc.argtypes = [VP, VP, VP, C.c_uint32, VP, VP]
     L.ckg_eval_create.argtypes = [VP, VP, C.POINTER(VP), C.c_uint32, C.c_uint32, C.POINTER(VP)]
     L.ckg_eval_destroy.argtypes = [VP]
     L.ckg_eval_fork.argtypes = [VP, C.POINTER(VP)]
@@ -264,6 +265,11 @@ class Context:
 
     def key_switch(self, key, src, level, out_b, out_a):
         _check(lib().ckg_key_switch(self.h, key.h, VP(src), level, VP(out_b), VP(out_a)))
+
+    def key_switch_noalloc(self, key, src, level, out_b, out_a):
+        """key_switch that allocates no device memory: its working space is the library's
+        fixed 128 MiB device array (for callers that cannot allocate while serving)."""
+        _check(lib().ckg_key_switch_noalloc(self.h, key.h if key else None, VP(src), level, VP(out_b), VP(out_a)))
 
 
 class Key:

@@ -119,6 +119,25 @@ CKG_API uint64_t ckg_key_bytes(const ckg_key* key);
 CKG_API int ckg_key_switch(ckg_ctx* ctx, const ckg_key* key, const uint64_t* in, uint32_t level, uint64_t* out_b,
                    uint64_t* out_a);
 
+/* ckg_key_switch without any device allocation. It has no counterpart in the reference.
+ * It is for callers that cannot allocate device memory while serving a request, for
+ * example a serving process that reserved its whole HBM budget up front and must not fail
+ * or stall on an allocation mid-request, or an embedding runtime that owns every device
+ * allocation. The caller still passes the input and both outputs.
+ *  - The working space is one fixed array of 128 MiB in device memory, held by every GPU
+ *    that loads this library until the process exits. A level whose key switch needs more
+ *    (e.g. N = 2^16 with 32 data + 4 special primes at its top level) is rejected with
+ *    CKG_INVALID_PARAMS and a message stating both sizes; N = 2^16 with 24 + 8 primes and
+ *    3 digits fits at every level.
+ *  - The first call on a device looks up that array's device address; make that first
+ *    call before any stream capture.
+ *  - Every call shares the array and leaves it holding its own intermediates; nothing in
+ *    it needs to start at zero (each call writes every word it reads). Calls that overlap
+ *    on the GPU, for instance from two contexts with different streams on one device,
+ *    race on it: order them on one stream. */
+CKG_API int ckg_key_switch_noalloc(ckg_ctx* ctx, const ckg_key* key, const uint64_t* in, uint32_t level,
+                                   uint64_t* out_b, uint64_t* out_a);
+
 /* ---- evaluator (HeOps, crates/ckks-train-ckks/src/ops.rs:198-356) ------------------- */
 
 /* Evaluator::with_config (evaluator.rs:193-206): relin may be NULL; galois[0..ngal) are
