@@ -1,18 +1,26 @@
 """Key-switching throughput of the B200 RNS-CKKS evaluator path (one JSON line).
 
-Workload (one step): N = 2^16, 24 x 50-bit data primes + 8 x 60-bit special primes,
-dnum = 3 (alpha = 8), 128 seeded uniform ciphertexts at 24 limbs (level 23):
-128 x (HMult + relinearization + rescale) and 128 rotations by +-2^k (k = 0..14, 30 Galois
-keys), i.e. 256 key switches. The metric is key switches per second.
+Parameters: N = 2^16, 24 x 50-bit data primes + 8 x 60-bit special primes, dnum = 3
+(alpha = 8), 31 evaluation keys (relinearization + 30 Galois keys for +-2^k, k = 0..14).
 
-`value` runs the inputs resident in HBM through the evaluator's C ABI; `e2e` runs the same
-step with the inputs copied from pinned host memory and every result copied back inside
-the timed region. `--impl reference` times the CPU path of the reference (the oracle's
-restatement of crates/ckks-train-ckks, OpenMP over the same units as its `parallel`
-feature) on a bounded sample of the same workload.
+Headline (`value`): the batched uneven-level stream. 512 ciphertexts with limb counts drawn
+uniformly from {4..24}, a seeded op mix of 40% HMult+relin+rescale, 40% rotation by
++-2^k and 20% plaintext-multiply+rescale, executed as one CUDA-graph-captured batch (one
+launch per stage for a chunk of ops); one step = one replay of the whole batch. The
+metric is key switches per second (HMult and rotation one each).
 
-Multi-GPU: each rank runs the same step on its own GPU with its own keys (independent
-ciphertexts shard with no exchange, weak scaling); the time is the max over ranks.
+Beside it (`plain`): the plain one-op-at-a-time path on the full-level workload, 128
+ciphertexts at 24 limbs, 128 x (HMult+relin+rescale) and 128 rotations, each op an
+individual evaluator call.
+
+`e2e`: the batched stream through the C ABI with host buffers: every input uploaded from
+pinned host memory, the batch built and run, every result downloaded to pinned host
+memory, all inside the timed region. `--impl reference` times the reference's CPU path
+(the oracle's restatement of crates/ckks-train-ckks with OpenMP over the units of its
+`parallel` feature) on a bounded sample of the same op mix.
+
+Multi-GPU: each rank runs the same stream on its own GPU with its own keys and inputs
+(independent ciphertexts shard with no exchange: weak scaling); time = max over ranks.
 """
 
 import argparse
@@ -34,9 +42,11 @@ Q_BITS = [50] * 24
 P_BITS = [60] * 8
 DNUM = 3
 SCALE = 2.0 ** 50
-NCT = 128
-LEVEL = 23
 ROT_STEPS = [s * (1 << k) for k in range(15) for s in (1, -1)]  # +-2^k, k = 0..14
+MIX_OPS = 512
+MIX_LIMBS = (4, 24)
+PLAIN_CTS = 128
+PLAIN_LEVEL = 23
 
 
 def load_package():
@@ -48,6 +58,23 @@ def load_package():
     sys.modules["ckks_train_b200"] = mod
     spec.loader.exec_module(mod)
     return mod
+
+
+def galois_elt(n, step):
+    return pow(3, step % (n // 2), 2 * n)
+
+
+def mix_ops(seed, count=MIX_OPS):
+    """The seeded op stream: (kind, level, steps)."""
+    rng = np.random.default_rng(seed)
+    ops = []
+    for _ in range(count):
+        r = rng.random()
+        kind = "mul" if r < 0.4 else ("rot" if r < 0.8 else "pmul")
+        limbs = int(rng.integers(MIX_LIMBS[0], MIX_LIMBS[1] + 1))
+        steps = ROT_STEPS[int(rng.integers(0, len(ROT_STEPS)))]
+        ops.append((kind, limbs - 1, steps))
+    return ops
 
 
 # ---- clocks during the timed region -------------------------------------------------
@@ -96,30 +123,24 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-# ---- the workload ---------------------------------------------------------------------
+# ---- set-up: context, keys, evaluator ------------------------------------------------
 
-class Workload:
-    """Keys, inputs and the evaluator of one rank (synthetic uniform key material)."""
+class Setup:
+    """Context, 31 keys (synthetic uniform key material: throughput does not depend on the
+    key values) and the evaluator of one rank."""
 
-    def __init__(self, ckg, torch, device, ncts=NCT):
-        self.ckg, self.torch = ckg, torch
+    def __init__(self, ckg, torch, device):
+        self.ckg, self.torch, self.device = ckg, torch, device
         self.ctx = ckg.Context.from_bits(LOG_N, Q_BITS, P_BITS, DNUM, device=device, scale_bits=50)
         ctx = self.ctx
         self.n = ctx.n
-        self.ncts = ncts
-        g = torch.Generator(device=f"cuda:{device}")
-        g.manual_seed(20261203 + device)
-        self.gen = g
-        q_all = torch.tensor(ctx.q + ctx.p, dtype=torch.int64, device=f"cuda:{device}")
-        self.q_all = q_all
-        key_limbs = torch.cat([q_all[: LEVEL + 1], q_all[len(ctx.q):]])  # key Q limbs 0..L then P
-        self.keys = []
+        self.gen = torch.Generator(device=f"cuda:{device}")
+        self.gen.manual_seed(20261203 + device)
+        self.q_all = torch.tensor(ctx.q + ctx.p, dtype=torch.int64, device=f"cuda:{device}")
+        shape = (DNUM, 2, len(ctx.q) + ctx.k, self.n)
 
         def make_key(elt):
-            shape = (DNUM, 2, len(ctx.q) + ctx.k, self.n)
-            qcol = torch.cat([q_all[: len(ctx.q)], q_all[len(ctx.q):]]).view(1, 1, -1, 1)
-            t = torch.randint(0, 1 << 62, shape, generator=g, device=q_all.device, dtype=torch.int64) % qcol
-            torch.cuda.synchronize()
+            t = self.uniform(shape, self.q_all.view(1, 1, -1, 1))
             k = ctx.upload_key_device(t.data_ptr(), shape, elt)
             del t
             return k
@@ -127,67 +148,117 @@ class Workload:
         self.relin = make_key(0)
         self.galois = {}
         for s in ROT_STEPS:
-            elt = galois_elt(self.n, s)
-            if elt not in self.galois:
-                self.galois[elt] = make_key(elt)
+            e = galois_elt(self.n, s)
+            if e not in self.galois:
+                self.galois[e] = make_key(e)
         self.ev = ckg.CudaEvaluator(ctx, self.relin, list(self.galois.values()))
-        # inputs: NCT ciphertexts of 2 components at LEVEL (24 limbs), uniform residues
-        shape = (ncts, 2, LEVEL + 1, self.n)
-        qcol = q_all[: LEVEL + 1].view(1, 1, -1, 1)
-        self.inputs = torch.randint(0, 1 << 62, shape, generator=g, device=q_all.device, dtype=torch.int64) % qcol
-        torch.cuda.synchronize()
-        self.host_in = torch.empty(shape, dtype=torch.int64, pin_memory=True)
-        self.host_in.copy_(self.inputs.cpu())
-        self.ct_words = 2 * (LEVEL + 1) * self.n
-        self.cts = [self.ev.upload_ct_device(self.inputs[i].data_ptr(), 2, LEVEL, SCALE) for i in range(ncts)]
+
+    def uniform(self, shape, qcol):
+        t = self.torch.randint(0, 1 << 62, shape, generator=self.gen, device=self.q_all.device,
+                               dtype=self.torch.int64) % qcol
+        self.torch.cuda.synchronize()
+        return t
+
+    def ct(self, level, ncomp=2):
+        t = self.uniform((ncomp, level + 1, self.n), self.q_all[: level + 1].view(1, -1, 1))
+        c = self.ev.upload_ct_device(t.data_ptr(), ncomp, level, SCALE)
         self.ctx.sync()
-        # pinned host staging of the results (largest result: 2 x 24 limbs)
-        self.host_out = torch.empty((2 * ncts, 2, LEVEL + 1, self.n), dtype=torch.int64, pin_memory=True)
+        return c, t
 
-    def step_ops(self, cts):
-        """128 x (mul + relin + rescale), 128 rotations by +-2^k; returns the results."""
-        ev = self.ev
-        out = []
-        for i in range(self.ncts):
-            out.append(ev.rescale(ev.mul(cts[i], cts[(i + 1) % self.ncts])))
-        for i in range(self.ncts):
-            out.append(ev.rotate(cts[i], ROT_STEPS[i % len(ROT_STEPS)]))
-        return out
+    def pt(self, level):
+        t = self.uniform((level + 1, self.n), self.q_all[: level + 1].view(-1, 1))
+        p = self.ev.upload_pt_device(t.data_ptr(), level, SCALE)
+        self.ctx.sync()
+        return p, t
 
-    def step_resident(self):
-        return self.step_ops(self.cts)
+
+class Mix:
+    """The batched uneven-level stream."""
+
+    def __init__(self, S, ops, keep_host=True):
+        self.S, self.ops = S, ops
+        self.inputs = []  # (kind, a, b_or_pt, steps)
+        host = []
+        for kind, level, steps in ops:
+            a, ta = S.ct(level)
+            if kind == "mul":
+                extra, tb = S.ct(level)
+            elif kind == "pmul":
+                extra, tb = S.pt(level)
+            else:
+                extra, tb = None, None
+            self.inputs.append((kind, a, extra, steps))
+            if keep_host:
+                host.append((ta.cpu().pin_memory(), None if tb is None else tb.cpu().pin_memory()))
+            del ta, tb
+        self.host = host
+        self.batch, self.outputs = self.make_batch(self.inputs)
+        self.ks = self.batch.key_switches()
+
+    def make_batch(self, inputs):
+        b = self.S.ckg.Batch(self.S.ev)
+        outs = []
+        for kind, a, extra, steps in inputs:
+            if kind == "mul":
+                outs.append(b.mul_relin_rescale(a, extra))
+            elif kind == "rot":
+                outs.append(b.rotate(a, steps))
+            else:
+                outs.append(b.mul_plain_rescale(a, extra))
+        return b, outs
+
+    def step_graph(self):
+        self.batch.launch_graph()
+
+    def prepare_e2e(self):
+        torch = self.S.torch
+        self.out_host = []
+        for (kind, level, steps) in self.ops:
+            lv = level if kind == "rot" else level - 1
+            self.out_host.append(torch.empty((2, lv + 1, self.S.n), dtype=torch.int64, pin_memory=True))
 
     def step_e2e(self):
-        """Through the C ABI with host buffers: upload_ct of the step's inputs from pinned
-        host memory, the ops, and an asynchronous download of every result to pinned host
-        memory; the caller's timing ends after the stream has drained."""
-        ev = self.ev
-        stride = self.ct_words * 8
-        base_in = self.host_in.data_ptr()
-        cts = [ev.upload_ct_host_ptr(base_in + i * stride, 2, LEVEL, SCALE) for i in range(self.ncts)]
-        res = self.step_ops(cts)
-        base_out = self.host_out.data_ptr()
-        for i, r in enumerate(res):
-            ev.download_ct_async(r, base_out + i * stride)
-        h2d = self.ncts * self.ct_words * 8
-        d2h = sum(2 * (r.level() + 1) * self.n * 8 for r in res)
+        """Upload every input from pinned host memory, build and run the batch, download
+        every result to pinned host memory (through the C ABI's host-buffer calls)."""
+        ev = self.S.ev
+        ins, h2d = [], 0
+        for (kind, level, steps), (ha, hb) in zip(self.ops, self.host):
+            a = ev.upload_ct_host_ptr(ha.data_ptr(), 2, level, SCALE)
+            h2d += ha.numel() * 8
+            extra = None
+            if kind == "mul":
+                extra = ev.upload_ct_host_ptr(hb.data_ptr(), 2, level, SCALE)
+                h2d += hb.numel() * 8
+            elif kind == "pmul":
+                extra = ev.upload_pt_host_ptr(hb.data_ptr(), level, SCALE)
+                h2d += hb.numel() * 8
+            ins.append((kind, a, extra, steps))
+        b, outs = self.make_batch(ins)
+        b.run()
+        d2h = 0
+        for r, dst in zip(outs, self.out_host):
+            ev.download_ct_async(r, dst.data_ptr())
+            d2h += r.size() * (r.level() + 1) * self.S.n * 8
+        self._last = (b, outs, ins)  # keep alive until the stream drains
         return h2d, d2h
 
-    def close(self):
-        self.ctx.sync()
-        self.cts = None
-        self.ev = None
-        self.galois = None
-        self.relin = None
-        self.inputs = None
-        self.host_in = None
-        self.host_out = None
 
+class Plain:
+    """The plain per-op path: 128 x (HMult+relin+rescale) + 128 rotations at 24 limbs."""
 
-def galois_elt(n, step):
-    m = 2 * n
-    k = step % (n // 2)
-    return pow(3, k, m)
+    def __init__(self, S):
+        self.S = S
+        self.cts = [S.ct(PLAIN_LEVEL)[0] for _ in range(PLAIN_CTS)]
+        self.ks = 2 * PLAIN_CTS
+
+    def step(self):
+        ev, cts = self.S.ev, self.cts
+        out = []
+        for i in range(PLAIN_CTS):
+            out.append(ev.rescale(ev.mul(cts[i], cts[(i + 1) % PLAIN_CTS])))
+        for i in range(PLAIN_CTS):
+            out.append(ev.rotate(cts[i], ROT_STEPS[i % len(ROT_STEPS)]))
+        return out
 
 
 # ---- timing ---------------------------------------------------------------------------
@@ -213,25 +284,24 @@ def timed(torch, ctx, fn, steps, warmup, dist=None):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-        dist.barrier()
     return ms, extra
 
 
-def ntt_roofline(ckg, torch, w, peaks):
-    """The forward + inverse NTT of 32 limbs (24 data + 8 special), timed alone with CUDA
-    events on the library's stream; algorithmic bytes = every limb read and written once
-    per transform."""
-    ctx = w.ctx
-    limbs = len(ctx.q) + ctx.k
-    buf = torch.randint(0, 1 << 40, (limbs, w.n), dtype=torch.int64, device="cuda")
+def ntt_roofline(torch, S, peaks, limbs=768):
+    """Forward + inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as in a
+    batched stage), timed alone with CUDA events on the library's stream. Algorithmic bytes
+    per transform: every limb read and written once (both passes together)."""
+    ctx = S.ctx
+    buf = torch.randint(0, 1 << 40, (limbs, S.n), dtype=torch.int64, device="cuda")
     torch.cuda.synchronize()
-    primes = list(range(limbs))
+    nprimes = len(ctx.q) + ctx.k
+    primes = [i % nprimes for i in range(limbs)]
     stream = torch.cuda.ExternalStream(ctx.stream)
     for _ in range(3):
         ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, False)
         ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, True)
     ctx.sync()
-    reps = 50
+    reps = 10
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
     for _ in range(reps):
@@ -239,77 +309,89 @@ def ntt_roofline(ckg, torch, w, peaks):
         ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, True)
     b.record(stream)
     ctx.sync()
-    ms = a.elapsed_time(b) / (2 * reps)  # one transform over 32 limbs
-    alg = limbs * w.n * 8 * 2
+    ms = a.elapsed_time(b) / (2 * reps)
+    alg = limbs * S.n * 8 * 2
     achieved = alg / (ms * 1e-3) / 1e9
     peak = peaks.get("hbm_gbs", 6650.0)
-    return {"kernel": "ntt (32 limbs, N=2^16, one transform = 2 passes)", "bound": "hbm",
+    return {"kernel": f"ntt forward/inverse, {limbs} limbs of N=2^16 per transform (2 passes)", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": None, "ms_per_launch": round(ms, 5), "alg_bytes": alg,
-            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+            "traffic": None, "ms_per_transform": round(ms, 4), "alg_bytes": alg,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
 
 
 # ---- CPU baseline / reference arm ------------------------------------------------------
 
-def cpu_sample(threads, budget_s=20.0):
-    """The oracle's CPU evaluator on a bounded sample of the workload (mul+relin+rescale and
-    rotations at level 23), keys generated by its own key generator."""
+def cpu_sample(threads, budget_s=20.0, seed=20261203):
+    """The oracle's CPU evaluator (the reference's CPU path restated, OpenMP over the units
+    of its `parallel` feature) on ops drawn from the same mix, keys from its own key
+    generator, until the time budget is used."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.set_threads(threads)
     P = O.Params.from_bits(LOG_N, Q_BITS, P_BITS, 50, DNUM)
     kg = O.KeyGenerator(P, 5)
     rk = kg.relin_key()
-    e1 = O.galois_elt(P.n, 1)
-    gk = {e1: kg.galois_key(e1)}
+    ops = mix_ops(seed, 64)
+    elts = sorted({O.galois_elt(P.n, s) for kind, _, s in ops if kind == "rot"})[:4]
+    gk = {e: kg.galois_key(e) for e in elts}
     ev = O.Evaluator(P, rk, gk)
-    a = ev.ct(np.stack([P.random_q(1, LEVEL), P.random_q(2, LEVEL)]), SCALE)
-    b = ev.ct(np.stack([P.random_q(3, LEVEL), P.random_q(4, LEVEL)]), SCALE)
-    done, t0 = 0, time.perf_counter()
-    while True:
-        ev.rescale(ev.mul(a, b))
-        ev.rotate(a, 1)
-        done += 2
-        if time.perf_counter() - t0 > budget_s / 2 or done >= 8:
+    ks, t0 = 0, time.perf_counter()
+    for kind, level, steps in ops:
+        if kind == "rot" and O.galois_elt(P.n, steps) not in gk:
+            continue
+        a = ev.ct(np.stack([P.random_q(ks * 2 + 1, level), P.random_q(ks * 2 + 2, level)]), SCALE)
+        if kind == "mul":
+            ev.rescale(ev.mul(a, a))
+            ks += 1
+        elif kind == "rot":
+            ev.rotate(a, steps)
+            ks += 1
+        else:
+            ev.rescale(ev.mul_plain(a, P.random_q(7, level), SCALE))
+        if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return done / dt, f"{done} key switches ({done // 2} mul+relin+rescale, {done // 2} rotations) at 24 limbs"
+    return ks / dt, f"{ks} key switches of the seeded op mix (limbs 4..24) in {dt:.1f} s"
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ncts", type=int, default=NCT, help="ciphertexts per step (smaller for profiling)")
-    ap.add_argument("--profile", action="store_true", help="run `warmup` + one step and exit (for ncu)")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ops", type=int, default=MIX_OPS, help="ops of the batched stream (smaller for profiling)")
+    ap.add_argument("--profile", default=None, choices=["batch", "plain"],
+                    help="run the set-up and `warmup` + 1 step of one path, print nothing (for ncu)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    metric, unit = "keyswitch/s N=2^16 L=24 (24+8 primes, dnum 3)", "keyswitch/s"
-    config = {"workload": "N=2^16, 24x50-bit q + 8x60-bit p, dnum 3; 128 uniform ciphertexts at 24 limbs; "
-                          "128 x (HMult+relin+rescale) + 128 rotations by +-2^k (k=0..14)",
-              "key_switches_per_step": 2 * NCT, "path": "plain per-op evaluator calls",
-              "l2": "inputs (3.2 GB) and keys (3 GB) larger than L2"}
+    metric, unit = "keyswitch/s N=2^16 L=24 (24+8 primes, dnum 3), batched uneven-level stream", "keyswitch/s"
+    config = {"workload": f"batched stream: {args.ops} ciphertexts, limbs uniform in 4..24, seeded mix 40% "
+                          "HMult+relin+rescale / 40% rotation +-2^k / 20% PtMult+rescale; one CUDA-graph replay "
+                          "per step",
+              "params": "N=2^16, 24x50-bit q + 8x60-bit p, dnum 3, 31 keys",
+              "l2": "inputs (~10 GB) and keys (3 GB) larger than L2"}
 
     if args.impl == "reference":
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        vals = []
-        for _ in range(args.warmup):
-            pass
+        vals, sample = [], ""
+        budget = max(5.0, 60.0 / max(args.steps, 1))
         for _ in range(max(args.steps, 1)):
-            v, sample = cpu_sample(threads, budget_s=20.0 / max(args.steps, 1))
+            v, sample = cpu_sample(threads, budget_s=budget)
             vals.append(v)
         v = float(np.mean(vals))
         print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 3), "unit": unit,
                           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                          "higher_is_better": True, "dtype": "u64", "data": "synthetic", "config": config,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                          "data": "synthetic", "config": config,
                           "cpu_baseline": {"value": round(v, 3), "unit": unit, "cores": threads, "kind": "port",
                                            "sample": sample},
                           "e2e": {"value": round(v, 3), "unit": unit, "h2d_bytes_per_step": 0,
@@ -318,13 +400,12 @@ def main():
 
     import torch
     dist = None
+    torch.cuda.set_device(local)
     if world > 1:
+        import datetime
         import torch.distributed as dist_mod
-        torch.cuda.set_device(local)
-        dist_mod.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+        dist_mod.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
         dist = dist_mod
-    else:
-        torch.cuda.set_device(local)
     ckg = load_package()
     peaks = {}
     try:
@@ -332,21 +413,43 @@ def main():
     except Exception:
         pass
 
-    w = Workload(ckg, torch, local, args.ncts)
-    if args.profile:
+    S = Setup(ckg, torch, local)
+    if args.profile == "plain":
+        P = Plain(S)
         for _ in range(args.warmup + 1):
-            w.step_resident()
-        w.close()
+            P.step()
+        S.ctx.sync()
         return
+    mix = Mix(S, mix_ops(20261203 + rank, args.ops), keep_host=not args.no_e2e and args.profile is None)
     l0 = ckg.launch_count()
+    mix.batch.capture_graph()
+    launches_per_step = ckg.launch_count() - l0
+    if args.profile == "batch":
+        for _ in range(args.warmup + 1):
+            mix.step_graph()
+        S.ctx.sync()
+        return
     with ClockSampler(local) as clk:
-        ms, _ = timed(torch, w.ctx, w.step_resident, args.steps, args.warmup, dist)
-    launches = (ckg.launch_count() - l0) // (args.steps + args.warmup) * args.steps
-    ks = 2 * w.ncts * args.steps * world
-    value = ks / (ms * 1e-3)
-    ms_e2e, bytes_e2e = timed(torch, w.ctx, w.step_e2e, args.steps, max(args.warmup, 1), dist)
-    e2e = 2 * w.ncts * args.steps * world / (ms_e2e * 1e-3)
-    roof = ntt_roofline(ckg, torch, w, peaks)
+        ms, _ = timed(torch, S.ctx, mix.step_graph, args.steps, args.warmup, dist)
+    value = mix.ks * args.steps * world / (ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        mix.prepare_e2e()
+        steps_e = max(1, min(args.steps, 3))
+        ms_e, (h2d, d2h) = timed(torch, S.ctx, mix.step_e2e, steps_e, 1, dist)
+        e2e = {"value": round(mix.ks * steps_e * world / (ms_e * 1e-3), 2), "unit": unit,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": round(ms_e / steps_e, 3)}
+    plain = None
+    if not args.no_plain:
+        P = Plain(S)
+        ms_p, _ = timed(torch, S.ctx, P.step, 2, 1, dist)
+        pv = P.ks * 2 * world / (ms_p * 1e-3)
+        plain = {"value": round(pv, 2), "unit": unit,
+                 "workload": "128 ciphertexts at 24 limbs: 128 x (HMult+relin+rescale) + 128 rotations, "
+                             "one evaluator call per op",
+                 "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2)}
+    roof = ntt_roofline(torch, S, peaks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -355,14 +458,16 @@ def main():
     if rank == 0:
         line = {"metric": metric, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded uniform "
-                "ciphertexts and uniform key material)", "config": config,
-                "e2e": {"value": round(e2e, 2), "unit": unit, "h2d_bytes_per_step": bytes_e2e[0],
-                        "d2h_bytes_per_step": bytes_e2e[1]},
-                "gpu_launches": int(launches), "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
+                "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
+                "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
+                "cpu_baseline": cpu, "clocks": clk.summary()}
         print(json.dumps(line))
-    w.close()
+    mix.batch = None
+    S.ctx.sync()
     if dist:
+        dist.barrier()
         dist.destroy_process_group()
 
 

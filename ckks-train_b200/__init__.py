@@ -6,6 +6,7 @@ hyphen, so loaders register it by path; see ``load_package`` in bench.py).
 
 from .heops import (  # noqa: F401
     BSGS,
+    Batch,
     HOIST,
     LAZY_RELIN,
     COUNTER_FIELDS,

@@ -1,0 +1,58 @@
+// Batched execution of many evaluator ops at uneven levels in one launch sequence.
+//
+// A Batch collects HMult+relinearize+rescale, rotation and plaintext-multiply+rescale ops
+// on ciphertexts of any levels, with the evaluator's checks at enqueue time. Running it
+// issues one launch per stage for all ops of a chunk (tensor products, Galois gathers,
+// INTT, ModUp conversions, NTT, key inner products, ModDown, rescale), each over work lists
+// resident in device memory, and can be captured once into a CUDA graph and replayed.
+// Every result is bit-identical to the same op run on its own (the same kernels compute
+// each ciphertext independently), and the OpCounter advances as the per-op calls would.
+#pragma once
+#include <vector>
+
+#include "evaluator.hpp"
+
+namespace ckg {
+
+class Batch {
+ public:
+  explicit Batch(Evaluator* ev);
+  ~Batch();
+
+  Ct mul_relin_rescale(const Ct& a, const Ct& b);
+  Ct rotate(const Ct& a, int32_t steps);
+  Ct mul_plain_rescale(const Ct& a, const Pt& p);
+
+  void run();           // queues the whole batch on the context's stream
+  void capture_graph(); // captures run()'s launches into a CUDA graph (once)
+  void launch_graph();  // replays the graph
+  uint64_t key_switches() const;
+  size_t size() const { return items_.size(); }
+
+ private:
+  enum Kind { MUL = 0, ROT = 1, PMUL = 2 };
+  struct Item {
+    Kind kind;
+    Ct a, b, out;
+    Pt p;
+    uint64_t elt = 0;
+    const DevKey* key = nullptr;
+    bool trivial = false;  // rotation by a multiple of the slot count: out = a
+  };
+  struct Stage;  // device work lists of one chunk
+  void build();
+  void issue();
+  void count_ops();
+
+  Evaluator* ev_;
+  Context* ctx_;
+  std::vector<Item> items_;
+  bool built_ = false;
+  DevBufPtr scratch_;
+  DevBufPtr desc_;
+  std::vector<Stage*> chunks_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+};
+
+}  // namespace ckg

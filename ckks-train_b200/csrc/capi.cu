@@ -493,4 +493,58 @@ int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* cons
   CKG_API_END
 }
 
+// ---- batched execution ------------------------------------------------------------------
+
+static Batch& batch_of(ckg_batch* b) {
+  if (!b || !b->b) throw Error(CKG_INVALID_PARAMS, "null batch");
+  return *b->b;
+}
+
+int ckg_batch_create(ckg_eval* ev, ckg_batch** out) {
+  CKG_API_BEGIN
+  Evaluator& e = ev_of(ev);
+  *out = new ckg_batch{std::make_unique<Batch>(&e), ev};
+  CKG_API_END
+}
+
+void ckg_batch_destroy(ckg_batch* b) { delete b; }
+
+int ckg_batch_mul_relin_rescale(ckg_batch* b, const ckg_ct* x, const ckg_ct* y, ckg_ct** out) {
+  CKG_API_BEGIN
+  *out = new ckg_ct{batch_of(b).mul_relin_rescale(ct_of(x), ct_of(y))};
+  CKG_API_END
+}
+
+int ckg_batch_rotate(ckg_batch* b, const ckg_ct* x, int32_t steps, ckg_ct** out) {
+  CKG_API_BEGIN
+  *out = new ckg_ct{batch_of(b).rotate(ct_of(x), steps)};
+  CKG_API_END
+}
+
+int ckg_batch_mul_plain_rescale(ckg_batch* b, const ckg_ct* x, const ckg_pt* p, ckg_ct** out) {
+  CKG_API_BEGIN
+  *out = new ckg_ct{batch_of(b).mul_plain_rescale(ct_of(x), pt_of(p))};
+  CKG_API_END
+}
+
+int ckg_batch_run(ckg_batch* b) {
+  CKG_API_BEGIN
+  batch_of(b).run();
+  CKG_API_END
+}
+
+int ckg_batch_capture_graph(ckg_batch* b) {
+  CKG_API_BEGIN
+  batch_of(b).capture_graph();
+  CKG_API_END
+}
+
+int ckg_batch_launch_graph(ckg_batch* b) {
+  CKG_API_BEGIN
+  batch_of(b).launch_graph();
+  CKG_API_END
+}
+
+uint64_t ckg_batch_key_switches(const ckg_batch* b) { return b && b->b ? b->b->key_switches() : 0; }
+
 }  // extern "C"

@@ -71,15 +71,20 @@ std::vector<uint64_t> conv_table(const std::vector<HostMod>& mods, const std::ve
     for (uint32_t s : src) S = m.mul(S, mods[s].q % m.q);
     // h = (S - 1)/2 mod t = (S - 1) * 2^-1
     uint64_t h = m.mul(m.sub(S, 1 % m.q), (m.q + 1) / 2);
+    const uint64_t r64 = (uint64_t)(((u128)1 << 64) % m.q);
     w.push_back(t);
     w.push_back(m.q - S);
     w.push_back(m.q - h);
+    w.push_back(m.q);
+    w.push_back(r64);
+    w.push_back(m.shoup(r64));
+    w.push_back(m.shoup(1));
     w.push_back(0);
     for (size_t j = 0; j < ns; ++j) {
       uint64_t qhat = 1 % m.q;
       for (size_t i = 0; i < ns; ++i)
         if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
-      w.push_back(qhat);
+      w.push_back((qhat & ((1ULL << 30) - 1)) | ((qhat >> 30) << 32));
     }
   }
   return w;
@@ -385,31 +390,21 @@ void check_ks(const Context& c, const KsJob& j, uint32_t l) {
 void ks_tail(Context& c, const std::vector<KsJob>& jobs, uint32_t l, const std::vector<const uint64_t*>& conv,
              const std::vector<uint64_t*>& acc, const std::vector<uint64_t*>& mdscratch) {
   const size_t N = c.n, ext = l + 1 + c.k;
-  IpBatch proto{};
-  proto.level = (int)l;
-  proto.ndig = (int)c.digits_at(l);
-  proto.alpha = (int)c.alpha;
-  proto.L = (int)c.L;
-  proto.k = (int)c.k;
   std::vector<IpJob> ip;
-  // Keys with different data-limb counts need separate launches (the layout stride).
-  std::map<uint32_t, std::vector<size_t>> by_key_q;
-  for (size_t i = 0; i < jobs.size(); ++i) by_key_q[jobs[i].key->q_limbs].push_back(i);
-  for (auto& kv : by_key_q) {
-    ip.clear();
-    proto.key_q = (int)kv.first;
-    for (size_t i : kv.second) {
-      IpJob jb{};
-      jb.in = jobs[i].in;
-      for (uint32_t j = 0; j < c.digits_at(l); ++j) jb.conv[j] = conv[i] + conv_offset_limbs(c, l, j) * N;
-      jb.key = jobs[i].key->buf->p;
-      jb.out_b = acc[i];
-      jb.out_a = acc[i] + ext * N;
-      jb.perm = jobs[i].perm;
-      ip.push_back(jb);
-    }
-    launch_inner_product(c.dt, proto, ip.data(), (int)ip.size(), c.stream);
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    IpJob jb{};
+    jb.level = (int)l;
+    jb.ndig = (int)c.digits_at(l);
+    jb.key_q = (int)jobs[i].key->q_limbs;
+    jb.in = jobs[i].in;
+    for (uint32_t j = 0; j < c.digits_at(l); ++j) jb.conv[j] = conv[i] + conv_offset_limbs(c, l, j) * N;
+    jb.key = jobs[i].key->buf->p;
+    jb.out_b = acc[i];
+    jb.out_a = acc[i] + ext * N;
+    jb.perm = jobs[i].perm;
+    ip.push_back(jb);
   }
+  launch_inner_product(c.dt, (int)c.alpha, (int)c.L, (int)c.k, ip.data(), (int)ip.size(), c.stream);
   // ModDown of both accumulators of every job, fused with the additions.
   const size_t per = c.k + l + 1;
   std::vector<LimbRef> refs;

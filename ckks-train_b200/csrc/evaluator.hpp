@@ -88,6 +88,7 @@ class Evaluator {
   Ct matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x);
 
  private:
+  friend class Batch;
   Ct add_sub(const Ct& a, const Ct& b, bool sub);
   Ct new_ct(uint32_t ncomp, uint32_t level, double scale);
   void check_basis(const Ct& a) const;

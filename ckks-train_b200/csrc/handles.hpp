@@ -2,6 +2,7 @@
 #pragma once
 #include <memory>
 
+#include "batch.hpp"
 #include "evaluator.hpp"
 
 struct ckg_ctx {
@@ -18,6 +19,10 @@ struct ckg_ct {
 };
 struct ckg_pt {
   ckg::Pt p;
+};
+struct ckg_batch {
+  std::unique_ptr<ckg::Batch> b;
+  ckg_eval* ev;
 };
 
 // Sets the calling thread's message returned by ckg_last_error().

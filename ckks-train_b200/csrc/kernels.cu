@@ -35,12 +35,19 @@ constexpr int kCols = 16;           // columns per CTA in the column pass
 constexpr int kRowsPerCta = 16;     // rows per CTA in the row pass
 constexpr int kRowPad = kRow + kRow / 16;  // padded row stride in shared memory
 
+// Harvey butterfly. With LAZY (primes below 2^58) x is not brought back below 2q: values
+// grow by at most 2q per stage from [0, q), so all 16 stages of N = 2^16 stay below
+// 33q < 2^64 and one reduction at the end suffices.
+template <bool LAZY>
 CKG_DEV void ct_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
-  uint64_t xr = csub(x, two_q);
+  uint64_t xr = LAZY ? x : csub(x, two_q);
   uint64_t t = mul_shoup_lazy(y, w.x, w.y, q);
   x = xr + t;
   y = xr + two_q - t;
 }
+
+// Primes below this bound take the lazy forward path.
+constexpr uint64_t kLazyBound = 1ULL << 58;
 
 CKG_DEV void gs_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
   uint64_t s = x + y;
@@ -54,15 +61,10 @@ CKG_DEV ulonglong2 ldtw(const ulonglong2* t, uint32_t i) { return __ldg(t + i); 
 CKG_DEV int pad_idx(int k) { return k + (k >> 4); }
 
 // Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
-template <int LOGS>
-__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
-    k_ntt_fwd_cols(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n) {
+template <int LOGS, bool LAZY>
+CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roots, uint64_t* sm) {
   constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
-  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
-  const LimbRef ref = b.r[blockIdx.y];
-  const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
-  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  const uint64_t two_q = 2 * q;
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
   const int col = blockIdx.x * kCols + c;
   uint64_t x[1 << E1];
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
     const int half = 1 << (E1 - 1 - r);
 #pragma unroll
     for (int j = 0; j < (1 << E1); ++j)
-      if (!(j & half)) ct_bf(x[j], x[j + half], ldtw(roots, (1u << r) + (j >> (E1 - r))), q, two_q);
+      if (!(j & half)) ct_bf<LAZY>(x[j], x[j + half], ldtw(roots, (1u << r) + (j >> (E1 - r))), q, two_q);
   }
 #pragma unroll
   for (int j = 0; j < (1 << E1); ++j) sm[(ts + TPS * j) * kCols + c] = x[j];
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
       for (int j = 0; j < (1 << E2); ++j)
         if (!(j & half)) {
           const int k = (t2 << E2) + j;
-          ct_bf(y[j], y[j + half], ldtw(roots, (1u << r) + (k >> (LOGS - r))), q, two_q);
+          ct_bf<LAZY>(y[j], y[j + half], ldtw(roots, (1u << r) + (k >> (LOGS - r))), q, two_q);
         }
     }
 #pragma unroll
@@ -99,14 +101,23 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
   }
 }
 
-// Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
-__global__ void __launch_bounds__(256)
-    k_ntt_fwd_rows(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n) {
-  __shared__ uint64_t sm[kRowsPerCta * kRowPad];
-  const LimbRef ref = b.r[blockIdx.y];
-  const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
+template <int LOGS, class B>
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
+    k_ntt_fwd_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
+  LimbRef ref = b.r[blockIdx.y];
+  if (in_place) ref.src = ref.dst;
+  const uint64_t q = __ldg(&pc[ref.prime].q);
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm);
+  else fwd_cols_body<LOGS, false>(ref, q, roots, sm);
+}
+
+// Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
+template <bool LAZY>
+CKG_DEV void fwd_rows_body(const LimbRef& ref, const PrimeConst* P, const ulonglong2* roots, int log_n, uint64_t* sm) {
+  const uint64_t q = __ldg(&P->q), two_q = 2 * q;
   const int s0 = log_n - kRowLog;
   const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
   const uint32_t row = blockIdx.x * kRowsPerCta + rr;
@@ -120,7 +131,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int j = 0; j < 16; ++j)
       if (!(j & half))
-        ct_bf(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, two_q);
+        ct_bf<LAZY>(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, two_q);
   }
   uint64_t* srow = sm + rr * kRowPad;
 #pragma unroll
@@ -136,13 +147,16 @@ __global__ void __launch_bounds__(256)
     for (int j = 0; j < 16; ++j)
       if (!(j & half)) {
         const int k = 16 * t + j;
-        ct_bf(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, two_q);
+        ct_bf<LAZY>(x[j], x[j + half], ldtw(roots, (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, two_q);
       }
   }
+  if (LAZY) {
+    const uint64_t one_s = __ldg(&P->one_s);
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    uint64_t v = csub(x[j], two_q);
-    srow[pad_idx(16 * t + j)] = csub(v, q);
+    for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = csub(mul_shoup_lazy(x[j], 1, one_s, q), q);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = csub(csub(x[j], two_q), q);
   }
   __syncthreads();
   uint64_t* dst = ref.dst + (size_t)blockIdx.x * kRowsPerCta * kRow;
@@ -150,12 +164,27 @@ __global__ void __launch_bounds__(256)
   for (int i = 0; i < kRowsPerCta; ++i) dst[i * kRow + threadIdx.x] = sm[i * kRowPad + pad_idx(threadIdx.x)];
 }
 
-// Inverse row pass: GS stages u = 0..7 (pair distance 2^u) within 256-point rows.
+template <class B>
 __global__ void __launch_bounds__(256)
-    k_ntt_inv_rows(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n) {
+    k_ntt_fwd_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
-  const LimbRef ref = b.r[blockIdx.y];
+  LimbRef ref = b.r[blockIdx.y];
+  if (in_place) ref.src = ref.dst;
+  const PrimeConst* P = pc + ref.prime;
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  if (__ldg(&P->q) < kLazyBound) fwd_rows_body<true>(ref, P, roots, log_n, sm);
+  else fwd_rows_body<false>(ref, P, roots, log_n, sm);
+}
+
+// Inverse row pass: GS stages u = 0..7 (pair distance 2^u) within 256-point rows.
+template <class B>
+__global__ void __launch_bounds__(256)
+    k_ntt_inv_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+  __shared__ uint64_t sm[kRowsPerCta * kRowPad];
+  LimbRef ref = b.r[blockIdx.y];
+  if (in_place) ref.src = ref.dst;
   const uint64_t q = __ldg(&pc[ref.prime].q), two_q = 2 * q;
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   const uint64_t* src = ref.src + (size_t)blockIdx.x * kRowsPerCta * kRow;
@@ -202,13 +231,14 @@ __global__ void __launch_bounds__(256)
 
 // Inverse column pass: GS stages u = 8..logN-1 on 2^LOGS-point columns, N^-1 fused into
 // the last stage, output in [0, q).
-template <int LOGS>
+template <int LOGS, class B>
 __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
-    k_ntt_inv_cols(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n) {
+    k_ntt_inv_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
   extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
-  const LimbRef ref = b.r[blockIdx.y];
+  LimbRef ref = b.r[blockIdx.y];
+  if (in_place) ref.src = ref.dst;
   const PrimeConst* P = pc + ref.prime;
   const uint64_t q = __ldg(&P->q), two_q = 2 * q;
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
@@ -265,7 +295,8 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
 }
 
 // Small transforms (logN <= 11): one CTA per limb, the limb in shared memory, radix-2.
-__global__ void k_ntt_small(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc,
+template <class B>
+__global__ void k_ntt_small(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
                             const ulonglong2* __restrict__ twf, const ulonglong2* __restrict__ twi, int log_n,
                             int inverse) {
   extern __shared__ uint64_t sm[];
@@ -282,7 +313,7 @@ __global__ void k_ntt_small(const __grid_constant__ LimbBatch b, const PrimeCons
       for (int bf = threadIdx.x; bf < half_n; bf += blockDim.x) {
         const int g = bf / t, k = bf % t;
         const int i0 = 2 * t * g + k;
-        ct_bf(sm[i0], sm[i0 + t], ldtw(roots, (1u << s) + g), q, two_q);
+        ct_bf<false>(sm[i0], sm[i0 + t], ldtw(roots, (1u << s) + g), q, two_q);
       }
       __syncthreads();
     }
@@ -310,49 +341,96 @@ __global__ void k_ntt_small(const __grid_constant__ LimbBatch b, const PrimeCons
 
 // ------------------------------------------------------------------------------------
 // Base conversion (ModUp digit lift, ModDown P -> Q, rescale last-prime lift).
-// One thread per coefficient: the source words are read once, the n_src values y_j stay
-// in registers, and each target is one 128-bit multiply-accumulate chain and one
-// reduction. Exact conversion (n_src > 1) subtracts e * S with the f64 estimate
-// e = floor(sum_j f64(y_j) * f64(1/s_j)), each product and sum rounded to nearest in source
-// order starting from 0 (crates/ckks-train-core/src/baseconv.rs:198-206, 221-230).
+// Each thread converts two coefficients (c and c + 256). The source words are read once;
+// y_j stays in registers split into 30-bit halves, so every product of a target's sum
+// sum_j y_j w_tj is one 32x32->64 multiply-add into one of four 64-bit accumulators
+// (A = lo*lo, B1 = lo*hi, B2 = hi*lo, C = hi*hi, each < 16 * 2^60), assembled into 128
+// bits and reduced once. The target records (weights pre-split, reduction constants)
+// are staged in shared memory. Exact conversion (n_src > 1) subtracts e * S with the f64
+// estimate e = floor(sum_j f64(y_j) * f64(1/s_j)), each product and sum rounded to nearest
+// in source order starting from the first product (crates/ckks-train-core/src/baseconv.rs:198-206).
 // ------------------------------------------------------------------------------------
 
-template <int NS>
+CKG_DEV void add128(uint64_t& hi, uint64_t& lo, uint64_t bhi, uint64_t blo) {
+  asm("add.cc.u64 %0, %0, %2;\n\taddc.u64 %1, %1, %3;" : "+l"(lo), "+l"(hi) : "l"(blo), "l"(bhi));
+}
+
+// (hi, lo) mod q with the reduction constants of a target record.
+CKG_DEV uint64_t reduce128_rec(uint64_t hi, uint64_t lo, const uint64_t* rec) {
+  const uint64_t q = rec[3];
+  const uint64_t a = csub(mul_shoup_lazy(hi, rec[4], rec[5], q), q);
+  const uint64_t b = csub(mul_shoup_lazy(lo, 1, rec[6], q), q);
+  return csub(a + b, q);
+}
+
+constexpr uint64_t kMask30 = (1ULL << 30) - 1;
+
+template <int NS, class B>
 __global__ void __launch_bounds__(256)
-    k_bconv(const __grid_constant__ ConvBatch cb, const PrimeConst* __restrict__ pc, int n) {
+    k_bconv(const __grid_constant__ B cb, const PrimeConst* __restrict__ pc, int n) {
+  __shared__ uint64_t sd[kMaxDst * (8 + kMaxSrc)];
   const ConvJob& job = cb.j[blockIdx.y];
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
   const int n_src = NS > 0 ? NS : cb.n_src;
+  const int dw = ConvLayout::dst_words(n_src);
   const uint64_t* tab = job.table;
-  uint64_t y[kMaxSrc];
-  double f = 0.0;
+  {
+    const uint64_t* dtab = tab + ConvLayout::kSrcWords * n_src;
+    for (int i = threadIdx.x; i < dw * job.n_dst; i += blockDim.x) sd[i] = __ldg(dtab + i);
+  }
+  const int c0 = blockIdx.x * 512 + threadIdx.x;
+  bool ok[2] = {c0 < n, c0 + 256 < n};
+  uint32_t ylo[2][kMaxSrc], yhi[2][kMaxSrc];
+  double f[2] = {0.0, 0.0};
 #pragma unroll
   for (int j = 0; j < kMaxSrc; ++j) {
     if (j < n_src) {
       const uint64_t* s = tab + ConvLayout::kSrcWords * j;
       const uint32_t p = (uint32_t)__ldg(s);
-      const uint64_t q = __ldg(&pc[p].q);
-      uint64_t x = job.src[j * job.src_stride + c];
-      x = add_mod(x, __ldg(s + 3), q);
-      const uint64_t yj = mul_shoup(x, __ldg(s + 1), __ldg(s + 2), q);
-      y[j] = yj;
-      const double prod = __dmul_rn(__ull2double_rn(yj), __longlong_as_double((long long)__ldg(s + 4)));
-      f = j == 0 ? prod : __dadd_rn(f, prod);
+      const uint64_t q = __ldg(&pc[p].q), h = __ldg(s + 3), w = __ldg(s + 1), ws = __ldg(s + 2);
+      const double inv = __longlong_as_double((long long)__ldg(s + 4));
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint64_t x = ok[u] ? job.src[j * job.src_stride + c0 + 256 * u] : 0;
+        const uint64_t yj = mul_shoup(add_mod(x, h, q), w, ws, q);
+        ylo[u][j] = (uint32_t)(yj & kMask30);
+        yhi[u][j] = (uint32_t)(yj >> 30);
+        const double prod = __dmul_rn(__ull2double_rn(yj), inv);
+        f[u] = j == 0 ? prod : __dadd_rn(f[u], prod);
+      }
     }
   }
-  const uint64_t e = n_src > 1 ? (uint64_t)floor(f) : 0;
-  const uint64_t* dtab = tab + ConvLayout::kSrcWords * n_src;
-  const int dw = ConvLayout::dst_words(n_src);
-  for (int t = 0; t < cb.n_dst; ++t) {
-    const uint64_t* d = dtab + dw * t;
-    const PrimeConst& P = pc[(uint32_t)__ldg(d)];
-    uint64_t hi = 0, lo = __ldg(d + 2);  // + (t - h_t)
-    mac128(hi, lo, e, __ldg(d + 1));      // + e * (t - S_t)
+  uint64_t e[2];
 #pragma unroll
-    for (int j = 0; j < kMaxSrc; ++j)
-      if (j < n_src) mac128(hi, lo, y[j], __ldg(d + 4 + j));
-    job.dst[t * job.dst_stride + c] = reduce128(hi, lo, P);
+  for (int u = 0; u < 2; ++u) e[u] = n_src > 1 ? (uint64_t)floor(f[u]) : 0;
+  __syncthreads();
+  for (int t = 0; t < job.n_dst; ++t) {
+    const uint64_t* d = sd + dw * t;
+    uint64_t A[2] = {0, 0}, B1[2] = {0, 0}, B2[2] = {0, 0}, Cc[2] = {0, 0};
+#pragma unroll
+    for (int j = 0; j < kMaxSrc; ++j) {
+      if (j < n_src) {
+        const uint64_t w = d[8 + j];
+        const uint32_t wl = (uint32_t)w, wh = (uint32_t)(w >> 32);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          A[u] += (uint64_t)ylo[u][j] * wl;
+          B1[u] += (uint64_t)ylo[u][j] * wh;
+          B2[u] += (uint64_t)yhi[u][j] * wl;
+          Cc[u] += (uint64_t)yhi[u][j] * wh;
+        }
+      }
+    }
+    const uint64_t negS = d[1], negH = d[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      uint64_t lo = A[u], hi = 0;
+      add128(hi, lo, B1[u] >> 34, B1[u] << 30);
+      add128(hi, lo, B2[u] >> 34, B2[u] << 30);
+      add128(hi, lo, Cc[u] >> 4, Cc[u] << 60);
+      add128(hi, lo, 0, e[u] * negS);  // e < 16, so e * (t - [S]_t) < 2^64
+      add128(hi, lo, 0, negH);
+      if (ok[u]) job.dst[t * job.dst_stride + c0 + 256 * u] = reduce128_rec(hi, lo, d);
+    }
   }
 }
 
@@ -364,21 +442,23 @@ __global__ void __launch_bounds__(256)
 // every digit word is read at perm[c] (hoisted rotation).
 // ------------------------------------------------------------------------------------
 
+template <class B>
 __global__ void __launch_bounds__(256)
-    k_inner_product(const __grid_constant__ IpBatch ib, const PrimeConst* __restrict__ pc, int log_n) {
+    k_inner_product(const __grid_constant__ B ib, const PrimeConst* __restrict__ pc, int log_n) {
   const int n = 1 << log_n;
   const IpJob& job = ib.j[blockIdx.z];
   const int i = blockIdx.y;  // limb of Q_l * P: 0..l data primes, l+1..l+k special
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  const int l = ib.level;
+  const int l = job.level;
+  if (c >= n || i > l + ib.k) return;
   const bool is_q = i <= l;
   const uint32_t prime = is_q ? i : (ib.L + 1) + (i - l - 1);
-  const int key_limb = is_q ? i : ib.key_q + (i - l - 1);
-  const size_t key_limbs = (size_t)(ib.key_q + ib.k);
+  const int key_limb = is_q ? i : job.key_q + (i - l - 1);
+  const size_t key_limbs = (size_t)(job.key_q + ib.k);
   const uint32_t src_c = job.perm ? __ldg(job.perm + c) : (uint32_t)c;
-  uint64_t bh = 0, bl = 0, ah = 0, al = 0;
-  for (int j = 0; j < ib.ndig; ++j) {
+  // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits)
+  uint64_t Ab = 0, B1b = 0, B2b = 0, Cb = 0, Aa = 0, B1a = 0, B2a = 0, Ca = 0;
+  for (int j = 0; j < job.ndig; ++j) {
     const int start = j * ib.alpha;
     const int end = min(start + ib.alpha, l + 1);
     uint64_t d;
@@ -388,22 +468,41 @@ __global__ void __launch_bounds__(256)
       const int t = i < start ? i : i - (end - start);
       d = job.conv[j][((size_t)t << log_n) + src_c];
     }
-    const uint64_t* kb = job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n;
-    const uint64_t* ka = job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n;
-    mac128(bh, bl, d, __ldcs(kb + c));
-    mac128(ah, al, d, __ldcs(ka + c));
+    const uint64_t kb = __ldcs(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c);
+    const uint64_t ka = __ldcs(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c);
+    const uint32_t dl = (uint32_t)(d & kMask30), dh = (uint32_t)(d >> 30);
+    const uint32_t bl = (uint32_t)(kb & kMask30), bh = (uint32_t)(kb >> 30);
+    const uint32_t al = (uint32_t)(ka & kMask30), ah = (uint32_t)(ka >> 30);
+    Ab += (uint64_t)dl * bl;
+    B1b += (uint64_t)dl * bh;
+    B2b += (uint64_t)dh * bl;
+    Cb += (uint64_t)dh * bh;
+    Aa += (uint64_t)dl * al;
+    B1a += (uint64_t)dl * ah;
+    B2a += (uint64_t)dh * al;
+    Ca += (uint64_t)dh * ah;
   }
   const PrimeConst& P = pc[prime];
-  job.out_b[((size_t)i << log_n) + c] = reduce128(bh, bl, P);
-  job.out_a[((size_t)i << log_n) + c] = reduce128(ah, al, P);
+  uint64_t lo = Ab, hi = 0;
+  add128(hi, lo, B1b >> 34, B1b << 30);
+  add128(hi, lo, B2b >> 34, B2b << 30);
+  add128(hi, lo, Cb >> 4, Cb << 60);
+  job.out_b[((size_t)i << log_n) + c] = reduce128(hi, lo, P);
+  lo = Aa;
+  hi = 0;
+  add128(hi, lo, B1a >> 34, B1a << 30);
+  add128(hi, lo, B2a >> 34, B2a << 30);
+  add128(hi, lo, Ca >> 4, Ca << 60);
+  job.out_a[((size_t)i << log_n) + c] = reduce128(hi, lo, P);
 }
 
 // ------------------------------------------------------------------------------------
 // ModDown / rescale finish (baseconv.rs:286-289, 505-510): out = (x - t) * c (+ add).
 // ------------------------------------------------------------------------------------
 
+template <class B>
 __global__ void __launch_bounds__(256)
-    k_finish(const __grid_constant__ FinBatch fb, const PrimeConst* __restrict__ pc, int n) {
+    k_finish(const __grid_constant__ B fb, const PrimeConst* __restrict__ pc, int n) {
   const FinRef& r = fb.r[blockIdx.y];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -418,8 +517,9 @@ __global__ void __launch_bounds__(256)
 // automorphism gather (poly.rs:255-262).
 // ------------------------------------------------------------------------------------
 
+template <class B>
 __global__ void __launch_bounds__(256)
-    k_binary(const __grid_constant__ BinBatch bb, const PrimeConst* __restrict__ pc, int n) {
+    k_binary(const __grid_constant__ B bb, const PrimeConst* __restrict__ pc, int n) {
   const BinRef& r = bb.r[blockIdx.y];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -454,8 +554,17 @@ __global__ void __launch_bounds__(256)
   r.dst[c] = v;
 }
 
+template <class B>
+__global__ void __launch_bounds__(256) k_gather(const __grid_constant__ B gb, int n) {
+  const GatherRef& r = gb.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  r.dst[c] = r.src[__ldg(r.perm + c)];
+}
+
+template <class B>
 __global__ void __launch_bounds__(256)
-    k_tensor(const __grid_constant__ TensorBatch tb, const PrimeConst* __restrict__ pc, int n) {
+    k_tensor(const __grid_constant__ B tb, const PrimeConst* __restrict__ pc, int n) {
   const TensorRef& r = tb.r[blockIdx.y];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
@@ -481,39 +590,76 @@ void set_smem(T* fn, int bytes) {
   cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-template <int LOGS>
-void launch_cols(bool inverse, const LimbBatch& b, const DevTables& d, cudaStream_t st) {
+template <int LOGS, class B>
+void launch_cols(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st) {
   const int smem = (1 << LOGS) * kCols * 8;
   const int threads = kCols * (1 << (LOGS / 2));
-  dim3 grid(kRow / kCols, b.count);
+  dim3 grid(kRow / kCols, count);
   if (!inverse) {
-    if (smem > 48 * 1024) set_smem(k_ntt_fwd_cols<LOGS>, smem);
-    k_ntt_fwd_cols<LOGS><<<grid, threads, smem, st>>>(b, d.prime, d.tw_fwd, d.log_n);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (smem > 48 * 1024) set_smem(k_ntt_fwd_cols<LOGS, B>, smem);
+    k_ntt_fwd_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_fwd, d.log_n, in_place);
   } else {
-    if (smem > 48 * 1024) set_smem(k_ntt_inv_cols<LOGS>, smem);
-    k_ntt_inv_cols<LOGS><<<grid, threads, smem, st>>>(b, d.prime, d.tw_inv, d.log_n);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (smem > 48 * 1024) set_smem(k_ntt_inv_cols<LOGS, B>, smem);
+    k_ntt_inv_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_inv, d.log_n, in_place);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+template <class B>
+void launch_cols_any(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st) {
+  switch (d.log_n - kRowLog) {
+    case 4: launch_cols<4>(inverse, b, count, d, in_place, st); break;
+    case 5: launch_cols<5>(inverse, b, count, d, in_place, st); break;
+    case 6: launch_cols<6>(inverse, b, count, d, in_place, st); break;
+    case 7: launch_cols<7>(inverse, b, count, d, in_place, st); break;
+    case 8: launch_cols<8>(inverse, b, count, d, in_place, st); break;
+    case 9: launch_cols<9>(inverse, b, count, d, in_place, st); break;
+    default: break;
   }
 }
 
-void launch_cols_any(bool inverse, const LimbBatch& b, const DevTables& d, cudaStream_t st) {
-  switch (d.log_n - kRowLog) {
-    case 4: launch_cols<4>(inverse, b, d, st); break;
-    case 5: launch_cols<5>(inverse, b, d, st); break;
-    case 6: launch_cols<6>(inverse, b, d, st); break;
-    case 7: launch_cols<7>(inverse, b, d, st); break;
-    case 8: launch_cols<8>(inverse, b, d, st); break;
-    case 9: launch_cols<9>(inverse, b, d, st); break;
-    default: break;
+// Both passes of a batched transform: src -> dst, then dst in place.
+template <class B>
+void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStream_t st) {
+  if (count == 0) return;
+  if (d.log_n <= 11) {
+    const int n = 1 << d.log_n;
+    const int threads = n / 2 < 512 ? (n / 2 < 32 ? 32 : n / 2) : 512;
+    k_ntt_small<B><<<dim3(1, count), threads, n * 8, st>>>(b, d.prime, d.tw_fwd, d.tw_inv, d.log_n, inverse);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return;
   }
+  const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), count);
+  if (!inverse) {
+    launch_cols_any(false, b, count, d, 0, st);
+    k_ntt_fwd_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.log_n, 1);
+  } else {
+    k_ntt_inv_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.log_n, 0);
+    launch_cols_any(true, b, count, d, 1, st);
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+template <class B>
+void bconv_launch(const DevTables& d, const B& cb, int count, int n_src, cudaStream_t st) {
+  const int n = 1 << d.log_n;
+  dim3 grid((n + 511) / 512, count);
+  switch (n_src) {
+    case 1: k_bconv<1, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 2: k_bconv<2, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 4: k_bconv<4, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 8: k_bconv<8, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    default: k_bconv<0, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+  }
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 }  // namespace
 
 // ------------------------------------------------------------------------------------
-// Host launchers (declared in launch.hpp). Lists longer than one launch's capacity are
-// split; every launch goes to stream `st` and is counted in g_launches.
+// Host launchers (declared in launch.hpp). By-value lists longer than one launch's
+// capacity are split; device-resident lists run in one launch. Every launch goes to
+// stream `st` and is counted in g_launches.
 // ------------------------------------------------------------------------------------
 
 std::atomic<uint64_t> g_launches{0};
@@ -523,64 +669,57 @@ void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse
   for (int off = 0; off < count; off += kMaxLimbs) {
     b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
     for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
-    if (d.log_n <= 11) {
-      const int n = 1 << d.log_n;
-      const int threads = n / 2 < 512 ? (n / 2 < 32 ? 32 : n / 2) : 512;
-      k_ntt_small<<<dim3(1, b.count), threads, n * 8, st>>>(b, d.prime, d.tw_fwd, d.tw_inv, d.log_n, inverse);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      continue;
-    }
-    const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), b.count);
-    if (!inverse) {
-      launch_cols_any(false, b, d, st);
-      for (int i = 0; i < b.count; ++i) b.r[i].src = b.r[i].dst;  // second pass in place on dst
-      k_ntt_fwd_rows<<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.log_n);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-    } else {
-      k_ntt_inv_rows<<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.log_n);
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      for (int i = 0; i < b.count; ++i) b.r[i].src = b.r[i].dst;
-      launch_cols_any(true, b, d, st);
-    }
+    ntt_passes(d, b, b.count, inverse, st);
   }
+}
+
+void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st) {
+  ntt_passes(d, LimbPtrs{count, 0, dev_refs}, count, inverse, st);
 }
 
 void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st) {
   ConvBatch cb;
   cb.n_src = n_src;
   cb.n_dst = n_dst;
-  const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxConv) {
     cb.count = count - off < kMaxConv ? count - off : kMaxConv;
-    for (int i = 0; i < cb.count; ++i) cb.j[i] = jobs[off + i];
-    dim3 grid((n + 255) / 256, cb.count);
-    switch (n_src) {
-      case 1: k_bconv<1><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      case 2: k_bconv<2><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      case 4: k_bconv<4><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      case 8: k_bconv<8><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
-      g_launches.fetch_add(1, std::memory_order_relaxed);
-      default: k_bconv<0><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
-      g_launches.fetch_add(1, std::memory_order_relaxed);
+    for (int i = 0; i < cb.count; ++i) {
+      cb.j[i] = jobs[off + i];
+      cb.j[i].n_dst = n_dst;
     }
+    bconv_launch(d, cb, cb.count, n_src, st);
   }
 }
 
-void launch_inner_product(const DevTables& d, const IpBatch& proto, const IpJob* jobs, int count,
-                          cudaStream_t st) {
-  IpBatch ib = proto;
+void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st) {
+  if (count) bconv_launch(d, ConvPtrs{count, n_src, 0, 0, dev_jobs}, count, n_src, st);
+}
+
+void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJob* jobs, int count, cudaStream_t st) {
+  IpBatch ib;
+  ib.alpha = alpha;
+  ib.L = L;
+  ib.k = k;
   const int n = 1 << d.log_n;
-  const int limbs = proto.level + 1 + proto.k;
   for (int off = 0; off < count; off += kMaxIp) {
     ib.count = count - off < kMaxIp ? count - off : kMaxIp;
-    for (int i = 0; i < ib.count; ++i) ib.j[i] = jobs[off + i];
-    dim3 grid((n + 255) / 256, limbs, ib.count);
-    k_inner_product<<<grid, 256, 0, st>>>(ib, d.prime, d.log_n);
+    int max_limbs = 0;
+    for (int i = 0; i < ib.count; ++i) {
+      ib.j[i] = jobs[off + i];
+      max_limbs = std::max(max_limbs, jobs[off + i].level + 1 + k);
+    }
+    k_inner_product<IpBatch><<<dim3((n + 255) / 256, max_limbs, ib.count), 256, 0, st>>>(ib, d.prime, d.log_n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+}
+
+void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const IpJob* dev_jobs, int count,
+                              int max_limbs, cudaStream_t st) {
+  if (!count) return;
+  const int n = 1 << d.log_n;
+  k_inner_product<IpPtrs><<<dim3((n + 255) / 256, max_limbs, count), 256, 0, st>>>(IpPtrs{count, alpha, L, k, dev_jobs},
+                                                                                  d.prime, d.log_n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {
@@ -589,9 +728,16 @@ void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream
   for (int off = 0; off < count; off += kMaxFin) {
     fb.count = count - off < kMaxFin ? count - off : kMaxFin;
     for (int i = 0; i < fb.count; ++i) fb.r[i] = refs[off + i];
-    k_finish<<<dim3((n + 255) / 256, fb.count), 256, 0, st>>>(fb, d.prime, n);
+    k_finish<FinBatch><<<dim3((n + 255) / 256, fb.count), 256, 0, st>>>(fb, d.prime, n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+}
+
+void launch_finish_ptr(const DevTables& d, const FinRef* dev_refs, int count, cudaStream_t st) {
+  if (!count) return;
+  const int n = 1 << d.log_n;
+  k_finish<FinPtrs><<<dim3((n + 255) / 256, count), 256, 0, st>>>(FinPtrs{count, 0, dev_refs}, d.prime, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st) {
@@ -601,9 +747,16 @@ void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cu
   for (int off = 0; off < count; off += kMaxBin) {
     bb.count = count - off < kMaxBin ? count - off : kMaxBin;
     for (int i = 0; i < bb.count; ++i) bb.r[i] = refs[off + i];
-    k_binary<<<dim3((n + 255) / 256, bb.count), 256, 0, st>>>(bb, d.prime, n);
+    k_binary<BinBatch><<<dim3((n + 255) / 256, bb.count), 256, 0, st>>>(bb, d.prime, n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+}
+
+void launch_binary_ptr(const DevTables& d, const BinRef* dev_refs, int count, int op, cudaStream_t st) {
+  if (!count) return;
+  const int n = 1 << d.log_n;
+  k_binary<BinPtrs><<<dim3((n + 255) / 256, count), 256, 0, st>>>(BinPtrs{count, op, dev_refs}, d.prime, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
@@ -618,15 +771,29 @@ void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, co
   }
 }
 
+void launch_gather_ptr(const DevTables& d, const GatherRef* dev_refs, int count, cudaStream_t st) {
+  if (!count) return;
+  const int n = 1 << d.log_n;
+  k_gather<GatherPtrs><<<dim3((n + 255) / 256, count), 256, 0, st>>>(GatherPtrs{count, 0, dev_refs}, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
 void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st) {
   TensorBatch tb;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxTensor) {
     tb.count = count - off < kMaxTensor ? count - off : kMaxTensor;
     for (int i = 0; i < tb.count; ++i) tb.r[i] = refs[off + i];
-    k_tensor<<<dim3((n + 255) / 256, tb.count), 256, 0, st>>>(tb, d.prime, n);
+    k_tensor<TensorBatch><<<dim3((n + 255) / 256, tb.count), 256, 0, st>>>(tb, d.prime, n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+}
+
+void launch_tensor_ptr(const DevTables& d, const TensorRef* dev_refs, int count, cudaStream_t st) {
+  if (!count) return;
+  const int n = 1 << d.log_n;
+  k_tensor<TensorPtrs><<<dim3((n + 255) / 256, count), 256, 0, st>>>(TensorPtrs{count, 0, dev_refs}, d.prime, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st) {

@@ -53,6 +53,8 @@ struct ConvJob {
   const uint64_t* table;
   uint64_t src_stride;
   uint64_t dst_stride;
+  int n_dst;             // targets of this job
+  int pad;
 };
 constexpr int kMaxConv = 32;
 struct ConvBatch {
@@ -65,16 +67,22 @@ struct ConvBatch {
 
 // Table record (u64 words):
 //   src block, 5 words per source j: prime, qhat_inv, qhat_inv_shoup, half_j, bits(1.0/s_j)
-//   dst block, (4 + n_src) words per target t: prime, (t - [S]_t), (t - [h]_t) mod t, pad, w_t0..w_t(n_src-1)
+//   dst block, (8 + n_src) words per target t: prime, (t - [S]_t), (t - [h]_t), t, [2^64]_t,
+//   its Shoup companion, floor(2^64/t), pad, then w_tj = [S/s_j]_t split into 30-bit halves
+//   (low half in bits 0..29, high half in bits 32..61)
 struct ConvLayout {
   static constexpr int kSrcWords = 5;
-  static __host__ __device__ int dst_words(int n_src) { return 4 + n_src; }
+  static __host__ __device__ int dst_words(int n_src) { return 8 + n_src; }
   static __host__ __device__ int size(int n_src, int n_dst) { return kSrcWords * n_src + dst_words(n_src) * n_dst; }
 };
 
 // Key-switch inner product of one level-l polynomial (module docs of keyswitch.cu).
 constexpr int kMaxDigits = 16;
 struct IpJob {
+  int level;                          // l
+  int ndig;                           // digits at level l
+  int key_q;                          // data limbs per key part (the key's max level + 1)
+  int pad;
   const uint64_t* in;                 // the switched polynomial (NTT form, l+1 limbs)
   const uint64_t* conv[kMaxDigits];   // digit j's converted limbs (targets, NTT form)
   const uint64_t* key;                // key base: part j, b/a, (L+1+k) limbs
@@ -85,13 +93,9 @@ struct IpJob {
 constexpr int kMaxIp = 16;
 struct IpBatch {
   int count;
-  int level;   // l
-  int ndig;    // digits at level l
   int alpha;   // primes per digit
   int L;       // max level of the parameters (special prime t has global index L+1+t)
   int k;       // special primes
-  int key_q;   // data limbs per key part (the key's max level + 1)
-  int pad;
   IpJob j[kMaxIp];
 };
 
@@ -138,6 +142,54 @@ constexpr int kMaxPrimes = 64;
 struct ScalarTable {
   uint64_t w[kMaxPrimes];
   uint64_t ws[kMaxPrimes];
+};
+
+// Work lists resident in device memory (the batched path): the same kernels read
+// items through a pointer instead of a by-value array.
+struct LimbPtrs {
+  int count;
+  int pad;
+  const LimbRef* r;
+};
+struct ConvPtrs {
+  int count;
+  int n_src;
+  int n_dst;
+  int pad;
+  const ConvJob* j;
+};
+struct IpPtrs {
+  int count;
+  int alpha;
+  int L;
+  int k;
+  const IpJob* j;
+};
+struct FinPtrs {
+  int count;
+  int pad;
+  const FinRef* r;
+};
+struct BinPtrs {
+  int count;
+  int op;
+  const BinRef* r;
+};
+struct TensorPtrs {
+  int count;
+  int pad;
+  const TensorRef* r;
+};
+// Gather through a per-limb permutation (NTT-form automorphism of many ciphertexts).
+struct GatherRef {
+  const uint64_t* src;
+  uint64_t* dst;
+  const uint32_t* perm;
+};
+struct GatherPtrs {
+  int count;
+  int pad;
+  const GatherRef* r;
 };
 
 }  // namespace ckg

@@ -21,14 +21,23 @@ struct DevTables {
 
 void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st);
 void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st);
-void launch_inner_product(const DevTables& d, const IpBatch& proto, const IpJob* jobs, int count,
-                          cudaStream_t st);
+void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJob* jobs, int count, cudaStream_t st);
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st);
 void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
                   const uint32_t* perm, cudaStream_t st);
 
 void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st);
+
+// The same kernels over work lists resident in device memory (one launch each).
+void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st);
+void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st);
+void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const IpJob* dev_jobs, int count,
+                              int max_limbs, cudaStream_t st);
+void launch_finish_ptr(const DevTables& d, const FinRef* dev_refs, int count, cudaStream_t st);
+void launch_binary_ptr(const DevTables& d, const BinRef* dev_refs, int count, int op, cudaStream_t st);
+void launch_tensor_ptr(const DevTables& d, const TensorRef* dev_refs, int count, cudaStream_t st);
+void launch_gather_ptr(const DevTables& d, const GatherRef* dev_refs, int count, cudaStream_t st);
 void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st);
 
 }  // namespace ckg

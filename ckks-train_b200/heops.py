@@ -151,6 +151,15 @@ def _declare(L):
     L.ckg_exact_product_scale.argtypes = [VP, C.c_uint32, C.c_double, C.POINTER(C.c_double)]
     L.ckg_matvec_plain.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
     L.ckg_matvec_enc.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
+    L.ckg_batch_create.argtypes = [VP, C.POINTER(VP)]
+    L.ckg_batch_destroy.argtypes = [VP]
+    L.ckg_batch_mul_relin_rescale.argtypes = [VP, VP, VP, C.POINTER(VP)]
+    L.ckg_batch_rotate.argtypes = [VP, VP, C.c_int32, C.POINTER(VP)]
+    L.ckg_batch_mul_plain_rescale.argtypes = [VP, VP, VP, C.POINTER(VP)]
+    for name in ("ckg_batch_run", "ckg_batch_capture_graph", "ckg_batch_launch_graph"):
+        getattr(L, name).argtypes = [VP]
+    L.ckg_batch_key_switches.argtypes = [VP]
+    L.ckg_batch_key_switches.restype = C.c_uint64
 
 
 def _check(code):
@@ -478,6 +487,12 @@ class CudaEvaluator:
         _check(lib().ckg_ct_upload(self.h, C.cast(VP(ptr), U64P), ncomp, level, scale, C.byref(h)))
         return Ciphertext(self, h)
 
+    def upload_pt_host_ptr(self, ptr, level, scale):
+        """upload_pt from a raw host address."""
+        h = VP()
+        _check(lib().ckg_pt_upload(self.h, C.cast(VP(ptr), U64P), level, scale, C.byref(h)))
+        return Plaintext(self, h, level, scale)
+
     def download_ct_async(self, ct, ptr):
         """Queues the copy of `ct` to the host address `ptr`; complete after ctx.sync()."""
         _check(lib().ckg_ct_download_async(ct.h, VP(ptr)))
@@ -579,3 +594,52 @@ class CudaEvaluator:
     def relin_lazy(self, s):
         """HeOps::relin_lazy (ops.rs:349-355)."""
         return self.relinearize(s) if self.config().lazy_relin else s
+
+
+class Batch:
+    """Many evaluator ops at uneven levels run as one launch sequence (include/ckg.h,
+    "batched execution"); results are returned at enqueue and valid after run()."""
+
+    def __init__(self, ev):
+        self.ev = ev
+        h = VP()
+        _check(lib().ckg_batch_create(ev.h, C.byref(h)))
+        self.h = h
+        self._keep = []
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_batch_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def _out(self, fn, *args):
+        h = VP()
+        _check(fn(self.h, *args, C.byref(h)))
+        return Ciphertext(self.ev, h)
+
+    def mul_relin_rescale(self, a, b):
+        self._keep += [a, b]
+        return self._out(lib().ckg_batch_mul_relin_rescale, a.h, b.h)
+
+    def rotate(self, a, steps):
+        self._keep.append(a)
+        return self._out(lib().ckg_batch_rotate, a.h, steps)
+
+    def mul_plain_rescale(self, a, p):
+        self._keep += [a, p]
+        return self._out(lib().ckg_batch_mul_plain_rescale, a.h, p.h)
+
+    def run(self):
+        _check(lib().ckg_batch_run(self.h))
+
+    def capture_graph(self):
+        _check(lib().ckg_batch_capture_graph(self.h))
+
+    def launch_graph(self):
+        _check(lib().ckg_batch_launch_graph(self.h))
+
+    def key_switches(self):
+        return lib().ckg_batch_key_switches(self.h)

@@ -206,6 +206,27 @@ CKG_API int ckg_matvec_plain(ckg_eval* ev, uint32_t d, uint32_t stride, const ck
 CKG_API int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* const* entries, const ckg_ct* x,
                    ckg_ct** out);
 
+/* ---- batched execution at uneven levels ----------------------------------------------
+ * A batch holds many ops on ciphertexts of any levels and runs them as one sequence of
+ * launches (one per stage for a chunk of ops), optionally captured once into a CUDA graph
+ * and replayed. Each op has the checks, errors and result of the evaluator op it stands
+ * for (HMult+relinearize+rescale = Evaluator::mul then ::rescale, evaluator.rs:463-510;
+ * rotate = evaluator.rs:534-540; mul_plain then rescale = evaluator.rs:262-271, 498-510),
+ * checked when the op is added; the outputs are returned at once and hold their values
+ * after run / launch_graph completes on the context's stream. Every run adds the ops'
+ * counts to the evaluator's OpCounter. This extends the reference's multi-stream
+ * matvec_enc_batch (crates/ckks-train-cuda/src/evaluator.rs:437-520) to any op mix. */
+typedef struct ckg_batch ckg_batch;
+CKG_API int ckg_batch_create(ckg_eval* ev, ckg_batch** out);
+CKG_API void ckg_batch_destroy(ckg_batch* b);
+CKG_API int ckg_batch_mul_relin_rescale(ckg_batch* b, const ckg_ct* x, const ckg_ct* y, ckg_ct** out);
+CKG_API int ckg_batch_rotate(ckg_batch* b, const ckg_ct* x, int32_t steps, ckg_ct** out);
+CKG_API int ckg_batch_mul_plain_rescale(ckg_batch* b, const ckg_ct* x, const ckg_pt* p, ckg_ct** out);
+CKG_API int ckg_batch_run(ckg_batch* b);
+CKG_API int ckg_batch_capture_graph(ckg_batch* b);
+CKG_API int ckg_batch_launch_graph(ckg_batch* b);
+CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
