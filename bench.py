@@ -243,6 +243,25 @@ class Mix:
         return h2d, d2h
 
 
+class PlainMix:
+    """The same uneven-level stream, one evaluator call per op (no batching)."""
+
+    def __init__(self, mix):
+        self.mix = mix
+        self.ks = mix.ks
+
+    def step(self):
+        ev, out = self.mix.S.ev, []
+        for kind, a, extra, steps in self.mix.inputs:
+            if kind == "mul":
+                out.append(ev.rescale(ev.mul(a, extra)))
+            elif kind == "rot":
+                out.append(ev.rotate(a, steps))
+            else:
+                out.append(ev.rescale(ev.mul_plain(a, extra)))
+        return out
+
+
 class Plain:
     """The plain per-op path: 128 x (HMult+relin+rescale) + 128 rotations at 24 limbs."""
 
@@ -263,6 +282,19 @@ class Plain:
 
 # ---- timing ---------------------------------------------------------------------------
 
+def max_over_ranks(dist, ms, device="cuda"):
+    """The slowest rank's time: every rank's device-measured milliseconds, max-reduced."""
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_stream(rank, count=MIX_OPS):
+    """The op stream of one rank: independent seeded ciphertexts per rank (weak scaling)."""
+    return mix_ops(20261203 + rank, count)
+
+
 def timed(torch, ctx, fn, steps, warmup, dist=None):
     for _ in range(warmup):
         fn()
@@ -281,9 +313,7 @@ def timed(torch, ctx, fn, steps, warmup, dist=None):
     torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(dist, ms)
     return ms, extra
 
 
@@ -321,20 +351,32 @@ def ntt_roofline(torch, S, peaks, limbs=768):
 
 # ---- CPU baseline / reference arm ------------------------------------------------------
 
-def cpu_sample(threads, budget_s=20.0, seed=20261203):
+class CpuPath:
     """The oracle's CPU evaluator (the reference's CPU path restated, OpenMP over the units
-    of its `parallel` feature) on ops drawn from the same mix, keys from its own key
-    generator, until the time budget is used."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    O.set_threads(threads)
-    P = O.Params.from_bits(LOG_N, Q_BITS, P_BITS, 50, DNUM)
-    kg = O.KeyGenerator(P, 5)
-    rk = kg.relin_key()
-    ops = mix_ops(seed, 64)
-    elts = sorted({O.galois_elt(P.n, s) for kind, _, s in ops if kind == "rot"})[:4]
-    gk = {e: kg.galois_key(e) for e in elts}
-    ev = O.Evaluator(P, rk, gk)
+    of its `parallel` feature) with keys from its own key generator (relinearization key
+    and the Galois keys of the first rotation steps of the mix)."""
+
+    def __init__(self, threads, seed=20261203):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        self.O = O
+        O.set_threads(threads)
+        self.P = O.Params.from_bits(LOG_N, Q_BITS, P_BITS, 50, DNUM)
+        kg = O.KeyGenerator(self.P, 5)
+        rk = kg.relin_key()
+        self.ops = mix_ops(seed, 256)
+        elts = sorted({O.galois_elt(self.P.n, s) for kind, _, s in self.ops if kind == "rot"})[:4]
+        self.gk = {e: kg.galois_key(e) for e in elts}
+        self.ev = O.Evaluator(self.P, rk, self.gk)
+        self.pos = 0
+
+
+def cpu_sample(threads, budget_s=20.0, seed=20261203, path=None):
+    """Key switches per second of the CPU path on ops drawn in order from the same mix
+    (rotations whose Galois key was not generated are skipped), until the budget is used."""
+    cp = path or CpuPath(threads, seed)
+    O, P, ev, gk = cp.O, cp.P, cp.ev, cp.gk
+    ops = cp.ops[cp.pos:] + cp.ops[:cp.pos]
     ks, t0 = 0, time.perf_counter()
     for kind, level, steps in ops:
         if kind == "rot" and O.galois_elt(P.n, steps) not in gk:
@@ -348,6 +390,7 @@ def cpu_sample(threads, budget_s=20.0, seed=20261203):
             ks += 1
         else:
             ev.rescale(ev.mul_plain(a, P.random_q(7, level), SCALE))
+        cp.pos = (cp.pos + 1) % len(cp.ops)
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
@@ -383,9 +426,12 @@ def main():
             return
         threads = os.cpu_count() or 1
         vals, sample = [], ""
-        budget = max(5.0, 60.0 / max(args.steps, 1))
+        path = CpuPath(threads)
+        budget = max(4.0, 40.0 / max(args.steps, 1))
+        for _ in range(args.warmup):
+            cpu_sample(threads, budget_s=1.0, path=path)
         for _ in range(max(args.steps, 1)):
-            v, sample = cpu_sample(threads, budget_s=budget)
+            v, sample = cpu_sample(threads, budget_s=budget, path=path)
             vals.append(v)
         v = float(np.mean(vals))
         print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 3), "unit": unit,
@@ -420,7 +466,7 @@ def main():
             P.step()
         S.ctx.sync()
         return
-    mix = Mix(S, mix_ops(20261203 + rank, args.ops), keep_host=not args.no_e2e and args.profile is None)
+    mix = Mix(S, rank_stream(rank, args.ops), keep_host=not args.no_e2e and args.profile is None)
     l0 = ckg.launch_count()
     mix.batch.capture_graph()
     launches_per_step = ckg.launch_count() - l0
@@ -445,10 +491,14 @@ def main():
         P = Plain(S)
         ms_p, _ = timed(torch, S.ctx, P.step, 2, 1, dist)
         pv = P.ks * 2 * world / (ms_p * 1e-3)
+        PM = PlainMix(mix)
+        ms_m, _ = timed(torch, S.ctx, PM.step, 2, 1, dist)
+        pm = PM.ks * 2 * world / (ms_m * 1e-3)
         plain = {"value": round(pv, 2), "unit": unit,
                  "workload": "128 ciphertexts at 24 limbs: 128 x (HMult+relin+rescale) + 128 rotations, "
                              "one evaluator call per op",
-                 "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2)}
+                 "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
+                 "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
     roof = ntt_roofline(torch, S, peaks)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -309,12 +309,12 @@ void Batch::issue() {
                              S->ip_max_limbs, c.stream);
     if (S->intt_p.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_p), S->intt_p.count, true, c.stream);
     launch_bconv_ptr(c.dt, (const ConvJob*)at(S->md_conv), S->md_conv.count, (int)c.k, c.stream);
-    if (S->fwd_md.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->fwd_md), S->fwd_md.count, false, c.stream);
-    launch_finish_ptr(c.dt, (const FinRef*)at(S->fin_ks), S->fin_ks.count, c.stream);
+    launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_md), (const FinRef*)at(S->fin_ks), S->fin_ks.count,
+                          c.stream);
     if (S->intt_last.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_last), S->intt_last.count, true, c.stream);
     launch_bconv_ptr(c.dt, (const ConvJob*)at(S->rs_conv), S->rs_conv.count, 1, c.stream);
-    if (S->fwd_rs.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->fwd_rs), S->fwd_rs.count, false, c.stream);
-    launch_finish_ptr(c.dt, (const FinRef*)at(S->fin_rs), S->fin_rs.count, c.stream);
+    launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_rs), (const FinRef*)at(S->fin_rs), S->fin_rs.count,
+                          c.stream);
   }
 }
 

@@ -278,8 +278,7 @@ void rescale_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l
                            c.qlinv[l][j].second, j, 0});
     }
   }
-  ntt_limbs(c, refs, false);
-  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+  launch_ntt_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
 }
 
 void mod_down_many(Context& c, const std::vector<ModDownJob>& jobs, uint32_t l) {
@@ -305,8 +304,7 @@ void mod_down_many(Context& c, const std::vector<ModDownJob>& jobs, uint32_t l) 
                            jobs[i].add_perm, jobs[i].out + j * N, c.pinv[j].first, c.pinv[j].second, j, 0});
     }
   }
-  ntt_limbs(c, refs, false);
-  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+  launch_ntt_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
 }
 
 size_t conv_limbs(const Context& c, uint32_t l) {
@@ -433,8 +431,7 @@ void ks_tail(Context& c, const std::vector<KsJob>& jobs, uint32_t l, const std::
                              c.pinv[j].second, j, 0});
       }
     }
-  ntt_limbs(c, refs, false);
-  launch_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+  launch_ntt_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
 }
 
 void ks_group(Context& c, const std::vector<KsJob>& jobs, uint32_t l, uint64_t* scratch) {

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <vector>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "launch.hpp"
@@ -35,19 +37,36 @@ constexpr int kCols = 16;           // columns per CTA in the column pass
 constexpr int kRowsPerCta = 16;     // rows per CTA in the row pass
 constexpr int kRowPad = kRow + kRow / 16;  // padded row stride in shared memory
 
-// Harvey butterfly. With LAZY (primes below 2^58) x is not brought back below 2q: values
-// grow by at most 2q per stage from [0, q), so all 16 stages of N = 2^16 stay below
-// 33q < 2^64 and one reduction at the end suffices.
+// High 64 bits of a * b from three of the four 32x32 partial products: the dropped low
+// product and carries make it at most 2 below the exact value.
+CKG_DEV uint64_t mulhi_approx(uint64_t a, uint64_t b) {
+  const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+  const uint64_t mid = (uint64_t)__umulhi(a0, b1) + __umulhi(a1, b0);
+  return (uint64_t)a1 * b1 + mid;
+}
+
+// Harvey butterfly. Exact form (any prime < 2^60): values in [0, 4q) between stages. LAZY
+// form (primes below 2^57): the Shoup quotient comes from mulhi_approx, so t = w*y mod q
+// lies in [0, 4q), and x is never brought back down: values grow by at most 4q per stage
+// from [0, q), so all 16 stages of N = 2^16 stay below 65q < 2^64 and one reduction at the
+// end suffices.
 template <bool LAZY>
 CKG_DEV void ct_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
-  uint64_t xr = LAZY ? x : csub(x, two_q);
-  uint64_t t = mul_shoup_lazy(y, w.x, w.y, q);
-  x = xr + t;
-  y = xr + two_q - t;
+  if (LAZY) {
+    const uint64_t t = y * w.x - mulhi_approx(y, w.y) * q;
+    const uint64_t xr = x;
+    x = xr + t;
+    y = xr + 2 * two_q - t;
+  } else {
+    const uint64_t xr = csub(x, two_q);
+    const uint64_t t = mul_shoup_lazy(y, w.x, w.y, q);
+    x = xr + t;
+    y = xr + two_q - t;
+  }
 }
 
 // Primes below this bound take the lazy forward path.
-constexpr uint64_t kLazyBound = 1ULL << 58;
+constexpr uint64_t kLazyBound = 1ULL << 57;
 
 CKG_DEV void gs_bf(uint64_t& x, uint64_t& y, const ulonglong2 w, uint64_t q, uint64_t two_q) {
   uint64_t s = x + y;
@@ -102,7 +121,7 @@ CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roo
 }
 
 template <int LOGS, class B>
-__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
     k_ntt_fwd_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
                    const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
@@ -115,13 +134,15 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
 }
 
 // Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
-template <bool LAZY>
-CKG_DEV void fwd_rows_body(const LimbRef& ref, const PrimeConst* P, const ulonglong2* roots, int log_n, uint64_t* sm) {
+// `store(i, col, v)` receives the reduced value of row (CTA row i, column col).
+template <bool LAZY, class Store>
+CKG_DEV void fwd_rows_body(const uint64_t* base, const PrimeConst* P, const ulonglong2* roots, int log_n,
+                           uint64_t* sm, Store store) {
   const uint64_t q = __ldg(&P->q), two_q = 2 * q;
   const int s0 = log_n - kRowLog;
   const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
   const uint32_t row = blockIdx.x * kRowsPerCta + rr;
-  const uint64_t* src = ref.src + (size_t)row * kRow;
+  const uint64_t* src = base + (size_t)row * kRow;
   uint64_t x[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) x[j] = src[t + 16 * j];
@@ -159,27 +180,51 @@ CKG_DEV void fwd_rows_body(const LimbRef& ref, const PrimeConst* P, const ulongl
     for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = csub(csub(x[j], two_q), q);
   }
   __syncthreads();
-  uint64_t* dst = ref.dst + (size_t)blockIdx.x * kRowsPerCta * kRow;
 #pragma unroll
-  for (int i = 0; i < kRowsPerCta; ++i) dst[i * kRow + threadIdx.x] = sm[i * kRowPad + pad_idx(threadIdx.x)];
+  for (int i = 0; i < kRowsPerCta; ++i) store(i, threadIdx.x, sm[i * kRowPad + pad_idx(threadIdx.x)]);
 }
 
 template <class B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_ntt_fwd_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
                    const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
-  LimbRef ref = b.r[blockIdx.y];
-  if (in_place) ref.src = ref.dst;
+  const LimbRef ref = b.r[blockIdx.y];
+  const uint64_t* src = in_place ? ref.dst : ref.src;
   const PrimeConst* P = pc + ref.prime;
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
-  if (__ldg(&P->q) < kLazyBound) fwd_rows_body<true>(ref, P, roots, log_n, sm);
-  else fwd_rows_body<false>(ref, P, roots, log_n, sm);
+  uint64_t* dst = ref.dst + (size_t)blockIdx.x * kRowsPerCta * kRow;
+  auto store = [&](int i, int col, uint64_t v) { dst[i * kRow + col] = v; };
+  if (__ldg(&P->q) < kLazyBound) fwd_rows_body<true>(src, P, roots, log_n, sm, store);
+  else fwd_rows_body<false>(src, P, roots, log_n, sm, store);
+}
+
+// The row pass of the forward NTT of t (its column pass already run in place) fused with
+// the ModDown / rescale finish: out = (x - NTT(t)) * c (+ add[perm]), so NTT(t) is never
+// written back (crates/ckks-train-core/src/baseconv.rs:286-289, 505-510).
+template <class B>
+__global__ void __launch_bounds__(256, 4)
+    k_ntt_fwd_rows_finish(const __grid_constant__ B fb, const PrimeConst* __restrict__ pc,
+                          const ulonglong2* __restrict__ tw, int log_n) {
+  __shared__ uint64_t sm[kRowsPerCta * kRowPad];
+  const FinRef& r = fb.r[blockIdx.y];
+  const PrimeConst* P = pc + r.prime;
+  const uint64_t q = __ldg(&P->q);
+  const ulonglong2* roots = tw + ((size_t)r.prime << log_n);
+  const size_t base = (size_t)blockIdx.x * kRowsPerCta * kRow;
+  auto store = [&](int i, int col, uint64_t v) {
+    const size_t g = base + i * kRow + col;
+    uint64_t o = mul_shoup(sub_mod(r.x[g], v, q), r.c, r.c_s, q);
+    if (r.add) o = add_mod(o, r.add[r.add_perm ? __ldg(r.add_perm + g) : g], q);
+    r.out[g] = o;
+  };
+  if (q < kLazyBound) fwd_rows_body<true>(r.t, P, roots, log_n, sm, store);
+  else fwd_rows_body<false>(r.t, P, roots, log_n, sm, store);
 }
 
 // Inverse row pass: GS stages u = 0..7 (pair distance 2^u) within 256-point rows.
 template <class B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_ntt_inv_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
                    const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
@@ -232,7 +277,7 @@ __global__ void __launch_bounds__(256)
 // Inverse column pass: GS stages u = 8..logN-1 on 2^LOGS-point columns, N^-1 fused into
 // the last stage, output in [0, q).
 template <int LOGS, class B>
-__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)))
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
     k_ntt_inv_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
                    const ulonglong2* __restrict__ tw, int log_n, int in_place) {
   constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
@@ -446,9 +491,13 @@ template <class B>
 __global__ void __launch_bounds__(256)
     k_inner_product(const __grid_constant__ B ib, const PrimeConst* __restrict__ pc, int log_n) {
   const int n = 1 << log_n;
-  const IpJob& job = ib.j[blockIdx.z];
-  const int i = blockIdx.y;  // limb of Q_l * P: 0..l data primes, l+1..l+k special
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  // By-value lists: grid (coefficient blocks, limbs, jobs). Device-resident lists (the
+  // batched path, jobs sorted by key): grid (jobs, coefficient blocks, limbs), so the jobs
+  // that share a key read the same key block back to back and it is served from L2.
+  constexpr bool kJobFast = std::is_same<B, IpPtrs>::value;
+  const IpJob& job = ib.j[kJobFast ? blockIdx.x : blockIdx.z];
+  const int i = kJobFast ? blockIdx.z : blockIdx.y;  // limb of Q_l * P: 0..l data, l+1..l+k special
+  const int c = (kJobFast ? blockIdx.y : blockIdx.x) * blockDim.x + threadIdx.x;
   const int l = job.level;
   if (c >= n || i > l + ib.k) return;
   const bool is_q = i <= l;
@@ -717,8 +766,47 @@ void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const
                               int max_limbs, cudaStream_t st) {
   if (!count) return;
   const int n = 1 << d.log_n;
-  k_inner_product<IpPtrs><<<dim3((n + 255) / 256, max_limbs, count), 256, 0, st>>>(IpPtrs{count, alpha, L, k, dev_jobs},
+  k_inner_product<IpPtrs><<<dim3(count, (n + 255) / 256, max_limbs), 256, 0, st>>>(IpPtrs{count, alpha, L, k, dev_jobs},
                                                                                   d.prime, d.log_n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {
+  if (d.log_n <= 11) {  // small transforms: separate NTT and finish
+    std::vector<LimbRef> lr(count);
+    for (int i = 0; i < count; ++i) lr[i] = LimbRef{refs[i].t, const_cast<uint64_t*>(refs[i].t), refs[i].prime, 0};
+    launch_ntt(d, lr.data(), count, false, st);
+    launch_finish(d, refs, count, st);
+    return;
+  }
+  LimbBatch b;
+  FinBatch fb;
+  const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), 1);
+  for (int off = 0; off < count; off += kMaxFin) {
+    const int cnt = count - off < kMaxFin ? count - off : kMaxFin;
+    b.count = cnt;
+    fb.count = cnt;
+    for (int i = 0; i < cnt; ++i) {
+      fb.r[i] = refs[off + i];
+      b.r[i] = LimbRef{refs[off + i].t, const_cast<uint64_t*>(refs[off + i].t), refs[off + i].prime, 0};
+    }
+    launch_cols_any(false, b, cnt, d, 1, st);
+    k_ntt_fwd_rows_finish<FinBatch><<<dim3(rgrid.x, cnt), 256, 0, st>>>(fb, d.prime, d.tw_fwd, d.log_n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const FinRef* dev_fin, int count,
+                           cudaStream_t st) {
+  if (!count) return;
+  if (d.log_n <= 11) {
+    launch_ntt_ptr(d, dev_cols, count, false, st);
+    launch_finish_ptr(d, dev_fin, count, st);
+    return;
+  }
+  launch_cols_any(false, LimbPtrs{count, 0, dev_cols}, count, d, 1, st);
+  k_ntt_fwd_rows_finish<FinPtrs><<<dim3((1 << d.log_n) / (kRow * kRowsPerCta), count), 256, 0, st>>>(
+      FinPtrs{count, 0, dev_fin}, d.prime, d.tw_fwd, d.log_n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

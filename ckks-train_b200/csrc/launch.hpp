@@ -23,6 +23,11 @@ void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse
 void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st);
 void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJob* jobs, int count, cudaStream_t st);
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
+// Forward NTT of each FinRef's t (in place for the column pass) fused with its finish:
+// out = (x - NTT(t)) * c (+ add). `dev_cols` holds the matching in-place LimbRefs of t.
+void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
+void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const FinRef* dev_fin, int count,
+                           cudaStream_t st);
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st);
 void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
                   const uint32_t* perm, cudaStream_t st);
