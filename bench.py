@@ -47,6 +47,11 @@ MIX_OPS = 512
 MIX_LIMBS = (4, 24)
 PLAIN_CTS = 128
 PLAIN_LEVEL = 23
+SERVE_OWNERS = 32
+SERVE_D = 64                 # BSGS mat-vec diagonals: baby 8, giant 8
+SERVE_BUDGET = 24 << 30      # HBM bytes for cached keys + queued work: about half the owners
+SERVE_REQUESTS = 1000
+SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
 
 
 def load_package():
@@ -282,6 +287,120 @@ class Plain:
 
 # ---- timing ---------------------------------------------------------------------------
 
+class Serving:
+    """The serving loop under Poisson arrivals from SERVE_OWNERS key owners. Each owner has
+    its own relinearization key and the 14 Galois keys of a 64-diagonal BSGS mat-vec (steps
+    1..7 and 8..56 by 8): 15 keys of 96 MiB (synthetic uniform key material), 45 GiB in all,
+    registered into pinned host memory; the server caches device copies LRU within
+    SERVE_BUDGET. Requests: 5/8 single ops (half HMult+relin+rescale, half rotation by one
+    of the owner's steps) and 3/8 64x64 plaintext mat-vecs, on the owner's resident inputs
+    (24, 18, 12 and 6 limbs; mat-vecs at 24 or 12 limbs against one shared 64-diagonal
+    matrix per level)."""
+
+    def __init__(self, S, owners=SERVE_OWNERS, budget=SERVE_BUDGET, seed=7):
+        ckg, torch = S.ckg, S.torch
+        self.S, self.owners = S, owners
+        self.rng = np.random.default_rng(seed)
+        ctx = S.ctx
+        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=S.ev)
+        bg = 8
+        self.steps = [k for k in range(1, bg)] + [bg * k for k in range(1, SERVE_D // bg)]
+        shape = (DNUM, 2, len(ctx.q) + ctx.k, ctx.n)
+        qcol = S.q_all.view(1, 1, -1, 1)
+        t0 = time.time()
+        for _ in range(owners):
+            o = self.srv.add_owner()
+            for e in [0] + [galois_elt(ctx.n, st) for st in self.steps]:
+                t = S.uniform(shape, qcol)
+                self.srv.add_key_device(o, t.data_ptr(), shape, e)
+                del t
+        self.register_s = time.time() - t0
+        self.key_bytes = owners * (1 + len(self.steps)) * int(np.prod(shape)) * 8
+        self.inputs = [[S.ct(l)[0] for l in (23, 17, 11, 5)] for _ in range(owners)]
+        self.diag = {l: [S.pt(l)[0] for _ in range(SERVE_D)] for l in (23, 11)}
+
+    def request(self):
+        o = int(self.rng.integers(self.owners))
+        r = self.rng.random()
+        ins = self.inputs[o]
+        if r < 5 / 16:
+            a = ins[int(self.rng.integers(4))]
+            return lambda: self.srv.submit_mul(o, a, a)
+        if r < 10 / 16:
+            a = ins[int(self.rng.integers(4))]
+            st = self.steps[int(self.rng.integers(len(self.steps)))]
+            return lambda: self.srv.submit_rotate(o, a, st)
+        i = int(self.rng.integers(2))
+        x, lvl = ins[0 if i == 0 else 2], (23, 11)[i]
+        return lambda: self.srv.submit_matvec(o, SERVE_D, 1, self.diag[lvl], x)
+
+    def run(self, count, rate=None):
+        """Submits `count` requests (all at once, or Poisson at `rate` per second) while a
+        collector takes the results; returns per-request (submitted, completed) in us."""
+        reqs = [self.request() for _ in range(count)]
+        gaps = self.rng.exponential(1.0 / rate, count) if rate else np.zeros(count)
+        ids, times, lag = [], [], [0.0]
+        done = threading.Event()
+
+        def collect():
+            i = 0
+            while i < count:
+                if i >= len(ids):
+                    time.sleep(0.0002)
+                    continue
+                code, _, t = self.srv.result_times(ids[i], -1)
+                assert code == 0, f"served request failed with status {code}"
+                times.append(t)
+                i += 1
+            done.set()
+
+        th = threading.Thread(target=collect, daemon=True)
+        th.start()
+        start = time.perf_counter()
+        due = 0.0
+        for k in range(count):
+            due += gaps[k]
+            now = time.perf_counter() - start
+            if due > now:
+                time.sleep(due - now)
+            lag[0] = max(lag[0], time.perf_counter() - start - due)
+            ids.append(reqs[k]())
+        done.wait()
+        th.join()
+        return np.array([(t[0], t[2]) for t in times]), lag[0]
+
+    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD):
+        self.run(96)  # warm-up: Galois permutations, pools, first key uploads
+        sat, _ = self.run(min(400, requests))
+        capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6)
+        st0 = self.srv.stats()
+        rate = load * capacity
+        t, lag = self.run(requests, rate)
+        st = self.srv.stats()
+        lat = (t[:, 1] - t[:, 0]) * 1e-3
+        span = (t[:, 1].max() - t[:, 0].min()) * 1e-6
+        d = {k: st[k] - st0[k] for k in ("batches", "multi_owner_batches", "key_hits", "key_misses",
+                                          "key_evictions", "key_upload_bytes", "budget_waits")}
+        return {"requests": requests, "owners": self.owners,
+                "mix": "5/8 single ops (HMult+relin+rescale | rotation), 3/8 64x64 BSGS plaintext mat-vec; "
+                       "bootstrap requests not served yet",
+                "capacity_req_s": round(capacity, 2), "offered_req_s": round(rate, 2),
+                "throughput_req_s": round(requests / span, 2),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "mean_ms": round(float(lat.mean()), 3), "max_submit_lag_ms": round(lag * 1e3, 3),
+                "hbm_budget_gib": round(self.srv.stats()["hbm_budget"] / 2 ** 30, 2),
+                "key_set_gib": round(self.key_bytes / 2 ** 30, 2),
+                "peak_device_gib": round(st["peak_device_bytes"] / 2 ** 30, 2),
+                "key_hit_rate": round(d["key_hits"] / max(1, d["key_hits"] + d["key_misses"]), 3),
+                "key_upload_gib": round(d["key_upload_bytes"] / 2 ** 30, 2),
+                "batches": d["batches"], "multi_owner_batches": d["multi_owner_batches"],
+                "key_evictions": d["key_evictions"], "budget_waits": d["budget_waits"],
+                "register_s": round(self.register_s, 1)}
+
+    def close(self):
+        self.srv.close()
+
+
 def max_over_ranks(dist, ms, device="cuda"):
     """The slowest rank's time: every rank's device-measured milliseconds, max-reduced."""
     import torch
@@ -407,6 +526,10 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ops", type=int, default=MIX_OPS, help="ops of the batched stream (smaller for profiling)")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
+    ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
+    ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
     ap.add_argument("--profile", default=None, choices=["batch", "plain"],
                     help="run the set-up and `warmup` + 1 step of one path, print nothing (for ncu)")
     args = ap.parse_args()
@@ -460,6 +583,13 @@ def main():
         pass
 
     S = Setup(ckg, torch, local)
+    if args.serve_only:
+        sv = Serving(S, owners=args.serve_owners)
+        out = sv.measure(args.serve_requests)
+        sv.close()
+        if rank == 0:
+            print(json.dumps({"serving": out}))
+        return
     if args.profile == "plain":
         P = Plain(S)
         for _ in range(args.warmup + 1):
@@ -500,6 +630,12 @@ def main():
                  "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
     roof = ntt_roofline(torch, S, peaks)
+    serving = None
+    if not args.no_serve:
+        mix.batch = None
+        sv = Serving(S, owners=args.serve_owners)
+        serving = sv.measure(args.serve_requests)
+        sv.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -512,7 +648,7 @@ def main():
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
                 "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
-                "cpu_baseline": cpu, "clocks": clk.summary()}
+                "serving": serving, "cpu_baseline": cpu, "clocks": clk.summary()}
         print(json.dumps(line))
     mix.batch = None
     S.ctx.sync()

@@ -7,6 +7,7 @@ hyphen, so loaders register it by path; see ``load_package`` in bench.py).
 from .heops import (  # noqa: F401
     BSGS,
     Batch,
+    Cancelled,
     HOIST,
     LAZY_RELIN,
     COUNTER_FIELDS,
@@ -24,7 +25,9 @@ from .heops import (  # noqa: F401
     NoLevelsLeft,
     OutOfMemory,
     Plaintext,
+    SERVER_STATS,
     ScaleMismatch,
+    Server,
     Timeout,
     build,
     launch_count,

@@ -57,55 +57,77 @@ Batch::~Batch() {
   for (auto* s : chunks_) delete s;
 }
 
-Ct Batch::mul_relin_rescale(const Ct& a, const Ct& b) {  // evaluator.rs:463-510
+Ct Batch::mul_relin_rescale(const Ct& a, const Ct& b, Evaluator* ev) {  // evaluator.rs:463-510
   if (built_) throw Error(ST_INVALID_PARAMS, "batch already built: create a new batch to add ops");
-  ev_->check_mul_operands(a, b);
-  const DevKey& rk = ev_->relin_key_checked();
+  ev = ev ? ev : ev_;
+  if (ev->ctx() != ctx_) throw Error(ST_INVALID_PARAMS, "evaluator is not over this batch's context");
+  ev->check_mul_operands(a, b);
+  const DevKey& rk = ev->relin_key_checked();
   const uint32_t l = a->level;
   const double s = a->scale * b->scale;
   Item it;
   it.kind = MUL;
+  it.ev = ev;
   it.a = a;
   it.b = b;
   it.key = &rk;
-  it.out = ev_->new_ct(2, l - 1, s / (double)ctx_->primes[l]);
+  it.out = ev->new_ct(2, l - 1, s / (double)ctx_->primes[l]);
   items_.push_back(it);
   return it.out;
 }
 
-Ct Batch::rotate(const Ct& a, int32_t steps) {  // evaluator.rs:534-540
+Ct Batch::rotate(const Ct& a, int32_t steps, Evaluator* ev) {  // evaluator.rs:534-540
   if (built_) throw Error(ST_INVALID_PARAMS, "batch already built: create a new batch to add ops");
-  ev_->check_galois_input(a);
-  auto e = ev_->rotation_elt(steps);
+  ev = ev ? ev : ev_;
+  if (ev->ctx() != ctx_) throw Error(ST_INVALID_PARAMS, "evaluator is not over this batch's context");
+  ev->check_galois_input(a);
+  auto e = ev->rotation_elt(steps);
   Item it;
   it.kind = ROT;
+  it.ev = ev;
   it.a = a;
   if (!e) {
     it.trivial = true;
     it.out = a;
   } else {
     it.elt = *e;
-    it.key = &ev_->galois_key(*e);
-    it.out = ev_->new_ct(2, a->level, a->scale);
+    it.key = &ev->galois_key(*e);
+    it.out = ev->new_ct(2, a->level, a->scale);
   }
   items_.push_back(it);
   return it.out;
 }
 
-Ct Batch::mul_plain_rescale(const Ct& a, const Pt& p) {  // evaluator.rs:262-271, 498-510
+Ct Batch::mul_plain_rescale(const Ct& a, const Pt& p, Evaluator* ev) {  // evaluator.rs:262-271, 498-510
   if (built_) throw Error(ST_INVALID_PARAMS, "batch already built: create a new batch to add ops");
-  ev_->check_basis(a);
-  ev_->check_basis_pt(p);
+  ev = ev ? ev : ev_;
+  if (ev->ctx() != ctx_) throw Error(ST_INVALID_PARAMS, "evaluator is not over this batch's context");
+  ev->check_basis(a);
+  ev->check_basis_pt(p);
   if (a->level != p->level) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
   if (a->level == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
   const double s = a->scale * p->scale;
   Item it;
   it.kind = PMUL;
+  it.ev = ev;
   it.a = a;
   it.p = p;
-  it.out = ev_->new_ct(a->ncomp, a->level - 1, s / (double)ctx_->primes[a->level]);
+  it.out = ev->new_ct(a->ncomp, a->level - 1, s / (double)ctx_->primes[a->level]);
   items_.push_back(it);
   return it.out;
+}
+
+size_t Batch::scratch_words(const Context& c, int kind, uint32_t level, uint32_t ncomp) {
+  const size_t l = level, k = c.k, ext = l + 1 + k;
+  size_t w = 0;
+  if (kind != PMUL) {
+    w += (kind == MUL ? 3 : 1) * (l + 1);                       // tensor product / gathered c1
+    w += (l + 1) + conv_limbs(c, l) + 2 * ext + 2 * (k + l + 1);  // key switch
+    if (kind == MUL) w += 2 * (l + 1) + 2 * (1 + l);             // relinearized, rescale
+  } else {
+    w += ncomp * (l + 1) + ncomp * (1 + l);                      // product, rescale
+  }
+  return w * c.n;
 }
 
 uint64_t Batch::key_switches() const {
@@ -127,18 +149,7 @@ void Batch::build() {
     if ((a.kind == PMUL) != (b.kind == PMUL)) return b.kind == PMUL;
     return a.key < b.key;
   });
-  auto item_words = [&](const Item& it) -> size_t {
-    const size_t l = it.a->level, ext = l + 1 + k;
-    size_t w = 0;
-    if (it.kind != PMUL) {
-      w += (it.kind == MUL ? 3 : 1) * (l + 1);                    // tensor product / gathered c1
-      w += (l + 1) + conv_limbs(c, l) + 2 * ext + 2 * (k + l + 1);  // key switch
-      if (it.kind == MUL) w += 2 * (l + 1) + 2 * (1 + l);          // relinearized, rescale
-    } else {
-      w += it.a->ncomp * (l + 1) + it.a->ncomp * (1 + l);          // product, rescale
-    }
-    return w * N;
-  };
+  auto item_words = [&](const Item& it) -> size_t { return scratch_words(c, it.kind, it.a->level, it.a->ncomp); };
   // chunks
   std::vector<std::vector<size_t>> chunks;
   size_t cur = 0;
@@ -286,10 +297,11 @@ void Batch::build() {
     S.fwd_rs = db.put(fwd_rs);
     S.fin_rs = db.put(fin_rs);
   }
+  // An asynchronous copy from pageable memory has staged the source when it returns, so
+  // `db` may go away at once and the host does not wait for work already on the stream.
   desc_ = c.alloc((db.bytes.size() + 7) / 8);
   if (!db.bytes.empty())
     CKG_CUDA(cudaMemcpyAsync(desc_->p, db.bytes.data(), db.bytes.size(), cudaMemcpyHostToDevice, c.stream));
-  CKG_CUDA(cudaStreamSynchronize(c.stream));
   for (auto& s : stages) chunks_.push_back(new Stage(s));
   built_ = true;
 }
@@ -319,8 +331,8 @@ void Batch::issue() {
 }
 
 void Batch::count_ops() {
-  OpCounter d;
   for (auto& it : items_) {
+    OpCounter d;
     if (it.kind == MUL) {
       d.ct_ct_tensor++;
       d.relins++;
@@ -331,8 +343,8 @@ void Batch::count_ops() {
       d.ct_pt_mults++;
       d.rescales++;
     }
+    it.ev->add_counts(d);
   }
-  ev_->add_counts(d);
 }
 
 void Batch::run() {

@@ -19,9 +19,11 @@ class Batch {
   explicit Batch(Evaluator* ev);
   ~Batch();
 
-  Ct mul_relin_rescale(const Ct& a, const Ct& b);
-  Ct rotate(const Ct& a, int32_t steps);
-  Ct mul_plain_rescale(const Ct& a, const Pt& p);
+  // Each op is checked by, draws its keys from and is counted on `ev` (default: the
+  // batch's evaluator), so one batch can serve the ops of several key owners.
+  Ct mul_relin_rescale(const Ct& a, const Ct& b, Evaluator* ev = nullptr);
+  Ct rotate(const Ct& a, int32_t steps, Evaluator* ev = nullptr);
+  Ct mul_plain_rescale(const Ct& a, const Pt& p, Evaluator* ev = nullptr);
 
   void run();           // queues the whole batch on the context's stream
   void capture_graph(); // captures run()'s launches into a CUDA graph (once)
@@ -29,10 +31,15 @@ class Batch {
   uint64_t key_switches() const;
   size_t size() const { return items_.size(); }
 
- private:
   enum Kind { MUL = 0, ROT = 1, PMUL = 2 };
+  // Device working words of one op (its share of the batch scratch) on a level-`level`,
+  // `ncomp`-component input.
+  static size_t scratch_words(const Context& c, int kind, uint32_t level, uint32_t ncomp);
+
+ private:
   struct Item {
     Kind kind;
+    Evaluator* ev = nullptr;
     Ct a, b, out;
     Pt p;
     uint64_t elt = 0;

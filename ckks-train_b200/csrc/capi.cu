@@ -547,4 +547,119 @@ int ckg_batch_launch_graph(ckg_batch* b) {
 
 uint64_t ckg_batch_key_switches(const ckg_batch* b) { return b && b->b ? b->b->key_switches() : 0; }
 
+// ---- serving loop ------------------------------------------------------------------------
+
+static Server& server_of(const ckg_server* s) {
+  if (!s || !s->s) throw Error(CKG_INVALID_PARAMS, "null server");
+  return *s->s;
+}
+
+int ckg_server_create(ckg_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t max_batch_ks, uint32_t max_inflight,
+                      uint32_t flags, ckg_server** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  ServerConfig cfg;
+  cfg.hbm_budget = hbm_budget_bytes;
+  cfg.max_batch_ks = max_batch_ks;
+  cfg.max_inflight = max_inflight;
+  cfg.eval = EvalConfig{(flags & CKG_HOIST) != 0, (flags & CKG_BSGS) != 0, (flags & CKG_LAZY_RELIN) != 0};
+  auto h = new ckg_server{std::make_unique<Server>(&ctx_of(ctx), cfg), hbm_budget_bytes};
+  *out = h;
+  CKG_API_END
+}
+
+void ckg_server_destroy(ckg_server* s) { delete s; }
+
+int ckg_server_add_owner(ckg_server* s, uint32_t* owner) {
+  CKG_API_BEGIN
+  if (!owner) throw Error(CKG_INVALID_PARAMS, "null output");
+  *owner = server_of(s).add_owner();
+  CKG_API_END
+}
+
+int ckg_server_add_key(ckg_server* s, uint32_t owner, const uint64_t* key, int device_src, uint32_t parts,
+                       uint32_t q_limbs, uint64_t galois_elt) {
+  CKG_API_BEGIN
+  server_of(s).add_key(owner, key, device_src != 0, parts, q_limbs, galois_elt);
+  CKG_API_END
+}
+
+int ckg_server_submit_mul(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_ct* b, uint64_t* id) {
+  CKG_API_BEGIN
+  *id = server_of(s).submit_mul(owner, ct_of(a), ct_of(b));
+  CKG_API_END
+}
+
+int ckg_server_submit_rotate(ckg_server* s, uint32_t owner, const ckg_ct* a, int32_t steps, uint64_t* id) {
+  CKG_API_BEGIN
+  *id = server_of(s).submit_rotate(owner, ct_of(a), steps);
+  CKG_API_END
+}
+
+int ckg_server_submit_mul_plain(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_pt* p, uint64_t* id) {
+  CKG_API_BEGIN
+  *id = server_of(s).submit_mul_plain(owner, ct_of(a), pt_of(p));
+  CKG_API_END
+}
+
+int ckg_server_submit_matvec(ckg_server* s, uint32_t owner, uint32_t d, uint32_t stride, const ckg_pt* const* diag,
+                             const ckg_ct* x, uint64_t* id) {
+  CKG_API_BEGIN
+  if (!diag && d) throw Error(CKG_INVALID_PARAMS, "null diagonals");
+  std::vector<Pt> ps;
+  for (uint32_t i = 0; i < d; ++i) ps.push_back(pt_of(diag[i]));
+  *id = server_of(s).submit_matvec(owner, d, stride, ps, ct_of(x));
+  CKG_API_END
+}
+
+int ckg_server_result(ckg_server* s, uint64_t id, int64_t timeout_ms, ckg_ct** out, double* times_us) {
+  int st = CKG_OK;
+  CKG_API_BEGIN
+  Ct c;
+  std::string err;
+  st = server_of(s).result(id, timeout_ms, &c, times_us, &err);
+  if (st == CKG_TIMEOUT) return fail(CKG_TIMEOUT, "request still running");
+  if (st != CKG_OK) return fail(st, err);
+  if (out) *out = new ckg_ct{c};
+  CKG_API_END
+}
+
+int ckg_server_cancel(ckg_server* s, uint64_t id, int* cancelled) {
+  CKG_API_BEGIN
+  const bool c = server_of(s).cancel(id);
+  if (cancelled) *cancelled = c ? 1 : 0;
+  CKG_API_END
+}
+
+int ckg_server_drain(ckg_server* s, int64_t timeout_ms) {
+  CKG_API_BEGIN
+  if (!server_of(s).drain(timeout_ms)) return fail(CKG_TIMEOUT, "requests still running");
+  CKG_API_END
+}
+
+int ckg_server_stats(const ckg_server* s, uint64_t* out, uint32_t n) {
+  CKG_API_BEGIN
+  const ServerStats st = server_of(s).stats();
+  const uint64_t w[17] = {st.submitted,       st.completed,      st.failed,         st.cancelled,
+                          st.batches,         st.multi_owner_batches, st.max_batch_requests, st.key_hits,
+                          st.key_misses,      st.key_evictions,  st.key_upload_bytes, st.key_bytes,
+                          st.peak_key_bytes,  st.peak_device_bytes, st.budget_waits, st.pending,
+                          s->budget};
+  for (uint32_t i = 0; i < n && i < 17; ++i) out[i] = w[i];
+  CKG_API_END
+}
+
+int ckg_server_owner_counter(const ckg_server* s, uint32_t owner, uint64_t* out7) {
+  CKG_API_BEGIN
+  const auto w = server_of(s).owner_counter(owner).words();
+  for (int i = 0; i < 7; ++i) out7[i] = w[i];
+  CKG_API_END
+}
+
+int ckg_server_inject_upload_failures(ckg_server* s, uint32_t count) {
+  CKG_API_BEGIN
+  server_of(s).inject_upload_failures(count);
+  CKG_API_END
+}
+
 }  // extern "C"

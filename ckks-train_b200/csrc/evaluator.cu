@@ -31,13 +31,13 @@ void check_ct_scale(double s) {  // ciphertext.rs:53-55
   if (!(std::isfinite(s) && s > 0.0)) throw Error(ST_INVALID_PARAMS, "ciphertext scale must be positive and finite");
 }
 
+}  // namespace
+
 std::pair<uint32_t, uint32_t> bsgs_split(uint32_t d) {  // linalg.rs:419-424
   uint32_t log_d = __builtin_ctz(d);
   uint32_t baby = 1u << ((log_d + 1) / 2);
   return {baby, d / baby};
 }
-
-}  // namespace
 
 Evaluator::Evaluator(Context* ctx, KeyPtr relin, std::vector<KeyPtr> galois, EvalConfig cfg)
     : ctx_(ctx), relin_(std::move(relin)), galois_(std::move(galois)), cfg_(cfg) {}
@@ -478,6 +478,8 @@ void check_diagonals(Context& c, uint32_t d, uint32_t stride, const std::vector<
     if (entry_scale(e) != entry_scale(entries[0])) throw Error(ST_SCALE_MISMATCH, "scale mismatch");
 }
 
+}  // namespace
+
 std::vector<int32_t> rotation_steps(uint32_t d, uint32_t stride) {  // linalg.rs:433-457
   auto bg = bsgs_split(d);
   std::vector<int32_t> s;
@@ -485,8 +487,6 @@ std::vector<int32_t> rotation_steps(uint32_t d, uint32_t stride) {  // linalg.rs
   for (uint32_t k1 = 1; k1 < bg.second; ++k1) s.push_back((int32_t)(bg.first * k1 * stride));
   return s;
 }
-
-}  // namespace
 
 template <class T, class MulF, class FinF>
 Ct Evaluator::bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, const Ct& x, MulF mul, FinF finish) {

@@ -50,6 +50,11 @@ struct EvalConfig {  // ops.rs:111-178
 
 typedef std::shared_ptr<DevKey> KeyPtr;
 
+// BSGS split of d diagonals into (baby, giant) steps (linalg.rs:419-424) and the rotation
+// steps a d-diagonal mat-vec with `stride` needs keys for (linalg.rs:433-457).
+std::pair<uint32_t, uint32_t> bsgs_split(uint32_t d);
+std::vector<int32_t> rotation_steps(uint32_t d, uint32_t stride);
+
 class Evaluator {
  public:
   Evaluator(Context* ctx, KeyPtr relin, std::vector<KeyPtr> galois, EvalConfig cfg);

@@ -4,6 +4,7 @@
 
 #include "batch.hpp"
 #include "evaluator.hpp"
+#include "serve.hpp"
 
 struct ckg_ctx {
   std::unique_ptr<ckg::Context> c;
@@ -23,6 +24,10 @@ struct ckg_pt {
 struct ckg_batch {
   std::unique_ptr<ckg::Batch> b;
   ckg_eval* ev;
+};
+struct ckg_server {
+  std::unique_ptr<ckg::Server> s;
+  uint64_t budget = 0;
 };
 
 // Sets the calling thread's message returned by ckg_last_error().

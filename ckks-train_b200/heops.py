@@ -63,8 +63,13 @@ class Timeout(Device):
     code = 8
 
 
+class Cancelled(HekitError):
+    """A served request was cancelled before it was admitted (no reference counterpart)."""
+    code = 9
+
+
 _ERRORS = {c.code: c for c in (InvalidParams, ScaleMismatch, LevelMismatch, NoLevelsLeft, Decode, Device,
-                               OutOfMemory, Timeout)}
+                               OutOfMemory, Timeout, Cancelled)}
 
 _lib = None
 
@@ -160,6 +165,20 @@ def _declare(L):
         getattr(L, name).argtypes = [VP]
     L.ckg_batch_key_switches.argtypes = [VP]
     L.ckg_batch_key_switches.restype = C.c_uint64
+    L.ckg_server_create.argtypes = [VP, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(VP)]
+    L.ckg_server_destroy.argtypes = [VP]
+    L.ckg_server_add_owner.argtypes = [VP, U32P]
+    L.ckg_server_add_key.argtypes = [VP, C.c_uint32, VP, C.c_int, C.c_uint32, C.c_uint32, C.c_uint64]
+    L.ckg_server_submit_mul.argtypes = [VP, C.c_uint32, VP, VP, U64P]
+    L.ckg_server_submit_rotate.argtypes = [VP, C.c_uint32, VP, C.c_int32, U64P]
+    L.ckg_server_submit_mul_plain.argtypes = [VP, C.c_uint32, VP, VP, U64P]
+    L.ckg_server_submit_matvec.argtypes = [VP, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, U64P]
+    L.ckg_server_result.argtypes = [VP, C.c_uint64, C.c_int64, C.POINTER(VP), C.POINTER(C.c_double)]
+    L.ckg_server_cancel.argtypes = [VP, C.c_uint64, C.POINTER(C.c_int)]
+    L.ckg_server_drain.argtypes = [VP, C.c_int64]
+    L.ckg_server_stats.argtypes = [VP, U64P, C.c_uint32]
+    L.ckg_server_owner_counter.argtypes = [VP, C.c_uint32, U64P]
+    L.ckg_server_inject_upload_failures.argtypes = [VP, C.c_uint32]
 
 
 def _check(code):
@@ -643,3 +662,113 @@ class Batch:
 
     def key_switches(self):
         return lib().ckg_batch_key_switches(self.h)
+
+
+SERVER_STATS = ("submitted", "completed", "failed", "cancelled", "batches", "multi_owner_batches",
+                "max_batch_requests", "key_hits", "key_misses", "key_evictions", "key_upload_bytes", "key_bytes",
+                "peak_key_bytes", "peak_device_bytes", "budget_waits", "pending", "hbm_budget")
+
+
+class Server:
+    """Serving loop over one context (include/ckg.h, "serving loop"): requests from many key
+    owners, admitted by HBM budget with LRU key spill to pinned host memory and run with
+    continuous batching. `ev` is any evaluator of the context; results are wrapped with it."""
+
+    def __init__(self, ctx, hbm_budget, max_batch_ks=128, max_inflight=2, config=None, ev=None):
+        self.ctx, self.ev = ctx, ev
+        flags = (config or EvalConfig()).flags
+        h = VP()
+        _check(lib().ckg_server_create(ctx.h, int(hbm_budget), max_batch_ks, max_inflight, flags, C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ckg_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_owner(self):
+        o = C.c_uint32()
+        _check(lib().ckg_server_add_owner(self.h, C.byref(o)))
+        return o.value
+
+    def add_key(self, owner, key, galois_elt=0):
+        """key: uint64 array (parts, 2, q_limbs + k, N), the layout Context.upload_key takes."""
+        key = np.ascontiguousarray(key, dtype=np.uint64)
+        parts, two, limbs, n = key.shape
+        assert two == 2 and n == self.ctx.n
+        _check(lib().ckg_server_add_key(self.h, owner, key.ctypes.data_as(VP), 0, parts, limbs - self.ctx.k,
+                                        galois_elt))
+
+    def add_key_device(self, owner, ptr, shape, galois_elt=0):
+        parts, two, limbs, n = shape
+        assert two == 2 and n == self.ctx.n
+        _check(lib().ckg_server_add_key(self.h, owner, VP(ptr), 1, parts, limbs - self.ctx.k, galois_elt))
+
+    def _submit(self, fn, owner, *args, keep=()):
+        i = C.c_uint64()
+        _check(fn(self.h, owner, *args, C.byref(i)))
+        self._keep[i.value] = keep
+        return i.value
+
+    def submit_mul(self, owner, a, b):
+        return self._submit(lib().ckg_server_submit_mul, owner, a.h, b.h, keep=(a, b))
+
+    def submit_rotate(self, owner, a, steps):
+        return self._submit(lib().ckg_server_submit_rotate, owner, a.h, steps, keep=(a,))
+
+    def submit_mul_plain(self, owner, a, p):
+        return self._submit(lib().ckg_server_submit_mul_plain, owner, a.h, p.h, keep=(a, p))
+
+    def submit_matvec(self, owner, d, stride, diag, x):
+        arr = (VP * len(diag))(*[p.h for p in diag])
+        return self._submit(lib().ckg_server_submit_matvec, owner, d, stride, arr, x.h, keep=(x, *diag))
+
+    def result(self, rid, timeout_ms=-1):
+        """(ciphertext, (submitted, admitted, completed) in microseconds); raises the op's
+        error, or Timeout (the request stays pending) when timeout_ms runs out."""
+        h = VP()
+        t = (C.c_double * 3)()
+        code = lib().ckg_server_result(self.h, rid, int(timeout_ms), C.byref(h), t)
+        if code != Timeout.code:
+            self._keep.pop(rid, None)
+        _check(code)
+        return Ciphertext(self.ev, h), (t[0], t[1], t[2])
+
+    def result_times(self, rid, timeout_ms=-1):
+        """Like result(), but also returns the status code instead of raising."""
+        h = VP()
+        t = (C.c_double * 3)()
+        code = lib().ckg_server_result(self.h, rid, int(timeout_ms), C.byref(h), t)
+        if code != Timeout.code:
+            self._keep.pop(rid, None)
+        ct = Ciphertext(self.ev, h) if code == 0 else None
+        return code, ct, (t[0], t[1], t[2])
+
+    def cancel(self, rid):
+        c = C.c_int()
+        _check(lib().ckg_server_cancel(self.h, rid, C.byref(c)))
+        return bool(c.value)
+
+    def drain(self, timeout_ms=-1):
+        _check(lib().ckg_server_drain(self.h, int(timeout_ms)))
+
+    def stats(self):
+        out = np.zeros(len(SERVER_STATS), np.uint64)
+        _check(lib().ckg_server_stats(self.h, _p64(out), len(SERVER_STATS)))
+        return {k: int(v) for k, v in zip(SERVER_STATS, out)}
+
+    def owner_counter(self, owner):
+        out = np.zeros(7, np.uint64)
+        _check(lib().ckg_server_owner_counter(self.h, owner, _p64(out)))
+        return dict(zip(COUNTER_FIELDS, (int(x) for x in out)))
+
+    def inject_upload_failures(self, count):
+        _check(lib().ckg_server_inject_upload_failures(self.h, count))

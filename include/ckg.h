@@ -51,7 +51,8 @@ enum {
   CKG_DECODE = 5,           /* HekitError::Decode */
   CKG_DEVICE = 6,           /* HekitError::Device */
   CKG_OOM = 7,              /* HekitError::Device (out of device memory) */
-  CKG_TIMEOUT = 8           /* HekitError::Device (a bounded wait gave up) */
+  CKG_TIMEOUT = 8,          /* HekitError::Device (a bounded wait gave up) */
+  CKG_CANCELLED = 9         /* serving loop only: request cancelled before admission (no counterpart) */
 };
 
 /* EvalConfig flags (crates/ckks-train-ckks/src/ops.rs:111-178). */
@@ -226,6 +227,52 @@ CKG_API int ckg_batch_run(ckg_batch* b);
 CKG_API int ckg_batch_capture_graph(ckg_batch* b);
 CKG_API int ckg_batch_launch_graph(ckg_batch* b);
 CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
+
+/* ---- serving loop ----------------------------------------------------------------------
+ * No counterpart in the reference, which runs one HeOps call at a time. A server admits
+ * requests from many key owners as they arrive and runs them with continuous batching:
+ * while one batch computes, the next is admitted, its missing keys are copied up on a
+ * second stream and it is queued behind (at most `max_inflight` batches on the device).
+ * Every key is registered once into pinned host memory; device copies are cached LRU and
+ * evicted (spilled back to the host copy) to keep the cached keys plus the working space of
+ * the queued batches within `hbm_budget_bytes`. A request that cannot fit even alone fails
+ * with CKG_OOM. Request kinds and the HeOps call each one stands for, with that call's
+ * checks and errors (crates/ckks-train-ckks/src/ops.rs:20-108):
+ *   mul        Evaluator::mul then ::rescale (evaluator.rs:463-510), relinearization key;
+ *   rotate     Evaluator::rotate (evaluator.rs:534-540), the step's Galois key;
+ *   mul_plain  Evaluator::mul_plain then ::rescale (evaluator.rs:262-271, 498-510);
+ *   matvec     matvec_plain with hoisted BSGS (linalg.rs:608-622), the step keys.
+ * Each result is bit-identical to the op run on its own. ckg_server_result waits for one
+ * request (timeout_ms < 0: no limit; CKG_TIMEOUT leaves it pending), returns its status
+ * (the op's error text via ckg_last_error), its output and times_us = {submitted, admitted,
+ * completed} in microseconds since the server was created, then forgets it. Inputs and
+ * outputs are ordinary ciphertext handles of the context; the context must outlive the
+ * server. ckg_server_destroy cancels waiting requests and waits for queued batches.
+ * Stats (ckg_server_stats, up to 17 words in this order): submitted, completed, failed,
+ * cancelled, batches, multi_owner_batches, max_batch_requests, key_hits, key_misses,
+ * key_evictions, key_upload_bytes, key_bytes, peak_key_bytes, peak_device_bytes,
+ * budget_waits, pending, hbm_budget. */
+typedef struct ckg_server ckg_server;
+enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVEC = 3 };
+CKG_API int ckg_server_create(ckg_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t max_batch_ks, uint32_t max_inflight,
+                              uint32_t flags, ckg_server** out);
+CKG_API void ckg_server_destroy(ckg_server* s);
+CKG_API int ckg_server_add_owner(ckg_server* s, uint32_t* owner);
+/* key: the layout of ckg_key_upload; galois_elt 0 registers the relinearization key. */
+CKG_API int ckg_server_add_key(ckg_server* s, uint32_t owner, const uint64_t* key, int device_src, uint32_t parts,
+                               uint32_t q_limbs, uint64_t galois_elt);
+CKG_API int ckg_server_submit_mul(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_ct* b, uint64_t* id);
+CKG_API int ckg_server_submit_rotate(ckg_server* s, uint32_t owner, const ckg_ct* a, int32_t steps, uint64_t* id);
+CKG_API int ckg_server_submit_mul_plain(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_pt* p, uint64_t* id);
+CKG_API int ckg_server_submit_matvec(ckg_server* s, uint32_t owner, uint32_t d, uint32_t stride,
+                                     const ckg_pt* const* diag, const ckg_ct* x, uint64_t* id);
+CKG_API int ckg_server_result(ckg_server* s, uint64_t id, int64_t timeout_ms, ckg_ct** out, double* times_us);
+CKG_API int ckg_server_cancel(ckg_server* s, uint64_t id, int* cancelled);
+CKG_API int ckg_server_drain(ckg_server* s, int64_t timeout_ms);
+CKG_API int ckg_server_stats(const ckg_server* s, uint64_t* out, uint32_t n);
+CKG_API int ckg_server_owner_counter(const ckg_server* s, uint32_t owner, uint64_t* out7);
+/* Test hook: the next `count` key uploads fail as an allocation failure would. */
+CKG_API int ckg_server_inject_upload_failures(ckg_server* s, uint32_t count);
 
 #ifdef __cplusplus
 }
