@@ -7,6 +7,8 @@ hyphen, so loaders register it by path; see ``load_package`` in bench.py).
 from .heops import (  # noqa: F401
     BSGS,
     Batch,
+    BootParams,
+    Bootstrapper,
     Cancelled,
     HOIST,
     LAZY_RELIN,
@@ -21,6 +23,7 @@ from .heops import (  # noqa: F401
     InvalidParams,
     Key,
     LevelMismatch,
+    LinearTransform,
     LIB_PATH,
     NoLevelsLeft,
     OutOfMemory,

@@ -547,6 +547,165 @@ int ckg_batch_launch_graph(ckg_batch* b) {
 
 uint64_t ckg_batch_key_switches(const ckg_batch* b) { return b && b->b ? b->b->key_switches() : 0; }
 
+// ---- bootstrapping ------------------------------------------------------------------------
+
+static BootParams boot_params_of(const uint32_t* bp) {
+  if (!bp) throw Error(CKG_INVALID_PARAMS, "null boot parameters");
+  BootParams b;
+  b.log_slots = bp[0];
+  b.ctos_levels = bp[1];
+  b.evalmod_levels = bp[2];
+  b.stoc_levels = bp[3];
+  b.k_intervals = bp[4];
+  b.cheb_degree = bp[5];
+  b.double_angle = bp[6];
+  return b;
+}
+
+static std::vector<LtPtr> stages_of(const ckg_lt* const* st, uint32_t n) {
+  std::vector<LtPtr> v;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!st || !st[i] || !st[i]->lt) throw Error(CKG_INVALID_PARAMS, "null stage");
+    v.push_back(st[i]->lt);
+  }
+  return v;
+}
+
+int ckg_boot_mul_const(ckg_eval* ev, const ckg_ct* a, double value, double scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).boot_mul_const(ct_of(a), value, scale), out);
+  CKG_API_END
+}
+
+int ckg_boot_add_const(ckg_eval* ev, const ckg_ct* a, double value, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).boot_add_const(ct_of(a), value), out);
+  CKG_API_END
+}
+
+int ckg_boot_zero(ckg_eval* ev, uint32_t level, double scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).boot_zero(level, scale), out);
+  CKG_API_END
+}
+
+int ckg_boot_relabel(ckg_eval* ev, const ckg_ct* a, double scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).relabel(ct_of(a), scale), out);
+  CKG_API_END
+}
+
+int ckg_mul_by_x_half(ckg_eval* ev, const ckg_ct* a, ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(ev_of(ev).mul_by_x_half(ct_of(a)), out);
+  CKG_API_END
+}
+
+int ckg_mod_raise(ckg_eval* ev, const ckg_ct* a, const ckg_key* to_sparse, const ckg_key* to_dense, ckg_ct** out) {
+  CKG_API_BEGIN
+  if (!to_sparse || !to_sparse->k || !to_dense || !to_dense->k) throw Error(CKG_INVALID_PARAMS, "null SSE key");
+  return emit(ev_of(ev).mod_raise(ct_of(a), *to_sparse->k, *to_dense->k), out);
+  CKG_API_END
+}
+
+int ckg_lt_create(int direction, uint32_t level, double scale, uint32_t d, uint32_t stride, int64_t offset,
+                  const ckg_pt* const* entries, const ckg_pt* const* second, ckg_lt** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  if (direction != DIR_COEFF_TO_SLOT && direction != DIR_SLOT_TO_COEFF)
+    throw Error(CKG_INVALID_PARAMS, "direction must be 0 (CoeffToSlot) or 1 (SlotToCoeff)");
+  if (!d || (d & (d - 1))) throw Error(CKG_INVALID_PARAMS, "d must be a power of two");
+  if (!(offset <= 0 && offset > -(int64_t)d))
+    throw Error(CKG_INVALID_PARAMS, "diagonal offset outside -d < offset <= 0");
+  if (!entries) throw Error(CKG_INVALID_PARAMS, "null entries");
+  auto lt = std::make_shared<LinearTransform>();
+  lt->direction = direction;
+  lt->level = level;
+  lt->scale = scale;
+  auto fill = [&](SparseDiag& sd, const ckg_pt* const* es) {
+    auto bg = bsgs_split(d);
+    sd.d = d;
+    sd.baby = bg.first;
+    sd.giant = bg.second;
+    sd.stride = stride;
+    sd.offset = offset;
+    for (uint32_t i = 0; i < d; ++i) sd.entries.push_back(es[i] && es[i]->p ? es[i]->p : Pt());
+  };
+  fill(lt->diags, entries);
+  if (second) {
+    lt->has_second = true;
+    fill(lt->second, second);
+  }
+  *out = new ckg_lt{lt};
+  CKG_API_END
+}
+
+void ckg_lt_free(ckg_lt* lt) { delete lt; }
+
+int ckg_coeff_to_slot(ckg_eval* ev, const ckg_ct* a, const ckg_lt* const* stages, uint32_t n, ckg_ct** re,
+                      ckg_ct** im) {
+  CKG_API_BEGIN
+  auto r = coeff_to_slot(ev_of(ev), ct_of(a), stages_of(stages, n));
+  check_launch();
+  *re = new ckg_ct{r.first};
+  *im = new ckg_ct{r.second};
+  CKG_API_END
+}
+
+int ckg_slot_to_coeff(ckg_eval* ev, const ckg_ct* re, const ckg_ct* im, const ckg_lt* const* stages, uint32_t n,
+                      ckg_ct** out) {
+  CKG_API_BEGIN
+  return emit(slot_to_coeff(ev_of(ev), ct_of(re), ct_of(im), stages_of(stages, n)), out);
+  CKG_API_END
+}
+
+int ckg_eval_chebyshev(ckg_eval* ev, const ckg_ct* a, const double* coeffs, uint32_t n, double lo, double hi,
+                       double target_scale, ckg_ct** out) {
+  CKG_API_BEGIN
+  if (!coeffs && n) throw Error(CKG_INVALID_PARAMS, "null coefficients");
+  return emit(eval_chebyshev_to_scale(ev_of(ev), ct_of(a), std::vector<double>(coeffs, coeffs + n), lo, hi,
+                                      target_scale),
+              out);
+  CKG_API_END
+}
+
+int ckg_eval_mod(ckg_eval* ev, const ckg_ct* a, const uint32_t* bp, const double* coeffs, uint32_t n, ckg_ct** out) {
+  CKG_API_BEGIN
+  if (!coeffs && n) throw Error(CKG_INVALID_PARAMS, "null coefficients");
+  return emit(eval_mod(ev_of(ev), ct_of(a), boot_params_of(bp), std::vector<double>(coeffs, coeffs + n)), out);
+  CKG_API_END
+}
+
+int ckg_boot_create(ckg_ctx* ctx, const uint32_t* bp, const ckg_lt* const* ctos, uint32_t nctos,
+                    const ckg_lt* const* stoc, uint32_t nstoc, const ckg_key* const* galois, uint32_t ngal,
+                    const ckg_key* to_sparse, const ckg_key* to_dense, const double* coeffs, uint32_t ncoeffs,
+                    const double* scales, ckg_boot** out) {
+  CKG_API_BEGIN
+  if (!out || !scales || (!coeffs && ncoeffs)) throw Error(CKG_INVALID_PARAMS, "null argument");
+  std::vector<KeyPtr> gk;
+  for (uint32_t i = 0; i < ngal; ++i) {
+    if (!galois || !galois[i] || !galois[i]->k) throw Error(CKG_INVALID_PARAMS, "null Galois key");
+    gk.push_back(galois[i]->k);
+  }
+  KeyPtr ts = to_sparse ? to_sparse->k : KeyPtr(), td = to_dense ? to_dense->k : KeyPtr();
+  *out = new ckg_boot{std::make_unique<Bootstrapper>(&ctx_of(ctx), boot_params_of(bp), stages_of(ctos, nctos),
+                                                     stages_of(stoc, nstoc), gk, ts, td,
+                                                     std::vector<double>(coeffs, coeffs + ncoeffs), scales[0],
+                                                     scales[1], scales[2])};
+  CKG_API_END
+}
+
+void ckg_boot_destroy(ckg_boot* b) { delete b; }
+
+int ckg_bootstrap(ckg_boot* b, ckg_eval* ev, const ckg_ct* a, ckg_ct** out) {
+  CKG_API_BEGIN
+  if (!b || !b->b) throw Error(CKG_INVALID_PARAMS, "null bootstrapper");
+  return emit(b->b->bootstrap(ev_of(ev), ct_of(a)), out);
+  CKG_API_END
+}
+
+uint32_t ckg_boot_output_level(const ckg_boot* b) { return b && b->b ? b->b->output_level() : 0; }
+
 // ---- serving loop ------------------------------------------------------------------------
 
 static Server& server_of(const ckg_server* s) {

@@ -224,10 +224,26 @@ Context::~Context() {
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
   for (auto& kv : perms) cudaFree(kv.second);
+  if (d_xhalf) cudaFree(d_xhalf);
   cudaFree(d_prime);
   cudaFree(d_tw_fwd);
   cudaFree(d_tw_inv);
   cudaFree(d_conv);
+}
+
+const uint64_t* Context::x_half() {
+  std::lock_guard<std::mutex> lk(mu);
+  if (d_xhalf) return d_xhalf;
+  std::vector<uint64_t> mono((size_t)(L + 1) * n, 0);
+  for (uint32_t i = 0; i <= L; ++i) mono[(size_t)i * n + n / 2] = 1;
+  uint64_t* d = nullptr;
+  CKG_CUDA(cudaMalloc(&d, mono.size() * 8));
+  CKG_CUDA(cudaMemcpy(d, mono.data(), mono.size() * 8, cudaMemcpyHostToDevice));
+  std::vector<LimbRef> refs;
+  for (uint32_t i = 0; i <= L; ++i) refs.push_back(LimbRef{d + (size_t)i * n, d + (size_t)i * n, i, 0});
+  launch_ntt(dt, refs.data(), (int)refs.size(), false, stream);
+  d_xhalf = d;
+  return d;
 }
 
 const uint32_t* Context::perm(uint64_t elt) {

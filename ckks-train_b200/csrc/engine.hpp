@@ -115,6 +115,8 @@ struct Context {
   uint32_t digit_end(uint32_t j, uint32_t l) const { return std::min((j + 1) * alpha, l + 1); }
   uint32_t p_prime(uint32_t t) const { return L + 1 + t; }  // global index of special prime t
   const uint32_t* perm(uint64_t elt);                       // cached device permutation
+  const uint64_t* x_half();  // NTT form of the monomial X^(N/2) over q_0..q_L (cached)
+  uint64_t* d_xhalf = nullptr;
   DevBufPtr alloc(size_t words);                            // stream-ordered, on `stream`
   void activate() const;                                    // makes `device` current
 };

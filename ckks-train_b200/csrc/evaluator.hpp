@@ -48,6 +48,25 @@ struct EvalConfig {  // ops.rs:111-178
   bool hoist = true, bsgs = true, lazy_relin = true;
 };
 
+// Plaintext diagonals of a BSGS product with the all-zero entries left out
+// (Diagonals<Option<Plaintext>>, linalg.rs:125-380): entry k1 * baby + k2 is diagonal
+// offset + baby * k1 + k2 (times `stride`), pre-rotated by its giant step; null = skipped.
+struct SparseDiag {
+  uint32_t d = 0, baby = 0, giant = 0, stride = 1;
+  int64_t offset = 0;
+  std::vector<Pt> entries;
+  uint32_t nonzero() const {
+    uint32_t c = 0;
+    for (auto& e : entries) c += e != nullptr;
+    return c;
+  }
+  const Pt* first() const {  // plain_scale() source (linalg.rs:371-373)
+    for (auto& e : entries)
+      if (e) return &e;
+    return nullptr;
+  }
+};
+
 typedef std::shared_ptr<DevKey> KeyPtr;
 
 // BSGS split of d diagonals into (baby, giant) steps (linalg.rs:419-424) and the rotation
@@ -91,6 +110,25 @@ class Evaluator {
   double exact_product_scale(uint32_t level, double target) const;
   Ct matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x);
   Ct matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x);
+  // Sum over terms of diag_t * x_t with shared giant rotations, skipping null entries and
+  // the baby rotations only they would use (linalg.rs:741-799).
+  Ct matvec_plain_sum_sparse(const std::vector<std::pair<const SparseDiag*, Ct>>& terms);
+
+  // BootstrapArithmetic (bootstrap/poly.rs:453-486), ModRaise (bootstrap/modraise.rs) and
+  // the exact monomial product of CoeffToSlot (bootstrap/linear.rs:921-936).
+  void check_boot_input(const Ct& a) const;
+  void check_conjugation_key() const;
+  Ct boot_mul_const(const Ct& a, double value, double product_scale);
+  Ct boot_add_const(const Ct& a, double value);
+  Ct boot_zero(uint32_t level, double scale);
+  Ct mul_by_x_half(const Ct& a);
+  Ct mod_raise(const Ct& a, const DevKey& to_sparse, const DevKey& to_dense);
+  Ct mod_raise_main_key(const Ct& a);
+  bool relin_key_present() const { return (bool)relin_; }
+  const std::vector<KeyPtr>& galois_keys() const { return galois_; }
+  KeyPtr relin_key() const { return relin_; }
+  void check_galois_input_pub(const Ct& a) const { check_galois_input(a); }
+  void check_rotation_keys_pub(const std::vector<int32_t>& steps) const { check_rotation_keys(steps); }
 
  private:
   friend class Batch;
@@ -106,6 +144,7 @@ class Evaluator {
   std::optional<uint64_t> rotation_elt(int32_t steps) const;
   void check_rotation_keys(const std::vector<int32_t>& steps) const;
   Ct apply_galois(const Ct& a, uint64_t elt);
+  Ct raise_level0(const Ct& a);
   template <class F>
   void count(F f) {
     std::lock_guard<std::mutex> lk(mu_);

@@ -3,6 +3,7 @@
 #include <memory>
 
 #include "batch.hpp"
+#include "boot.hpp"
 #include "evaluator.hpp"
 #include "serve.hpp"
 
@@ -24,6 +25,12 @@ struct ckg_pt {
 struct ckg_batch {
   std::unique_ptr<ckg::Batch> b;
   ckg_eval* ev;
+};
+struct ckg_lt {
+  ckg::LtPtr lt;
+};
+struct ckg_boot {
+  std::unique_ptr<ckg::Bootstrapper> b;
 };
 struct ckg_server {
   std::unique_ptr<ckg::Server> s;

@@ -624,14 +624,34 @@ __global__ void __launch_bounds__(256)
   r.d2[c] = mul_mod(a1, b1, P);
 }
 
+// mode 0: dst = src * w (Shoup pair per prime); mode 1: dst = src + w (w < q).
 __global__ void __launch_bounds__(256)
     k_scalar(const __grid_constant__ LimbBatch b, const __grid_constant__ ScalarTable st,
-             const PrimeConst* __restrict__ pc, int n) {
+             const PrimeConst* __restrict__ pc, int n, int mode) {
   const LimbRef& r = b.r[blockIdx.y];
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   const uint64_t q = __ldg(&pc[r.prime].q);
-  r.dst[c] = mul_shoup(r.src[c], st.w[r.prime], st.ws[r.prime], q);
+  r.dst[c] = mode == 0 ? mul_shoup(r.src[c], st.w[r.prime], st.ws[r.prime], q) : add_mod(r.src[c], st.w[r.prime], q);
+}
+
+// Centered lift of a level-0 coefficient-form limb (src of every ref) into prime r.prime:
+// residues above (q_0 - 1) / 2 are read as negative (poly.rs:298-345).
+__global__ void __launch_bounds__(256)
+    k_lift_level0(const __grid_constant__ LimbBatch b, const PrimeConst* __restrict__ pc, int n) {
+  const LimbRef& r = b.r[blockIdx.y];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const uint64_t q0 = __ldg(&pc[0].q), q = __ldg(&pc[r.prime].q);
+  const uint64_t x = r.src[c];
+  uint64_t v;
+  if (x > q0 / 2) {
+    const uint64_t m = (q0 - x) % q;
+    v = m ? q - m : 0;
+  } else {
+    v = x % q;
+  }
+  r.dst[c] = v;
 }
 
 template <class T>
@@ -884,13 +904,25 @@ void launch_tensor_ptr(const DevTables& d, const TensorRef* dev_refs, int count,
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st) {
+void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st,
+                   int mode) {
   LimbBatch b;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxLimbs) {
     b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
     for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
-    k_scalar<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, table, d.prime, n);
+    k_scalar<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, table, d.prime, n, mode);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_lift_level0(const DevTables& d, const LimbRef* refs, int count, cudaStream_t st) {
+  LimbBatch b;
+  const int n = 1 << d.log_n;
+  for (int off = 0; off < count; off += kMaxLimbs) {
+    b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
+    for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
+    k_lift_level0<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, d.prime, n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
 }

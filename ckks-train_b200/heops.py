@@ -165,6 +165,26 @@ def _declare(L):
         getattr(L, name).argtypes = [VP]
     L.ckg_batch_key_switches.argtypes = [VP]
     L.ckg_batch_key_switches.restype = C.c_uint64
+    DP = C.POINTER(C.c_double)
+    L.ckg_boot_mul_const.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
+    L.ckg_boot_add_const.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
+    L.ckg_boot_zero.argtypes = [VP, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_boot_relabel.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
+    L.ckg_mul_by_x_half.argtypes = [VP, VP, C.POINTER(VP)]
+    L.ckg_mod_raise.argtypes = [VP, VP, VP, VP, C.POINTER(VP)]
+    L.ckg_lt_create.argtypes = [C.c_int, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, C.c_int64, C.POINTER(VP),
+                                C.POINTER(VP), C.POINTER(VP)]
+    L.ckg_lt_free.argtypes = [VP]
+    L.ckg_coeff_to_slot.argtypes = [VP, VP, C.POINTER(VP), C.c_uint32, C.POINTER(VP), C.POINTER(VP)]
+    L.ckg_slot_to_coeff.argtypes = [VP, VP, VP, C.POINTER(VP), C.c_uint32, C.POINTER(VP)]
+    L.ckg_eval_chebyshev.argtypes = [VP, VP, DP, C.c_uint32, C.c_double, C.c_double, C.c_double, C.POINTER(VP)]
+    L.ckg_eval_mod.argtypes = [VP, VP, U32P, DP, C.c_uint32, C.POINTER(VP)]
+    L.ckg_boot_create.argtypes = [VP, U32P, C.POINTER(VP), C.c_uint32, C.POINTER(VP), C.c_uint32, C.POINTER(VP),
+                                  C.c_uint32, VP, VP, DP, C.c_uint32, DP, C.POINTER(VP)]
+    L.ckg_boot_destroy.argtypes = [VP]
+    L.ckg_bootstrap.argtypes = [VP, VP, VP, C.POINTER(VP)]
+    L.ckg_boot_output_level.argtypes = [VP]
+    L.ckg_boot_output_level.restype = C.c_uint32
     L.ckg_server_create.argtypes = [VP, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(VP)]
     L.ckg_server_destroy.argtypes = [VP]
     L.ckg_server_add_owner.argtypes = [VP, U32P]
@@ -594,6 +614,49 @@ class CudaEvaluator:
         arr = (VP * len(entries))(*[e.h for e in entries])
         return self._ct(lib().ckg_matvec_enc, d, stride, arr, x.h)
 
+    # ---- bootstrapping (include/ckg.h, "bootstrapping") ----
+
+    def boot_mul_const(self, a, value, scale):
+        """Integer multiple round(value * scale / a.scale) of a, labelled `scale` (poly.rs:380-400)."""
+        return self._ct(lib().ckg_boot_mul_const, a.h, value, scale)
+
+    def boot_add_const(self, a, value):
+        return self._ct(lib().ckg_boot_add_const, a.h, value)
+
+    def boot_zero(self, level, scale):
+        h = VP()
+        _check(lib().ckg_boot_zero(self.h, level, scale, C.byref(h)))
+        return Ciphertext(self, h)
+
+    def boot_relabel(self, a, scale):
+        return self._ct(lib().ckg_boot_relabel, a.h, scale)
+
+    def mul_by_x_half(self, a):
+        return self._ct(lib().ckg_mul_by_x_half, a.h)
+
+    def mod_raise(self, a, to_sparse, to_dense):
+        return self._ct(lib().ckg_mod_raise, a.h, to_sparse.h, to_dense.h)
+
+    def coeff_to_slot(self, a, stages):
+        arr = (VP * len(stages))(*[s.h for s in stages])
+        re, im = VP(), VP()
+        _check(lib().ckg_coeff_to_slot(self.h, a.h, arr, len(stages), C.byref(re), C.byref(im)))
+        return Ciphertext(self, re), Ciphertext(self, im)
+
+    def slot_to_coeff(self, re, im, stages):
+        arr = (VP * len(stages))(*[s.h for s in stages])
+        return self._ct(lib().ckg_slot_to_coeff, re.h, im.h, arr, len(stages))
+
+    def eval_chebyshev(self, a, coeffs, lo=-1.0, hi=1.0, target_scale=None):
+        c = np.ascontiguousarray(coeffs, np.float64)
+        t = a.scale() if target_scale is None else target_scale
+        return self._ct(lib().ckg_eval_chebyshev, a.h, c.ctypes.data_as(C.POINTER(C.c_double)), len(c), lo, hi, t)
+
+    def eval_mod(self, a, bp, coeffs):
+        b = (C.c_uint32 * 7)(*bp.words())
+        c = np.ascontiguousarray(coeffs, np.float64)
+        return self._ct(lib().ckg_eval_mod, a.h, b, c.ctypes.data_as(C.POINTER(C.c_double)), len(c))
+
     def exact_product_scale(self, level, target_scale):
         out = C.c_double()
         _check(lib().ckg_exact_product_scale(self.h, level, target_scale, C.byref(out)))
@@ -772,3 +835,74 @@ class Server:
 
     def inject_upload_failures(self, count):
         _check(lib().ckg_server_inject_upload_failures(self.h, count))
+
+
+class BootParams:
+    """Bootstrapping parameters (crates/ckks-train-ckks/src/bootstrap/params.rs:35-66)."""
+
+    def __init__(self, log_slots=15, ctos_levels=4, evalmod_levels=7, stoc_levels=4, k_intervals=13,
+                 cheb_degree=127, double_angle=0):
+        self.log_slots, self.ctos_levels, self.evalmod_levels = log_slots, ctos_levels, evalmod_levels
+        self.stoc_levels, self.k_intervals = stoc_levels, k_intervals
+        self.cheb_degree, self.double_angle = cheb_degree, double_angle
+
+    def words(self):
+        return (self.log_slots, self.ctos_levels, self.evalmod_levels, self.stoc_levels, self.k_intervals,
+                self.cheb_degree, self.double_angle)
+
+
+class LinearTransform:
+    """One CoeffToSlot (direction 0) or SlotToCoeff (1) stage of encoded diagonals
+    (bootstrap/linear.rs:482-497); entries / second: d Plaintexts or None (zero diagonal)."""
+
+    def __init__(self, direction, level, scale, d, stride, offset, entries, second=None):
+        self._keep = (list(entries), list(second or []))
+        arr = (VP * d)(*[e.h if e is not None else None for e in entries])
+        arr2 = (VP * d)(*[e.h if e is not None else None for e in second]) if second is not None else None
+        self.h = VP()
+        _check(lib().ckg_lt_create(direction, level, scale, d, stride, offset, arr, arr2, C.byref(self.h)))
+        self.direction, self.level, self.scale = direction, level, scale
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_lt_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Bootstrapper:
+    """The device bootstrap (bootstrap/bootstrapper.rs:385-473) over encoded stages, the
+    Galois keys of the stages plus the conjugation key, optional SSE keys and the EvalMod
+    series; scales = (evalmod_scale, stoc_input_scale, delta)."""
+
+    def __init__(self, ctx, bp, ctos, stoc, galois_keys, to_sparse, to_dense, coeffs, scales):
+        self.ctx, self.bp = ctx, bp
+        self._keep = (list(ctos), list(stoc), list(galois_keys), to_sparse, to_dense)
+        b = (C.c_uint32 * 7)(*bp.words())
+        a1 = (VP * len(ctos))(*[s.h for s in ctos])
+        a2 = (VP * len(stoc))(*[s.h for s in stoc])
+        g = (VP * max(len(galois_keys), 1))(*[k.h for k in galois_keys])
+        c = np.ascontiguousarray(coeffs, np.float64)
+        sc = (C.c_double * 3)(*scales)
+        self.h = VP()
+        _check(lib().ckg_boot_create(ctx.h, b, a1, len(ctos), a2, len(stoc), g, len(galois_keys),
+                                     to_sparse.h if to_sparse else None, to_dense.h if to_dense else None,
+                                     c.ctypes.data_as(C.POINTER(C.c_double)), len(c), sc, C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().ckg_boot_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def output_level(self):
+        return lib().ckg_boot_output_level(self.h)
+
+    def bootstrap(self, ev, ct):
+        h = VP()
+        _check(lib().ckg_bootstrap(self.h, ev.h, ct.h, C.byref(h)))
+        return Ciphertext(ev, h)

@@ -228,6 +228,52 @@ CKG_API int ckg_batch_capture_graph(ckg_batch* b);
 CKG_API int ckg_batch_launch_graph(ckg_batch* b);
 CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
 
+/* ---- bootstrapping ---------------------------------------------------------------------
+ * The device side of the reference's bootstrap (crates/ckks-train-ckks/src/bootstrap/): the
+ * BootstrapArithmetic ops (poly.rs:453-486), ModRaise with sparse-secret encapsulation
+ * (modraise.rs:53-73; to_sparse: 1 part at level 0, to_dense: dnum parts at max_level,
+ * both uploaded with ckg_key_upload and Galois element 0), CoeffToSlot / SlotToCoeff over
+ * encoded stages (linear.rs:776-859), the level-optimal Chebyshev evaluation
+ * (poly.rs:655-714), EvalMod (evalmod.rs:147-189) and the assembled bootstrap
+ * (bootstrapper.rs:385-473). Checks, errors, scale labels and OpCounter increments are the
+ * CPU code's. Boot parameter arrays `bp` hold 7 words: log_slots, ctos_levels,
+ * evalmod_levels, stoc_levels, k_intervals, cheb_degree, double_angle (params.rs:35-66).
+ * A stage (ckg_lt) is one LinearTransform (linear.rs:482-497): direction 0 = CoeffToSlot,
+ * 1 = SlotToCoeff; `entries` holds d plaintext handles in BSGS order (entry k1*baby + k2 is
+ * diagonal offset + baby*k1 + k2 at `stride`, pre-rotated), NULL for an all-zero diagonal;
+ * `second` is NULL or d more entries (the conjugate's diagonals in CoeffToSlot's last
+ * stage, im's in SlotToCoeff's first). Handles copy what they keep. */
+CKG_API int ckg_boot_mul_const(ckg_eval* ev, const ckg_ct* a, double value, double scale, ckg_ct** out); /* :380 */
+CKG_API int ckg_boot_add_const(ckg_eval* ev, const ckg_ct* a, double value, ckg_ct** out);               /* :404 */
+CKG_API int ckg_boot_zero(ckg_eval* ev, uint32_t level, double scale, ckg_ct** out);                    /* :436 */
+CKG_API int ckg_boot_relabel(ckg_eval* ev, const ckg_ct* a, double scale, ckg_ct** out);                /* :481 */
+CKG_API int ckg_mul_by_x_half(ckg_eval* ev, const ckg_ct* a, ckg_ct** out);          /* linear.rs:921-936 */
+CKG_API int ckg_mod_raise(ckg_eval* ev, const ckg_ct* a, const ckg_key* to_sparse, const ckg_key* to_dense,
+                          ckg_ct** out);
+typedef struct ckg_lt ckg_lt;
+CKG_API int ckg_lt_create(int direction, uint32_t level, double scale, uint32_t d, uint32_t stride, int64_t offset,
+                          const ckg_pt* const* entries, const ckg_pt* const* second, ckg_lt** out);
+CKG_API void ckg_lt_free(ckg_lt* lt);
+CKG_API int ckg_coeff_to_slot(ckg_eval* ev, const ckg_ct* a, const ckg_lt* const* stages, uint32_t n, ckg_ct** re,
+                              ckg_ct** im);
+CKG_API int ckg_slot_to_coeff(ckg_eval* ev, const ckg_ct* re, const ckg_ct* im, const ckg_lt* const* stages,
+                              uint32_t n, ckg_ct** out);
+CKG_API int ckg_eval_chebyshev(ckg_eval* ev, const ckg_ct* a, const double* coeffs, uint32_t n, double lo, double hi,
+                               double target_scale, ckg_ct** out);
+CKG_API int ckg_eval_mod(ckg_eval* ev, const ckg_ct* a, const uint32_t* bp, const double* coeffs, uint32_t n,
+                         ckg_ct** out);
+typedef struct ckg_boot ckg_boot;
+/* scales: {evalmod_scale, stoc_input_scale, delta} (bootstrapper.rs:207-230); galois: the
+ * stages' rotation keys and the conjugation key; to_sparse / to_dense both NULL: ModRaise
+ * under the main key. */
+CKG_API int ckg_boot_create(ckg_ctx* ctx, const uint32_t* bp, const ckg_lt* const* ctos, uint32_t nctos,
+                            const ckg_lt* const* stoc, uint32_t nstoc, const ckg_key* const* galois, uint32_t ngal,
+                            const ckg_key* to_sparse, const ckg_key* to_dense, const double* coeffs, uint32_t ncoeffs,
+                            const double* scales, ckg_boot** out);
+CKG_API void ckg_boot_destroy(ckg_boot* b);
+CKG_API int ckg_bootstrap(ckg_boot* b, ckg_eval* ev, const ckg_ct* a, ckg_ct** out);
+CKG_API uint32_t ckg_boot_output_level(const ckg_boot* b);
+
 /* ---- serving loop ----------------------------------------------------------------------
  * No counterpart in the reference, which runs one HeOps call at a time. A server admits
  * requests from many key owners as they arrive and runs them with continuous batching:

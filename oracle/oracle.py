@@ -123,6 +123,42 @@ def _declare(L):
     L.orc_matvec_enc.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(vp), vp, C.POINTER(vp)]
     L.orc_set_threads.argtypes = [C.c_int]
     L.orc_get_threads.restype = C.c_int
+    # bootstrapping (oracle_boot.inc)
+    DP = C.POINTER(C.c_double)
+    L.orc_encoder_new.argtypes = [vp, C.POINTER(vp)]
+    L.orc_encoder_free.argtypes = [vp]
+    L.orc_encode_complex.argtypes = [vp, DP, C.c_uint64, C.c_double, C.c_uint64, U64P]
+    L.orc_decode_complex.argtypes = [vp, U64P, C.c_uint64, C.c_double, DP]
+    L.orc_encrypt_sk.argtypes = [vp, C.c_char_p, U64P, C.c_uint64, C.c_double, C.POINTER(vp)]
+    L.orc_decrypt.argtypes = [vp, vp, U64P]
+    L.orc_boot_new.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                               C.c_uint64, C.c_int64, C.POINTER(vp)]
+    L.orc_boot_free.argtypes = [vp]
+    L.orc_boot_output_level.argtypes = [vp]
+    L.orc_boot_output_level.restype = C.c_uint64
+    L.orc_boot_scales.argtypes = [vp, DP, DP]
+    L.orc_boot_coeffs.argtypes = [vp, DP]
+    L.orc_boot_coeffs.restype = C.c_uint64
+    L.orc_boot_num_stages.argtypes = [vp, C.c_int]
+    L.orc_boot_num_stages.restype = C.c_uint64
+    L.orc_boot_stage_info.argtypes = [vp, C.c_int, C.c_uint64, U64P, C.POINTER(C.c_int64), DP]
+    L.orc_boot_stage_entry.argtypes = [vp, C.c_int, C.c_uint64, C.c_int, C.c_uint64, U64P]
+    L.orc_boot_num_galois.argtypes = [vp]
+    L.orc_boot_num_galois.restype = C.c_uint64
+    L.orc_boot_galois.argtypes = [vp, C.c_uint64, U64P, C.POINTER(vp)]
+    L.orc_boot_num_steps.argtypes = [vp, I32P]
+    L.orc_boot_num_steps.restype = C.c_uint64
+    L.orc_boot_sse.argtypes = [vp, C.POINTER(vp), C.POINTER(vp)]
+    L.orc_boot_eval.argtypes = [vp, vp, C.POINTER(vp)]
+    L.orc_bootstrap.argtypes = [vp, vp, vp, C.POINTER(vp)]
+    L.orc_boot_mod_raise.argtypes = [vp, vp, vp, C.POINTER(vp)]
+    L.orc_boot_coeff_to_slot.argtypes = [vp, vp, vp, C.POINTER(vp), C.POINTER(vp)]
+    L.orc_boot_eval_mod.argtypes = [vp, vp, vp, C.POINTER(vp)]
+    L.orc_boot_slot_to_coeff.argtypes = [vp, vp, vp, vp, C.POINTER(vp)]
+    L.orc_eval_chebyshev.argtypes = [vp, vp, DP, C.c_uint64, C.c_double, C.c_double, C.c_double, C.POINTER(vp)]
+    L.orc_boot_mul_const.argtypes = [vp, vp, C.c_double, C.c_double, C.POINTER(vp)]
+    L.orc_boot_add_const.argtypes = [vp, vp, C.c_double, C.POINTER(vp)]
+    L.orc_mul_by_x_half.argtypes = [vp, vp, C.POINTER(vp)]
 
 
 def _p64(a):
@@ -571,3 +607,186 @@ class Evaluator:
         h = C.c_void_p()
         _check(lib().orc_matvec_enc(self.h, d, stride, arr, x.h, C.byref(h)))
         return Ct(self, h)
+
+
+# ---- bootstrapping (oracle_boot.inc) ----------------------------------------------------
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Encoder:
+    """The reference Encoder (crates/ckks-train-ckks/src/encoder.rs)."""
+
+    def __init__(self, params):
+        self.params = params
+        self.h = C.c_void_p()
+        _check(lib().orc_encoder_new(params.h, C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            lib().orc_encoder_free(self.h)
+        except Exception:
+            pass
+
+    def encode(self, values, scale, level):
+        """values: complex (or real) array of at most `slots` entries -> (level+1, N) NTT form."""
+        z = np.asarray(values, np.complex128)
+        flat = np.ascontiguousarray(np.stack([z.real, z.imag], axis=-1).reshape(-1), np.float64)
+        out = np.zeros((level + 1, self.params.n), np.uint64)
+        _check(lib().orc_encode_complex(self.h, _dp(flat), len(z), scale, level, _p64(out)))
+        return out
+
+    def decode(self, pt, scale):
+        p = np.ascontiguousarray(pt, np.uint64)
+        out = np.zeros(2 * (self.params.n // 2), np.float64)
+        _check(lib().orc_decode_complex(self.h, _p64(p), p.shape[0] - 1, scale, _dp(out)))
+        return out[0::2] + 1j * out[1::2]
+
+
+def encrypt_sk(ev, kg, seed, pt, scale):
+    """Symmetric encryption of the NTT-form plaintext `pt` under kg's secret (encrypt.rs)."""
+    if isinstance(seed, int):
+        seed = bytes([seed]) * 32
+    p = np.ascontiguousarray(pt, np.uint64)
+    h = C.c_void_p()
+    _check(lib().orc_encrypt_sk(kg.h, seed, _p64(p), p.shape[0] - 1, scale, C.byref(h)))
+    return Ct(ev, h)
+
+
+def decrypt(kg, ct):
+    """c_0 + c_1 s (+ c_2 s^2 ...) in NTT form, (level+1, N)."""
+    out = np.zeros((ct.level + 1, kg.params.n), np.uint64)
+    _check(lib().orc_decrypt(kg.h, ct.h, _p64(out)))
+    return out
+
+
+class Bootstrapper:
+    """Bootstrapper::new and its pieces (crates/ckks-train-ckks/src/bootstrap/bootstrapper.rs):
+    encoded CoeffToSlot / SlotToCoeff stages, Galois and SSE keys, EvalMod coefficients."""
+
+    def __init__(self, params, kg, encoder, log_slots, ctos=4, evalmod=7, stoc=4, k_intervals=13, degree=127,
+                 double_angle=0, ephemeral_hw=32):
+        self.params = params
+        self._keep = (kg, encoder)
+        self.h = C.c_void_p()
+        _check(lib().orc_boot_new(params.h, kg.h, encoder.h, log_slots, ctos, evalmod, stoc, k_intervals, degree,
+                                  double_angle, -1 if ephemeral_hw is None else ephemeral_hw, C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            lib().orc_boot_free(self.h)
+        except Exception:
+            pass
+
+    def output_level(self):
+        return lib().orc_boot_output_level(self.h)
+
+    def scales(self):
+        a, b = C.c_double(), C.c_double()
+        lib().orc_boot_scales(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def coeffs(self):
+        n = lib().orc_boot_coeffs(self.h, None)
+        out = np.zeros(n, np.float64)
+        lib().orc_boot_coeffs(self.h, _dp(out))
+        return out
+
+    def stages(self, direction):
+        """[(info dict, entries, second entries)] with entries a list of (level+1, N) arrays
+        or None for skipped all-zero diagonals; direction 0 = CoeffToSlot, 1 = SlotToCoeff."""
+        out = []
+        n = self.params.n
+        for k in range(lib().orc_boot_num_stages(self.h, direction)):
+            info = np.zeros(4, np.uint64)
+            off = C.c_int64()
+            sc = np.zeros(2, np.float64)
+            lib().orc_boot_stage_info(self.h, direction, k, _p64(info), C.byref(off), _dp(sc))
+            level, d, stride, has2 = (int(x) for x in info)
+
+            def entries(second):
+                es = []
+                for i in range(d):
+                    buf = np.zeros((level + 1, n), np.uint64)
+                    es.append(buf if lib().orc_boot_stage_entry(self.h, direction, k, second, i, _p64(buf)) else None)
+                return es
+
+            out.append((dict(level=level, d=d, stride=stride, offset=off.value, scale=float(sc[0]),
+                             pt_scale=float(sc[1]), direction=direction), entries(0), entries(1) if has2 else None))
+        return out
+
+    def galois_keys(self):
+        keys = {}
+        for i in range(lib().orc_boot_num_galois(self.h)):
+            e = C.c_uint64()
+            h = C.c_void_p()
+            lib().orc_boot_galois(self.h, i, C.byref(e), C.byref(h))
+            keys[e.value] = Key(self.params, h)
+        return keys
+
+    def rotation_steps(self):
+        n = lib().orc_boot_num_steps(self.h, None)
+        out = (C.c_int32 * max(n, 1))()
+        lib().orc_boot_num_steps(self.h, out)
+        return list(out[:n])
+
+    def sse_keys(self):
+        a, b = C.c_void_p(), C.c_void_p()
+        _check(lib().orc_boot_sse(self.h, C.byref(a), C.byref(b)))
+        return Key(self.params, a), Key(self.params, b)
+
+    def inner_evaluator(self, relin):
+        ev = Evaluator.__new__(Evaluator)
+        ev.params = self.params
+        ev._keep = (relin, self)
+        ev.h = C.c_void_p()
+        _check(lib().orc_boot_eval(self.h, relin.h if relin else None, C.byref(ev.h)))
+        return ev
+
+    def _one(self, fn, ev, *args):
+        h = C.c_void_p()
+        _check(fn(self.h, ev.h, *args, C.byref(h)))
+        return Ct(ev, h)
+
+    def bootstrap(self, ev, ct):
+        return self._one(lib().orc_bootstrap, ev, ct.h)
+
+    def mod_raise(self, inner, ct):
+        return self._one(lib().orc_boot_mod_raise, inner, ct.h)
+
+    def coeff_to_slot(self, inner, ct):
+        a, b = C.c_void_p(), C.c_void_p()
+        _check(lib().orc_boot_coeff_to_slot(self.h, inner.h, ct.h, C.byref(a), C.byref(b)))
+        return Ct(inner, a), Ct(inner, b)
+
+    def eval_mod(self, inner, ct):
+        return self._one(lib().orc_boot_eval_mod, inner, ct.h)
+
+    def slot_to_coeff(self, inner, re, im):
+        return self._one(lib().orc_boot_slot_to_coeff, inner, re.h, im.h)
+
+
+def eval_chebyshev(ev, ct, coeffs, a, b, target):
+    c = np.ascontiguousarray(coeffs, np.float64)
+    h = C.c_void_p()
+    _check(lib().orc_eval_chebyshev(ev.h, ct.h, _dp(c), len(c), a, b, target, C.byref(h)))
+    return Ct(ev, h)
+
+
+def boot_mul_const(ev, ct, value, scale):
+    h = C.c_void_p()
+    _check(lib().orc_boot_mul_const(ev.h, ct.h, value, scale, C.byref(h)))
+    return Ct(ev, h)
+
+
+def boot_add_const(ev, ct, value):
+    h = C.c_void_p()
+    _check(lib().orc_boot_add_const(ev.h, ct.h, value, C.byref(h)))
+    return Ct(ev, h)
+
+
+def mul_by_x_half(ev, ct):
+    h = C.c_void_p()
+    _check(lib().orc_mul_by_x_half(ev.h, ct.h, C.byref(h)))
+    return Ct(ev, h)

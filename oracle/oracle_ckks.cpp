@@ -5,7 +5,8 @@
 // ModUp/ModDown (crates/ckks-train-core/src/baseconv.rs), the samplers
 // (crates/ckks-train-core/src/sampler.rs), CKKS parameters (crates/ckks-train-ckks/src/params.rs),
 // keys (keys.rs), hybrid key switching (keyswitch.rs), the Evaluator with its checks,
-// scale labels and OpCounter (evaluator.rs, counter.rs) and the BSGS products (linalg.rs).
+// scale labels and OpCounter (evaluator.rs, counter.rs), the BSGS products (linalg.rs) and
+// bootstrapping with its encoder and setup (oracle_boot.inc).
 // The `parallel` feature's data parallelism (crates/ckks-train-ckks/src/par.rs) is
 // restated with OpenMP at the same call sites; results are identical for any thread count.
 //
@@ -16,9 +17,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <map>
 #include <omp.h>
 #include <optional>
+#include <set>
 
 namespace orc {
 
@@ -1187,6 +1190,8 @@ Ciphertext matvec_enc(Evaluator& ev, const Diagonals<Ciphertext>& diag, const Ci
       [](Ciphertext c) { return c; });
 }
 
+#include "oracle_boot.inc"
+
 }  // namespace orc
 
 // =======================================================================================
@@ -1582,5 +1587,7 @@ int orc_matvec_enc(OrcEval* e, uint64_t d, uint64_t stride, const OrcCt* const* 
     *out = new OrcCt{matvec_enc(*e->ev, dg, x->ct)};
   })
 }
+
+#include "oracle_boot_api.inc"
 
 }  // extern "C"
