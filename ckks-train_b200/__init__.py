@@ -32,7 +32,12 @@ from .heops import (  # noqa: F401
     ScaleMismatch,
     Server,
     Timeout,
+    boot_encode_stages,
+    boot_plan,
+    boot_rotation_steps,
     build,
+    encode_complex_host,
+    evalmod_coeffs,
     launch_count,
     lib,
     primes_for_bits,

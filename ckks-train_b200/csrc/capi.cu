@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/ckg.h"
+#include "bootsetup.hpp"
 #include "handles.hpp"
 
 using namespace ckg;
@@ -705,6 +706,108 @@ int ckg_bootstrap(ckg_boot* b, ckg_eval* ev, const ckg_ct* a, ckg_ct** out) {
 }
 
 uint32_t ckg_boot_output_level(const ckg_boot* b) { return b && b->b ? b->b->output_level() : 0; }
+
+// ---- bootstrap setup ---------------------------------------------------------------------
+
+int ckg_encode_complex(ckg_eval* ev, const double* values, uint32_t count, double scale, uint32_t level,
+                       ckg_pt** out) {
+  CKG_API_BEGIN
+  if (!values && count) throw Error(CKG_INVALID_PARAMS, "null values");
+  Evaluator& e = ev_of(ev);
+  e.ctx()->activate();
+  Pt p = encode_plaintext(e, values, count, scale, level);
+  check_launch();
+  *out = new ckg_pt{p};
+  CKG_API_END
+}
+
+int ckg_encode_complex_host(uint32_t log_n, const uint64_t* q, uint32_t nq, const double* values, uint32_t count,
+                            double scale, uint32_t level, uint64_t* out) {
+  CKG_API_BEGIN
+  if (log_n < 1 || log_n > 17) throw Error(CKG_INVALID_PARAMS, "log_n outside [1, 17]");
+  if (!q || !nq || !out || (!values && count)) throw Error(CKG_INVALID_PARAMS, "null argument");
+  auto v = encode_complex_coeffs(log_n, q, nq, values, count, scale, level);
+  memcpy(out, v.data(), v.size() * 8);
+  CKG_API_END
+}
+
+int ckg_boot_rotation_steps(const uint32_t* bp, int32_t* out, uint32_t cap, uint32_t* n) {
+  CKG_API_BEGIN
+  auto st = boot_rotation_steps(boot_params_of(bp));
+  if (n) *n = (uint32_t)st.size();
+  if (out)
+    for (uint32_t i = 0; i < cap && i < st.size(); ++i) out[i] = st[i];
+  CKG_API_END
+}
+
+int ckg_evalmod_coeffs(const uint32_t* bp, double* out, uint32_t cap) {
+  CKG_API_BEGIN
+  auto c = evalmod_coeffs(boot_params_of(bp));
+  if (!out || cap < c.size()) throw Error(CKG_INVALID_PARAMS, "output holds fewer than cheb_degree + 1 values");
+  memcpy(out, c.data(), c.size() * 8);
+  CKG_API_END
+}
+
+int ckg_boot_plan(const uint32_t* bp, int direction, uint32_t stage, int64_t* info, uint8_t* kept) {
+  CKG_API_BEGIN
+  if (!info) throw Error(CKG_INVALID_PARAMS, "null output");
+  auto plan = plan_boot_stages(boot_params_of(bp), direction);
+  if (stage >= plan.size()) throw Error(CKG_INVALID_PARAMS, "stage index out of range");
+  const StagePlan& p = plan[stage];
+  info[0] = p.d;
+  info[1] = p.stride;
+  info[2] = p.offset;
+  info[3] = p.has_second;
+  info[4] = (int64_t)plan.size();
+  if (kept)
+    for (uint32_t i = 0; i < p.d; ++i) {
+      kept[i] = p.kept[i];
+      kept[p.d + i] = p.has_second ? p.kept2[i] : 0;
+    }
+  CKG_API_END
+}
+
+int ckg_boot_stage_scales(ckg_ctx* ctx, const uint32_t* bp, double delta, double* out2) {
+  CKG_API_BEGIN
+  auto s = boot_stage_scales(ctx_of(ctx), boot_params_of(bp), delta);
+  out2[0] = s.first;
+  out2[1] = s.second;
+  CKG_API_END
+}
+
+int ckg_boot_encode_stages(ckg_eval* ev, const uint32_t* bp, int direction, double delta, ckg_lt** out,
+                           uint32_t cap) {
+  CKG_API_BEGIN
+  Evaluator& e = ev_of(ev);
+  e.ctx()->activate();
+  auto st = encode_boot_stages(e, boot_params_of(bp), direction, delta);
+  check_launch();
+  if (!out || cap < st.size()) throw Error(CKG_INVALID_PARAMS, "output holds fewer handles than stages");
+  for (size_t i = 0; i < st.size(); ++i) out[i] = new ckg_lt{st[i]};
+  CKG_API_END
+}
+
+int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double delta, const ckg_key* const* galois,
+                            uint32_t ngal, const ckg_key* to_sparse, const ckg_key* to_dense, ckg_boot** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  Evaluator& e = ev_of(ev);
+  e.ctx()->activate();
+  const BootParams b = boot_params_of(bp);
+  auto ctos = encode_boot_stages(e, b, DIR_COEFF_TO_SLOT, delta);
+  auto stoc = encode_boot_stages(e, b, DIR_SLOT_TO_COEFF, delta);
+  check_launch();
+  std::vector<KeyPtr> gk;
+  for (uint32_t i = 0; i < ngal; ++i) {
+    if (!galois || !galois[i] || !galois[i]->k) throw Error(CKG_INVALID_PARAMS, "null Galois key");
+    gk.push_back(galois[i]->k);
+  }
+  auto sc = boot_stage_scales(*e.ctx(), b, delta);
+  KeyPtr ts = to_sparse ? to_sparse->k : KeyPtr(), td = to_dense ? to_dense->k : KeyPtr();
+  *out = new ckg_boot{std::make_unique<Bootstrapper>(e.ctx(), b, ctos, stoc, gk, ts, td, evalmod_coeffs(b), sc.first,
+                                                     sc.second, delta)};
+  CKG_API_END
+}
 
 // ---- serving loop ------------------------------------------------------------------------
 

@@ -185,6 +185,14 @@ def _declare(L):
     L.ckg_bootstrap.argtypes = [VP, VP, VP, C.POINTER(VP)]
     L.ckg_boot_output_level.argtypes = [VP]
     L.ckg_boot_output_level.restype = C.c_uint32
+    L.ckg_encode_complex.argtypes = [VP, DP, C.c_uint32, C.c_double, C.c_uint32, C.POINTER(VP)]
+    L.ckg_encode_complex_host.argtypes = [C.c_uint32, U64P, C.c_uint32, DP, C.c_uint32, C.c_double, C.c_uint32, U64P]
+    L.ckg_boot_rotation_steps.argtypes = [U32P, I32P, C.c_uint32, U32P]
+    L.ckg_evalmod_coeffs.argtypes = [U32P, DP, C.c_uint32]
+    L.ckg_boot_plan.argtypes = [U32P, C.c_int, C.c_uint32, C.POINTER(C.c_int64), C.POINTER(C.c_uint8)]
+    L.ckg_boot_stage_scales.argtypes = [VP, U32P, C.c_double, DP]
+    L.ckg_boot_encode_stages.argtypes = [VP, U32P, C.c_int, C.c_double, C.POINTER(VP), C.c_uint32]
+    L.ckg_boot_create_encoded.argtypes = [VP, U32P, C.c_double, C.POINTER(VP), C.c_uint32, VP, VP, C.POINTER(VP)]
     L.ckg_server_create.argtypes = [VP, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(VP)]
     L.ckg_server_destroy.argtypes = [VP]
     L.ckg_server_add_owner.argtypes = [VP, U32P]
@@ -652,6 +660,14 @@ class CudaEvaluator:
         t = a.scale() if target_scale is None else target_scale
         return self._ct(lib().ckg_eval_chebyshev, a.h, c.ctypes.data_as(C.POINTER(C.c_double)), len(c), lo, hi, t)
 
+    def encode(self, values, scale, level):
+        """Encoder::encode_complex (encoder.rs:215-283) into a device plaintext."""
+        flat = _complex_pairs(values)
+        h = VP()
+        _check(lib().ckg_encode_complex(self.h, flat.ctypes.data_as(C.POINTER(C.c_double)), len(flat) // 2, scale,
+                                        level, C.byref(h)))
+        return Plaintext(self, h, level, scale)
+
     def eval_mod(self, a, bp, coeffs):
         b = (C.c_uint32 * 7)(*bp.words())
         c = np.ascontiguousarray(coeffs, np.float64)
@@ -851,6 +867,67 @@ class BootParams:
                 self.cheb_degree, self.double_angle)
 
 
+def _complex_pairs(values):
+    z = np.asarray(values, np.complex128).reshape(-1)
+    return np.ascontiguousarray(np.stack([z.real, z.imag], axis=-1).reshape(-1), np.float64)
+
+
+def _bp(bp):
+    return (C.c_uint32 * 7)(*bp.words())
+
+
+def encode_complex_host(log_n, q, values, scale, level):
+    """Host encoding over the data primes `q` (coefficient form, (level+1, 2^log_n))."""
+    flat = _complex_pairs(values)
+    qa = np.ascontiguousarray(q, np.uint64)
+    out = np.zeros((level + 1, 1 << log_n), np.uint64)
+    _check(lib().ckg_encode_complex_host(log_n, _p64(qa), len(qa), flat.ctypes.data_as(C.POINTER(C.c_double)),
+                                         len(flat) // 2, scale, level, _p64(out)))
+    return out
+
+
+def boot_rotation_steps(bp):
+    n = C.c_uint32()
+    _check(lib().ckg_boot_rotation_steps(_bp(bp), None, 0, C.byref(n)))
+    out = (C.c_int32 * max(n.value, 1))()
+    _check(lib().ckg_boot_rotation_steps(_bp(bp), out, n.value, C.byref(n)))
+    return list(out[:n.value])
+
+
+def evalmod_coeffs(bp):
+    out = np.zeros(bp.cheb_degree + 1, np.float64)
+    _check(lib().ckg_evalmod_coeffs(_bp(bp), out.ctypes.data_as(C.POINTER(C.c_double)), len(out)))
+    return out
+
+
+def boot_plan(bp, direction):
+    """[(d, stride, offset, kept, kept_second or None)] for each stage of a direction."""
+    out = []
+    k = 0
+    while True:
+        info = (C.c_int64 * 5)()
+        _check(lib().ckg_boot_plan(_bp(bp), direction, k, info, None))
+        d = info[0]
+        kept = (C.c_uint8 * (2 * d))()
+        _check(lib().ckg_boot_plan(_bp(bp), direction, k, info, kept))
+        out.append((d, info[1], info[2], [bool(x) for x in kept[:d]], [bool(x) for x in kept[d:]] if info[3] else None))
+        k += 1
+        if k >= info[4]:
+            return out
+
+
+def boot_encode_stages(ev, bp, direction, delta):
+    n = bp.ctos_levels if direction == 0 else bp.stoc_levels
+    arr = (VP * n)()
+    _check(lib().ckg_boot_encode_stages(ev.h, _bp(bp), direction, delta, arr, n))
+    stages = []
+    for i in range(n):
+        lt = LinearTransform.__new__(LinearTransform)
+        lt.h, lt._keep, lt.direction = VP(arr[i]), (), direction
+        stages.append(lt)
+    return stages
+
+
 class LinearTransform:
     """One CoeffToSlot (direction 0) or SlotToCoeff (1) stage of encoded diagonals
     (bootstrap/linear.rs:482-497); entries / second: d Plaintexts or None (zero diagonal)."""
@@ -890,6 +967,19 @@ class Bootstrapper:
         _check(lib().ckg_boot_create(ctx.h, b, a1, len(ctos), a2, len(stoc), g, len(galois_keys),
                                      to_sparse.h if to_sparse else None, to_dense.h if to_dense else None,
                                      c.ctypes.data_as(C.POINTER(C.c_double)), len(c), sc, C.byref(self.h)))
+
+    @classmethod
+    def encoded(cls, ev, bp, delta, galois_keys, to_sparse=None, to_dense=None):
+        """Stages and EvalMod series encoded by the library itself (ckg_boot_create_encoded)."""
+        self = cls.__new__(cls)
+        self.ctx, self.bp = ev.ctx, bp
+        self._keep = (list(galois_keys), to_sparse, to_dense)
+        g = (VP * max(len(galois_keys), 1))(*[k.h for k in galois_keys])
+        self.h = VP()
+        _check(lib().ckg_boot_create_encoded(ev.h, _bp(bp), delta, g, len(galois_keys),
+                                             to_sparse.h if to_sparse else None, to_dense.h if to_dense else None,
+                                             C.byref(self.h)))
+        return self
 
     def __del__(self):
         try:

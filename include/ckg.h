@@ -274,6 +274,35 @@ CKG_API void ckg_boot_destroy(ckg_boot* b);
 CKG_API int ckg_bootstrap(ckg_boot* b, ckg_eval* ev, const ckg_ct* a, ckg_ct** out);
 CKG_API uint32_t ckg_boot_output_level(const ckg_boot* b);
 
+/* ---- bootstrap setup (what the reference's Bootstrapper::new prepares on the host,
+ * bootstrapper.rs:250-290): the encoder (encoder.rs:215-283), the special-DFT stages adapted
+ * and encoded at their exact diagonal scales (linear.rs:401-677, linalg.rs:334-369), their
+ * rotation steps (linear.rs:432-450) and the EvalMod series (evalmod.rs:58-96). The f64 steps
+ * follow the reference's operation order, so encodings carry the reference's integers.
+ * Functions marked host need no GPU. Keys are not generated here (they are the owner's). */
+/* values: `count` complex numbers as (re, im) pairs; NTT-form device plaintext at `level`. */
+CKG_API int ckg_encode_complex(ckg_eval* ev, const double* values, uint32_t count, double scale, uint32_t level,
+                               ckg_pt** out);
+/* host: the same encoding over the data primes q[0..nq), coefficient form, (level+1) x 2^log_n. */
+CKG_API int ckg_encode_complex_host(uint32_t log_n, const uint64_t* q, uint32_t nq, const double* values,
+                                    uint32_t count, double scale, uint32_t level, uint64_t* out);
+/* host: rotation steps of both transforms (n set to the count; out may be NULL). */
+CKG_API int ckg_boot_rotation_steps(const uint32_t* bp, int32_t* out, uint32_t cap, uint32_t* n);
+/* host: the cheb_degree + 1 EvalMod coefficients. */
+CKG_API int ckg_evalmod_coeffs(const uint32_t* bp, double* out, uint32_t cap);
+/* host: layout of stage `stage` of a direction: info = {d, stride, offset, has_second,
+ * stages}; kept[i] / kept[d + i]: entry i of the main / second diagonals is stored. */
+CKG_API int ckg_boot_plan(const uint32_t* bp, int direction, uint32_t stage, int64_t* info, uint8_t* kept);
+/* (evalmod_scale, stoc_input_scale) for inputs at scale delta (bootstrapper.rs:207-230). */
+CKG_API int ckg_boot_stage_scales(ckg_ctx* ctx, const uint32_t* bp, double delta, double* out2);
+/* All stages of a direction, encoded on this evaluator's context (out holds `cap` handles). */
+CKG_API int ckg_boot_encode_stages(ckg_eval* ev, const uint32_t* bp, int direction, double delta, ckg_lt** out,
+                                   uint32_t cap);
+/* A bootstrapper whose stages and EvalMod series are encoded here (ckg_boot_create with
+ * ckg_boot_encode_stages, ckg_evalmod_coeffs and ckg_boot_stage_scales). */
+CKG_API int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double delta, const ckg_key* const* galois,
+                                    uint32_t ngal, const ckg_key* to_sparse, const ckg_key* to_dense, ckg_boot** out);
+
 /* ---- serving loop ----------------------------------------------------------------------
  * No counterpart in the reference, which runs one HeOps call at a time. A server admits
  * requests from many key owners as they arrive and runs them with continuous batching:

@@ -159,6 +159,8 @@ def _declare(L):
     L.orc_boot_mul_const.argtypes = [vp, vp, C.c_double, C.c_double, C.POINTER(vp)]
     L.orc_boot_add_const.argtypes = [vp, vp, C.c_double, C.POINTER(vp)]
     L.orc_mul_by_x_half.argtypes = [vp, vp, C.POINTER(vp)]
+    L.orc_boot_plan.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_uint64,
+                                C.POINTER(C.c_int64), C.POINTER(C.c_uint8)]
 
 
 def _p64(a):
@@ -790,3 +792,19 @@ def mul_by_x_half(ev, ct):
     h = C.c_void_p()
     _check(lib().orc_mul_by_x_half(ev.h, ct.h, C.byref(h)))
     return Ct(ev, h)
+
+
+def boot_plan(log_slots, ctos_levels, stoc_levels, k_intervals, direction):
+    """[(d, stride, offset, kept, kept_second or None)] per stage (no keys, no encoding)."""
+    out = []
+    k = 0
+    while True:
+        info = (C.c_int64 * 5)()
+        _check(lib().orc_boot_plan(log_slots, ctos_levels, stoc_levels, k_intervals, direction, k, info, None))
+        d = info[0]
+        kept = (C.c_uint8 * (2 * d))()
+        _check(lib().orc_boot_plan(log_slots, ctos_levels, stoc_levels, k_intervals, direction, k, info, kept))
+        out.append((d, info[1], info[2], [bool(x) for x in kept[:d]], [bool(x) for x in kept[d:]] if info[3] else None))
+        k += 1
+        if k >= info[4]:
+            return out

@@ -193,3 +193,52 @@ def test_bootstrap_errors(boot):
     with pytest.raises(b.ckg.InvalidParams):
         b.dev_bs.bootstrap(no_rk, no_rk.upload_ct(random_ct(P, 53, 0), DELTA))
     assert ev.counter()["bootstraps"] == 0
+
+
+N16_Q = [54] + [42] * 16 + [34] * 4 + [58] * 7 + [56] * 4  # params.rs n16_boot
+
+
+def test_n16_boot_bootstrap(ckg, oracle):
+    """n16_boot (N = 2^16, 32 + 4 primes, dnum 8) with BootParams::default_n16: the library
+    encodes its own stages and EvalMod series; the bootstrap is bit-identical to the
+    oracle's, performs the reference's 111 key switches (69 rotations, 40 relinearizations,
+    2 SSE switches, docs/bootstrap.md §11.2) and keeps >= 16 bits (the reference measures
+    17.46 on this chain)."""
+    import time
+    P = oracle.Params.from_bits(16, N16_Q, [60] * 4, 42, 8)
+    kg = oracle.KeyGenerator(P, 9)
+    enc = oracle.Encoder(P)
+    rk = kg.relin_key()
+    bs = oracle.Bootstrapper(P, kg, enc, 15)
+    ctx = ckg.Context(16, P.q, P.p, 8, scale=DELTA)
+    d_rk = ctx.upload_key(rk.export())
+    d_gk = [ctx.upload_key(k.export(), e) for e, k in bs.galois_keys().items()]
+    ts, td = bs.sse_keys()
+    d_ts, d_td = ctx.upload_key(ts.export()), ctx.upload_key(td.export())
+    ev_gpu = ckg.CudaEvaluator(ctx, d_rk, [])
+    dev = ckg.Bootstrapper.encoded(ev_gpu, ckg.BootParams(), DELTA, d_gk, d_ts, d_td)
+    assert dev.output_level() == bs.output_level() == 16
+    rng = np.random.default_rng(17)
+    m = rng.uniform(-1, 1, P.n // 2)
+    ev_cpu = oracle.Evaluator(P, rk)
+    ct = oracle.encrypt_sk(ev_cpu, kg, 5, enc.encode(m, DELTA, P.max_level), DELTA)
+    ct0 = ev_cpu.mod_switch_to_level(ct, 0)
+    g0 = ev_gpu.upload_ct(ct0.data(), DELTA)
+    got = dev.bootstrap(ev_gpu, g0)  # warm-up (Galois tables, pools)
+    ev_gpu.reset_counter()
+    ctx.sync()
+    t = time.perf_counter()
+    got = dev.bootstrap(ev_gpu, g0)
+    ctx.sync()
+    ms = (time.perf_counter() - t) * 1e3
+    want = bs.bootstrap(ev_cpu, ct0)
+    data, scale = ev_gpu.download_ct(got)
+    assert scale == want.scale == DELTA and got.level() == want.level == 16
+    assert_same(data, want.data(), "n16_boot bootstrap")
+    c = ev_gpu.counter()
+    assert c == ev_cpu.counter()
+    assert (c["rotations"], c["relins"], c["sse_switches"], c["bootstraps"]) == (69, 40, 2, 1)
+    dec = enc.decode(oracle.decrypt(kg, want), want.scale)
+    bits = -np.log2(np.abs(dec.real - m).max())
+    print(f"n16_boot bootstrap on the GPU: {ms:.1f} ms wall (host-synchronised), precision {bits:.2f} bits")
+    assert bits >= 16.0
