@@ -1,5 +1,8 @@
 """Key-switching throughput of the B200 RNS-CKKS evaluator path (one JSON line).
 
+Beside it: `bootstrap` -- one full n16_boot bootstrap (ms, device events) -- and `serving`
+-- the serving loop's throughput and p50/p99 latency under Poisson arrivals.
+
 Parameters: N = 2^16, 24 x 50-bit data primes + 8 x 60-bit special primes, dnum = 3
 (alpha = 8), 31 evaluation keys (relinearization + 30 Galois keys for +-2^k, k = 0..14).
 
@@ -47,6 +50,10 @@ MIX_OPS = 512
 MIX_LIMBS = (4, 24)
 PLAIN_CTS = 128
 PLAIN_LEVEL = 23
+BOOT_Q_BITS = [54] + [42] * 16 + [34] * 4 + [58] * 7 + [56] * 4  # n16_boot: 32 data primes
+BOOT_P_BITS = [60] * 4
+BOOT_DNUM = 8
+BOOT_DELTA = 2.0 ** 42
 SERVE_OWNERS = 32
 SERVE_D = 64                 # BSGS mat-vec diagonals: baby 8, giant 8
 SERVE_BUDGET = 24 << 30      # HBM bytes for cached keys + queued work: about half the owners
@@ -401,6 +408,86 @@ class Serving:
         self.srv.close()
 
 
+class BootBench:
+    """One full bootstrap on the n16_boot chain (N = 2^16, 32 data primes of 54/42/34/58/56
+    bits, 4 x 60-bit special primes, dnum 8) with BootParams::default_n16 (SSE h' = 32, K = 13,
+    degree 127, CoeffToSlot 4 / EvalMod 7 / SlotToCoeff 4 levels): mod-raise, CoeffToSlot,
+    two EvalMods, SlotToCoeff, 111 key switches. The library encodes the stages and the EvalMod
+    series itself; the 35 keys (relinearization, 32 rotations, conjugation, the two SSE
+    switches) are synthetic uniform key material, since a bootstrap's time does not depend on
+    the key values, and the input is a uniform level-0 ciphertext."""
+
+    def __init__(self, ckg, torch, device):
+        self.ckg, self.torch = ckg, torch
+        q, p = ckg.primes_for_bits(16, BOOT_Q_BITS, BOOT_P_BITS)
+        self.ctx = ckg.Context(16, q, p, BOOT_DNUM, device=device)
+        ctx, n = self.ctx, 1 << 16
+        gen = torch.Generator(device=f"cuda:{device}")
+        gen.manual_seed(424242 + device)
+        qall = torch.tensor(q + p, dtype=torch.int64, device=f"cuda:{device}")
+        k = len(p)
+
+        def uniform(shape, qcol):
+            t = torch.randint(0, 1 << 62, shape, generator=gen, device=qall.device, dtype=torch.int64) % qcol
+            torch.cuda.synchronize()
+            return t
+
+        def key(parts, qlimbs, elt):
+            shape = (parts, 2, qlimbs + k, n)
+            qcol = torch.cat([qall[:qlimbs], qall[len(q):]]).view(1, 1, -1, 1)
+            t = uniform(shape, qcol)
+            kk = ctx.upload_key_device(t.data_ptr(), shape, elt)
+            del t
+            return kk
+
+        bp = ckg.BootParams()
+        relin = key(BOOT_DNUM, len(q), 0)
+        self.galois = [key(BOOT_DNUM, len(q), galois_elt(n, s)) for s in ckg.boot_rotation_steps(bp)]
+        self.galois.append(key(BOOT_DNUM, len(q), 2 * n - 1))
+        self.to_sparse, self.to_dense = key(1, 1, 0), key(BOOT_DNUM, len(q), 0)
+        self.key_bytes = sum(x.nbytes for x in self.galois) + relin.nbytes + self.to_sparse.nbytes + \
+            self.to_dense.nbytes
+        self.ev = ckg.CudaEvaluator(ctx, relin, [])
+        t0 = time.time()
+        self.bs = ckg.Bootstrapper.encoded(self.ev, bp, BOOT_DELTA, self.galois, self.to_sparse, self.to_dense)
+        ctx.sync()
+        self.setup_s = time.time() - t0
+        self.setup_launches = ckg.launch_count()
+        t = uniform((2, 1, n), qall[:1].view(1, 1, 1))
+        self.ct = self.ev.upload_ct_device(t.data_ptr(), 2, 0, BOOT_DELTA)
+        ctx.sync()
+        del t
+        self.out = None
+
+    def step(self):
+        self.out = self.bs.bootstrap(self.ev, self.ct)
+
+    def measure(self, steps=5, warmup=2):
+        ckg, torch = self.ckg, self.torch
+        self.step()
+        self.ctx.sync()
+        l0 = ckg.launch_count()
+        self.ev.reset_counter()
+        self.step()
+        self.ctx.sync()
+        launches = ckg.launch_count() - l0
+        c = self.ev.counter()
+        ms, _ = timed(torch, self.ctx, self.step, steps, warmup)
+        t0 = time.perf_counter()
+        self.step()
+        self.ctx.sync()
+        wall = (time.perf_counter() - t0) * 1e3
+        return {"ms": round(ms / steps, 3), "unit": "ms per bootstrap (device events, back-to-back)",
+                "single_call_wall_ms": round(wall, 3), "target_ms": 150,
+                "params": "n16_boot: N=2^16, 32 q primes (54, 42x16, 34x4, 58x7, 56x4 bits) + 4x60-bit P, "
+                          "dnum 8; SSE h'=32, K=13, Chebyshev degree 127, CtS/EvalMod/StC 4/7/4 levels",
+                "key_switches": c["rotations"] + c["relins"] + c["sse_switches"],
+                "counts": c, "launches": int(launches), "setup_launches": int(self.setup_launches),
+                "output_level": self.bs.output_level(),
+                "setup_s": round(self.setup_s, 2), "key_gib": round(self.key_bytes / 2 ** 30, 2),
+                "data": "synthetic uniform key material and level-0 input; stages encoded by the library"}
+
+
 def max_over_ranks(dist, ms, device="cuda"):
     """The slowest rank's time: every rank's device-measured milliseconds, max-reduced."""
     import torch
@@ -527,10 +614,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ops", type=int, default=MIX_OPS, help="ops of the batched stream (smaller for profiling)")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-boot", action="store_true")
+    ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
     ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
-    ap.add_argument("--profile", default=None, choices=["batch", "plain"],
+    ap.add_argument("--profile", default=None, choices=["batch", "plain", "boot"],
                     help="run the set-up and `warmup` + 1 step of one path, print nothing (for ncu)")
     args = ap.parse_args()
 
@@ -582,6 +671,17 @@ def main():
     except Exception:
         pass
 
+    if args.profile == "boot":
+        B = BootBench(ckg, torch, local)
+        for _ in range(args.warmup + 1):
+            B.step()
+        B.ctx.sync()
+        return
+    if args.boot_only:
+        out = BootBench(ckg, torch, local).measure()
+        if rank == 0:
+            print(json.dumps({"bootstrap": out}))
+        return
     S = Setup(ckg, torch, local)
     if args.serve_only:
         sv = Serving(S, owners=args.serve_owners)
@@ -630,6 +730,10 @@ def main():
                  "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
     roof = ntt_roofline(torch, S, peaks)
+    boot = None
+    if not args.no_boot:
+        mix.batch = None
+        boot = BootBench(ckg, torch, local).measure()
     serving = None
     if not args.no_serve:
         mix.batch = None
@@ -648,7 +752,7 @@ def main():
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
                 "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
-                "serving": serving, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "bootstrap": boot, "serving": serving, "cpu_baseline": cpu, "clocks": clk.summary()}
         print(json.dumps(line))
     mix.batch = None
     S.ctx.sync()
