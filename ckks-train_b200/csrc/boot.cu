@@ -265,18 +265,44 @@ Ct Evaluator::matvec_plain_sum_sparse(const std::vector<std::pair<const SparseDi
           block = block ? add(block, t) : t;
         }
     } else {
-      Ct inner;
+      std::vector<std::pair<Ct, Pt>> prods;
       for (size_t ti = 0; ti < terms.size(); ++ti)
         for (uint32_t k2 = 0; k2 < baby; ++k2) {
           const Pt& w = terms[ti].first->entries[k1 * baby + k2];
-          if (!w) continue;
-          Ct t = mul_plain(xs[ti][k2], w);
-          inner = inner ? add(inner, t) : t;
+          if (w) prods.push_back({xs[ti][k2], w});
         }
-      if (inner) block = shift != 0 ? rotate(inner, (int32_t)shift) : inner;
+      if (!prods.empty()) {
+        Ct inner = mac_plain(prods);
+        block = shift != 0 ? rotate(inner, (int32_t)shift) : inner;
+      }
     }
     if (block) acc = acc ? add(acc, block) : block;
   }
+  return acc;
+}
+
+Ct Evaluator::mac_plain(const std::vector<std::pair<Ct, Pt>>& terms) {
+  const Ct& x0 = terms[0].first;
+  const uint32_t level = x0->level;
+  ctx_->activate();
+  Ct acc;
+  for (size_t first = 0; first < terms.size(); first += kMaxMacTerms) {
+    const size_t cnt = std::min<size_t>(kMaxMacTerms, terms.size() - first);
+    Ct r = new_ct(2, level, x0->scale * terms[0].second->scale);
+    MacBatch b{};
+    b.count = (int)cnt;
+    b.limbs = (int)level + 1;
+    b.out0 = r->comp_mut(0);
+    b.out1 = r->comp_mut(1);
+    for (size_t t = 0; t < cnt; ++t) {
+      b.x0[t] = terms[first + t].first->comp(0);
+      b.x1[t] = terms[first + t].first->comp(1);
+      b.w[t] = terms[first + t].second->data();
+    }
+    launch_mac_plain(ctx_->dt, b, ctx_->stream);
+    acc = acc ? add(acc, r) : r;
+  }
+  count([&](OpCounter& c) { c.ct_pt_mults += terms.size(); });
   return acc;
 }
 

@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <type_traits>
+
 #include "evaluator.hpp"
 
 namespace ckg {
@@ -508,9 +510,15 @@ Ct Evaluator::bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, c
       }
     } else {
       Ct inner;
-      for (uint32_t k2 = 0; k2 < baby; ++k2) {
-        Ct t = mul(entries[k1 * baby + k2], xs[k2]);
-        inner = inner ? add(inner, t) : t;
+      if constexpr (std::is_same<T, Pt>::value) {  // plaintext diagonals: one fused pass
+        std::vector<std::pair<Ct, Pt>> prods;
+        for (uint32_t k2 = 0; k2 < baby; ++k2) prods.push_back({xs[k2], entries[k1 * baby + k2]});
+        inner = mac_plain(prods);
+      } else {
+        for (uint32_t k2 = 0; k2 < baby; ++k2) {
+          Ct t = mul(entries[k1 * baby + k2], xs[k2]);
+          inner = inner ? add(inner, t) : t;
+        }
       }
       block = finish(inner);
       if (shift != 0) block = rotate(block, (int32_t)shift);

@@ -113,6 +113,9 @@ class Evaluator {
   // Sum over terms of diag_t * x_t with shared giant rotations, skipping null entries and
   // the baby rotations only they would use (linalg.rs:741-799).
   Ct matvec_plain_sum_sparse(const std::vector<std::pair<const SparseDiag*, Ct>>& terms);
+  // sum_t mul_plain(x_t, w_t) in one pass (operands checked by the caller: 2 components,
+  // one level, equal scales); counts one ct_pt_mults per term as the separate ops would.
+  Ct mac_plain(const std::vector<std::pair<Ct, Pt>>& terms);
 
   // BootstrapArithmetic (bootstrap/poly.rs:453-486), ModRaise (bootstrap/modraise.rs) and
   // the exact monomial product of CoeffToSlot (bootstrap/linear.rs:921-936).

@@ -635,6 +635,25 @@ __global__ void __launch_bounds__(256)
   r.dst[c] = mode == 0 ? mul_shoup(r.src[c], st.w[r.prime], st.ws[r.prime], q) : add_mod(r.src[c], st.w[r.prime], q);
 }
 
+// One pass over every term's limb: 128-bit accumulation of up to kMaxMacTerms products
+// (each < 2^120), one reduction per output word.
+__global__ void __launch_bounds__(256)
+    k_mac_plain(const __grid_constant__ MacBatch b, const PrimeConst* __restrict__ pc, int n) {
+  const int i = blockIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const size_t off = (size_t)i * n + c;
+  uint64_t h0 = 0, l0 = 0, h1 = 0, l1 = 0;
+  for (int t = 0; t < b.count; ++t) {
+    const uint64_t w = __ldg(b.w[t] + off);
+    mac128(h0, l0, __ldg(b.x0[t] + off), w);
+    mac128(h1, l1, __ldg(b.x1[t] + off), w);
+  }
+  const PrimeConst P = pc[i];
+  b.out0[off] = reduce128(h0, l0, P);
+  b.out1[off] = reduce128(h1, l1, P);
+}
+
 // Centered lift of a level-0 coefficient-form limb (src of every ref) into prime r.prime:
 // residues above (q_0 - 1) / 2 are read as negative (poly.rs:298-345).
 __global__ void __launch_bounds__(256)
@@ -914,6 +933,12 @@ void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const Sca
     k_scalar<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, table, d.prime, n, mode);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
+}
+
+void launch_mac_plain(const DevTables& d, const MacBatch& b, cudaStream_t st) {
+  const int n = 1 << d.log_n;
+  k_mac_plain<<<dim3((n + 255) / 256, b.limbs), 256, 0, st>>>(b, d.prime, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_lift_level0(const DevTables& d, const LimbRef* refs, int count, cudaStream_t st) {

@@ -137,6 +137,19 @@ struct TensorBatch {
   TensorRef r[kMaxTensor];
 };
 
+// Fused plaintext multiply-accumulate over the limbs of 2-component ciphertexts:
+// out_c[i] = sum_t x_c[t][i] * w[t][i] (c = 0, 1), limb i at offset i * N of every base
+// pointer, prime index i.
+constexpr int kMaxMacTerms = 48;
+struct MacBatch {
+  int count, limbs;
+  uint64_t* out0;
+  uint64_t* out1;
+  const uint64_t* x0[kMaxMacTerms];
+  const uint64_t* x1[kMaxMacTerms];
+  const uint64_t* w[kMaxMacTerms];
+};
+
 // Multiplication of limbs by a per-prime constant (Shoup pair per global prime index).
 constexpr int kMaxPrimes = 64;
 struct ScalarTable {
