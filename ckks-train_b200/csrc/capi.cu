@@ -846,6 +846,26 @@ int ckg_server_add_key(ckg_server* s, uint32_t owner, const uint64_t* key, int d
   CKG_API_END
 }
 
+int ckg_server_add_sse_keys(ckg_server* s, uint32_t owner, const uint64_t* to_sparse, const uint64_t* to_dense,
+                            int device_src) {
+  CKG_API_BEGIN
+  server_of(s).add_sse_keys(owner, to_sparse, to_dense, device_src != 0);
+  CKG_API_END
+}
+
+int ckg_server_enable_bootstrap(ckg_server* s, const uint32_t* bp, double delta) {
+  CKG_API_BEGIN
+  server_of(s).enable_bootstrap(boot_params_of(bp), delta);
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_server_submit_bootstrap(ckg_server* s, uint32_t owner, const ckg_ct* a, uint64_t* id) {
+  CKG_API_BEGIN
+  *id = server_of(s).submit_bootstrap(owner, ct_of(a));
+  CKG_API_END
+}
+
 int ckg_server_submit_mul(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_ct* b, uint64_t* id) {
   CKG_API_BEGIN
   *id = server_of(s).submit_mul(owner, ct_of(a), ct_of(b));

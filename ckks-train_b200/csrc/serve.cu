@@ -4,6 +4,7 @@
 #include <set>
 #include <unordered_set>
 
+#include "bootsetup.hpp"
 #include "serve.hpp"
 
 namespace ckg {
@@ -16,16 +17,33 @@ double us_since(std::chrono::steady_clock::time_point t0, std::chrono::steady_cl
 
 }  // namespace
 
+// A flight is what one worker iteration queued on the device: the batch of key-switching
+// ops, then each mat-vec and each bootstrap, every one closed by its own event (a segment), so
+// a request completes when its own work does.
 struct Server::Flight {
-  cudaEvent_t done = nullptr;
-  std::map<uint32_t, std::unique_ptr<Evaluator>> evs;  // per owner, holding the batch's keys
+  struct Segment {
+    cudaEvent_t done = nullptr;
+    std::vector<ReqPtr> reqs;
+  };
+  std::vector<Segment> segs;
+  std::map<uint32_t, std::unique_ptr<Evaluator>> evs;  // per owner, holding the flight's keys
   std::unique_ptr<Batch> batch;                        // refers to evs: released first
+  std::vector<std::unique_ptr<Bootstrapper>> boots;
   std::vector<ReqPtr> reqs;
   size_t work = 0;
   ~Flight() {
     batch.reset();
+    boots.clear();
     evs.clear();
-    if (done) cudaEventDestroy(done);
+    for (auto& s : segs)
+      if (s.done) cudaEventDestroy(s.done);
+  }
+  void close_segment(cudaStream_t st, std::vector<ReqPtr> rs) {
+    Segment s;
+    s.reqs = std::move(rs);
+    if (cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) s.done = nullptr;
+    if (s.done) cudaEventRecord(s.done, st);
+    segs.push_back(std::move(s));
   }
 };
 
@@ -70,8 +88,11 @@ Server::~Server() {
     ctx_->activate();
   } catch (...) {
   }
+  boot_ctos_.clear();
+  boot_stoc_.clear();
   for (auto& o : owners_) {  // device copies are freed on the copy stream before it goes
-    if (o->relin) o->relin->dev.reset();
+    for (auto* hk : {o->relin.get(), o->to_sparse.get(), o->to_dense.get()})
+      if (hk) hk->dev.reset();
     for (auto& g : o->galois) g.second->dev.reset();
   }
   owners_.clear();
@@ -97,8 +118,21 @@ void Server::add_key(uint32_t owner, const uint64_t* src, bool device_src, uint3
     if (elt ? o.galois.count(elt) != 0 : (bool)o.relin)
       throw Error(ST_INVALID_PARAMS, "the owner already has this key");
   }
+  auto hk = host_key(src, device_src, parts, q_limbs, elt);
+  hk->role = elt ? 1 : 0;
+  std::lock_guard<std::mutex> lk(mu_);
+  Owner& o = *owners_[owner];
+  if (elt ? o.galois.count(elt) != 0 : (bool)o.relin) throw Error(ST_INVALID_PARAMS, "the owner already has this key");
+  if (elt)
+    o.galois[elt] = std::move(hk);
+  else
+    o.relin = std::move(hk);
+}
+
+std::unique_ptr<Server::HostKey> Server::host_key(const uint64_t* src, bool device_src, uint32_t parts,
+                                                 uint32_t q_limbs, uint64_t elt) {
   auto hk = std::make_unique<HostKey>();
-  hk->words = (size_t)parts * 2 * (q_limbs + c.k) * c.n;
+  hk->words = (size_t)parts * 2 * (q_limbs + ctx_->k) * ctx_->n;
   hk->parts = parts;
   hk->q_limbs = q_limbs;
   hk->elt = elt;
@@ -110,13 +144,48 @@ void Server::add_key(uint32_t owner, const uint64_t* src, bool device_src, uint3
   } else {
     std::copy(src, src + hk->words, hk->host);
   }
+  return hk;
+}
+
+void Server::add_sse_keys(uint32_t owner, const uint64_t* to_sparse, const uint64_t* to_dense, bool device_src) {
+  if (!to_sparse || !to_dense) throw Error(ST_INVALID_PARAMS, "null key data");
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (owner >= owners_.size()) throw Error(ST_INVALID_PARAMS, "unknown key owner");
+    if (owners_[owner]->to_sparse) throw Error(ST_INVALID_PARAMS, "the owner already has SSE keys");
+  }
+  auto ts = host_key(to_sparse, device_src, 1, 1, 0);  // modraise.rs:109-129 shapes
+  auto td = host_key(to_dense, device_src, ctx_->dnum, ctx_->L + 1, 0);
+  ts->role = 2;
+  td->role = 3;
   std::lock_guard<std::mutex> lk(mu_);
   Owner& o = *owners_[owner];
-  if (elt ? o.galois.count(elt) != 0 : (bool)o.relin) throw Error(ST_INVALID_PARAMS, "the owner already has this key");
-  if (elt)
-    o.galois[elt] = std::move(hk);
-  else
-    o.relin = std::move(hk);
+  if (o.to_sparse) throw Error(ST_INVALID_PARAMS, "the owner already has SSE keys");
+  o.to_sparse = std::move(ts);
+  o.to_dense = std::move(td);
+}
+
+void Server::enable_bootstrap(const BootParams& bp, double delta) {
+  Evaluator enc(ctx_, nullptr, {}, cfg_.eval);  // keyless: only encodes
+  auto ctos = encode_boot_stages(enc, bp, DIR_COEFF_TO_SLOT, delta);
+  auto stoc = encode_boot_stages(enc, bp, DIR_SLOT_TO_COEFF, delta);
+  auto coeffs = evalmod_coeffs(bp);
+  auto sc = boot_stage_scales(*ctx_, bp, delta);
+  std::vector<uint64_t> elts;
+  for (int32_t s : boot_rotation_steps(bp)) elts.push_back(galois_elt(ctx_->n, s));
+  elts.push_back(2 * ctx_->n - 1);
+  CKG_CUDA(cudaStreamSynchronize(ctx_->stream));
+  std::lock_guard<std::mutex> lk(mu_);
+  if (boot_) throw Error(ST_INVALID_PARAMS, "bootstrap requests are already enabled");
+  boot_bp_ = bp;
+  boot_delta_ = delta;
+  boot_ctos_ = std::move(ctos);
+  boot_stoc_ = std::move(stoc);
+  boot_coeffs_ = std::move(coeffs);
+  boot_em_ = sc.first;
+  boot_si_ = sc.second;
+  boot_elts_ = std::move(elts);
+  boot_ = true;
 }
 
 // ---- submission ----------------------------------------------------------------------
@@ -194,6 +263,21 @@ uint64_t Server::submit_matvec(uint32_t owner, uint32_t d, uint32_t stride, cons
       r->work_bytes = ((baby + 6) * ct_words + conv_limbs(*ctx_, x->level) * ctx_->n + ks) * 8;
     }
   }
+  return enqueue(r);
+}
+
+uint64_t Server::submit_bootstrap(uint32_t owner, const Ct& a) {
+  auto r = std::make_shared<Req>();
+  r->owner = owner;
+  r->kind = REQ_BOOTSTRAP;
+  r->a = a;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!boot_) throw Error(ST_INVALID_PARAMS, "bootstrap requests are not enabled on this server");
+  }
+  // ciphertexts at the top level and the hoisted key-switch scratch of the widest stage
+  const size_t ct_words = 2 * (size_t)(ctx_->L + 1) * ctx_->n;
+  r->work_bytes = (32 * ct_words + 8 * key_switch_scratch_words(*ctx_, ctx_->L)) * 8;
   return enqueue(r);
 }
 
@@ -287,10 +371,20 @@ void Server::keys_of(Req& r) {
     if (it != o.galois.end() && std::find(r.keys.begin(), r.keys.end(), it->second.get()) == r.keys.end())
       r.keys.push_back(it->second.get());
   };
-  if (r.kind == REQ_MUL && o.relin) r.keys.push_back(o.relin.get());
+  if ((r.kind == REQ_MUL || r.kind == REQ_BOOTSTRAP) && o.relin) r.keys.push_back(o.relin.get());
   if (r.kind == REQ_ROTATE) galois(r.steps);
   if (r.kind == REQ_MATVEC && r.d && (r.d & (r.d - 1)) == 0)
     for (int32_t s : rotation_steps(r.d, r.stride)) galois(s);
+  if (r.kind == REQ_BOOTSTRAP) {
+    for (uint64_t e : boot_elts_) {
+      auto it = o.galois.find(e);
+      if (it != o.galois.end()) r.keys.push_back(it->second.get());
+    }
+    if (o.to_sparse && o.to_dense) {
+      r.keys.push_back(o.to_sparse.get());
+      r.keys.push_back(o.to_dense.get());
+    }
+  }
 }
 
 KeyPtr Server::upload(HostKey* hk) {
@@ -342,6 +436,10 @@ void Server::worker() {
       ReqPtr r = pending_.front();
       keys_of(*r);
       if (!batch.empty() && ks + r->ks > cfg_.max_batch_ks) break;
+      if (r->kind == REQ_BOOTSTRAP && std::any_of(batch.begin(), batch.end(), [](const ReqPtr& x) {
+            return x->kind == REQ_BOOTSTRAP;
+          }))
+        break;  // one bootstrap per flight
       size_t extra = 0;
       for (HostKey* hk : r->keys)
         if (!hk->dev && !need_set.count(hk)) extra += hk->words * 8;
@@ -448,9 +546,9 @@ void Server::worker() {
         auto& slot = keys[r->owner];
         for (HostKey* hk : r->keys) {
           if (!hk->dev) continue;
-          if (hk->elt == 0)
+          if (hk->role == 0)
             slot.first = hk->dev;
-          else if (std::find(slot.second.begin(), slot.second.end(), hk->dev) == slot.second.end())
+          else if (hk->role == 1 && std::find(slot.second.begin(), slot.second.end(), hk->dev) == slot.second.end())
             slot.second.push_back(hk->dev);
         }
       }
@@ -458,15 +556,20 @@ void Server::worker() {
         f->evs[kv.first] = std::make_unique<Evaluator>(ctx_, kv.second.first, kv.second.second, cfg_.eval);
     }
     std::set<uint32_t> owners_in_batch;
+    std::unordered_set<const Req*> placed;  // requests whose work closed a segment
+    auto failed_req = [&](const ReqPtr& r) {
+      return std::any_of(errs.begin(), errs.end(), [&](auto& x) { return x.first == r; });
+    };
     try {
       f->batch = std::make_unique<Batch>(f->evs.begin()->second.get());
+      std::vector<ReqPtr> in_batch;
       for (auto& r : batch) {
         auto bad = std::find_if(r->keys.begin(), r->keys.end(), [&](HostKey* hk) { return failed.count(hk) != 0; });
         if (bad != r->keys.end()) {
           errs.push_back({r, failed[*bad]});
           continue;
         }
-        if (r->kind == REQ_MATVEC) continue;
+        if (r->kind == REQ_MATVEC || r->kind == REQ_BOOTSTRAP) continue;
         Evaluator* ev = f->evs[r->owner].get();
         try {
           if (r->kind == REQ_MUL)
@@ -476,30 +579,53 @@ void Server::worker() {
           else
             r->out = f->batch->mul_plain_rescale(r->a, r->p, ev);
           owners_in_batch.insert(r->owner);
+          in_batch.push_back(r);
         } catch (const Error& e) {
           errs.push_back({r, {e.code, e.what()}});
         }
       }
       if (f->batch->size()) f->batch->run();
+      if (!in_batch.empty()) {
+        for (auto& r : in_batch) placed.insert(r.get());
+        f->close_segment(ctx_->stream, in_batch);
+      }
       for (auto& r : batch) {
-        if (r->kind != REQ_MATVEC || std::any_of(errs.begin(), errs.end(), [&](auto& x) { return x.first == r; }))
-          continue;
+        if (r->kind != REQ_MATVEC || failed_req(r)) continue;
         try {
           r->out = f->evs[r->owner]->matvec_plain(r->d, r->stride, r->diag, r->a);
           owners_in_batch.insert(r->owner);
+          placed.insert(r.get());
+          f->close_segment(ctx_->stream, {r});
         } catch (const Error& e) {
           errs.push_back({r, {e.code, e.what()}});
         }
       }
-      CKG_CUDA(cudaEventCreateWithFlags(&f->done, cudaEventDisableTiming));
-      CKG_CUDA(cudaEventRecord(f->done, ctx_->stream));
+      for (auto& r : batch) {
+        if (r->kind != REQ_BOOTSTRAP || failed_req(r)) continue;
+        try {
+          std::vector<KeyPtr> gk;
+          KeyPtr ts, td;
+          for (HostKey* hk : r->keys) {
+            if (!hk->dev) continue;
+            if (hk->role == 1) gk.push_back(hk->dev);
+            if (hk->role == 2) ts = hk->dev;
+            if (hk->role == 3) td = hk->dev;
+          }
+          auto bs = std::make_unique<Bootstrapper>(ctx_, boot_bp_, boot_ctos_, boot_stoc_, gk, ts, td, boot_coeffs_,
+                                                   boot_em_, boot_si_, boot_delta_);
+          r->out = bs->bootstrap(*f->evs[r->owner], r->a);
+          f->boots.push_back(std::move(bs));
+          owners_in_batch.insert(r->owner);
+          placed.insert(r.get());
+          f->close_segment(ctx_->stream, {r});
+        } catch (const Error& e) {
+          errs.push_back({r, {e.code, e.what()}});
+        }
+      }
     } catch (const std::exception& e) {
       const int code = dynamic_cast<const Error*>(&e) ? dynamic_cast<const Error*>(&e)->code : ST_DEVICE;
       for (auto& r : batch)
-        if (!std::any_of(errs.begin(), errs.end(), [&](auto& x) { return x.first == r; }))
-          errs.push_back({r, {code, e.what()}});
-      if (!f->done && cudaEventCreateWithFlags(&f->done, cudaEventDisableTiming) != cudaSuccess) f->done = nullptr;
-      if (f->done) cudaEventRecord(f->done, ctx_->stream);
+        if (!placed.count(r.get()) && !failed_req(r)) errs.push_back({r, {code, e.what()}});
     }
 
     lk.lock();
@@ -527,23 +653,30 @@ void Server::completer() {
       if (flights_.empty()) break;
       f = flights_.front();
     }
-    cudaError_t e = cudaSuccess;
-    if (f->done)
-      while ((e = cudaEventQuery(f->done)) == cudaErrorNotReady) std::this_thread::sleep_for(std::chrono::microseconds(20));
-    else
-      e = cudaErrorUnknown;
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      const auto t = Clock::now();
-      for (auto& r : f->reqs) {
-        if (r->status != -1) continue;
-        if (e == cudaSuccess) {
-          finish(*r, ST_OK, "");
-          r->t_done = t;
-        } else {
-          finish(*r, ST_DEVICE, std::string("device error in a served batch: ") + cudaGetErrorString(e));
+    for (auto& seg : f->segs) {  // each segment completes its own requests
+      cudaError_t e = cudaSuccess;
+      if (seg.done)
+        while ((e = cudaEventQuery(seg.done)) == cudaErrorNotReady)
+          std::this_thread::sleep_for(std::chrono::microseconds(20));
+      else
+        e = cudaErrorUnknown;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        const auto t = Clock::now();
+        for (auto& r : seg.reqs) {
+          if (r->status != -1) continue;
+          if (e == cudaSuccess) {
+            finish(*r, ST_OK, "");
+            r->t_done = t;
+          } else {
+            finish(*r, ST_DEVICE, std::string("device error in a served batch: ") + cudaGetErrorString(e));
+          }
         }
       }
+      cv_done_.notify_all();
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
       for (auto& kv : f->evs) {
         OpCounter c = kv.second->counter();
         OpCounter& o = owners_[kv.first]->counter;

@@ -28,10 +28,11 @@
 #include <unordered_map>
 
 #include "batch.hpp"
+#include "boot.hpp"
 
 namespace ckg {
 
-enum ReqKind : uint32_t { REQ_MUL = 0, REQ_ROTATE = 1, REQ_MUL_PLAIN = 2, REQ_MATVEC = 3 };
+enum ReqKind : uint32_t { REQ_MUL = 0, REQ_ROTATE = 1, REQ_MUL_PLAIN = 2, REQ_MATVEC = 3, REQ_BOOTSTRAP = 4 };
 constexpr int ST_CANCELLED = 9;  // request cancelled before it was admitted
 
 struct ServerConfig {
@@ -56,11 +57,19 @@ class Server {
   // Registers a key of `owner` (Galois element `elt`, 0 for the relinearization key) by
   // copying it into pinned host memory; the layout is the one ckg_key_upload takes.
   void add_key(uint32_t owner, const uint64_t* src, bool device_src, uint32_t parts, uint32_t q_limbs, uint64_t elt);
+  // The owner's sparse-secret-encapsulation keys (to_sparse: 1 part at level 0; to_dense:
+  // dnum parts at the top level), needed by its bootstrap requests.
+  void add_sse_keys(uint32_t owner, const uint64_t* to_sparse, const uint64_t* to_dense, bool device_src);
+  // Encodes the bootstrap stages and EvalMod series once (shared by every owner: they do not
+  // depend on keys) so that bootstrap requests can be served; inputs must be at level 0 and
+  // scale `delta`. Each bootstrap runs in its own completion segment.
+  void enable_bootstrap(const BootParams& bp, double delta);
 
   uint64_t submit_mul(uint32_t owner, const Ct& a, const Ct& b);
   uint64_t submit_rotate(uint32_t owner, const Ct& a, int32_t steps);
   uint64_t submit_mul_plain(uint32_t owner, const Ct& a, const Pt& p);
   uint64_t submit_matvec(uint32_t owner, uint32_t d, uint32_t stride, const std::vector<Pt>& diag, const Ct& x);
+  uint64_t submit_bootstrap(uint32_t owner, const Ct& a);
 
   // Waits up to timeout_ms (negative: no limit) for request `id`. On completion returns its
   // status (ST_OK with *out set, or the op's error with *err), fills times (microseconds
@@ -80,12 +89,13 @@ class Server {
     size_t words = 0;
     uint32_t parts = 0, q_limbs = 0;
     uint64_t elt = 0;
+    int role = 0;  // 0 relinearization, 1 Galois, 2 SSE to_sparse, 3 SSE to_dense
     KeyPtr dev;  // the cache's reference to the device copy
     std::list<HostKey*>::iterator lru;
     ~HostKey();
   };
   struct Owner {
-    std::unique_ptr<HostKey> relin;
+    std::unique_ptr<HostKey> relin, to_sparse, to_dense;
     std::map<uint64_t, std::unique_ptr<HostKey>> galois;
     OpCounter counter;
   };
@@ -113,6 +123,8 @@ class Server {
   void worker();
   void completer();
   KeyPtr upload(HostKey* hk);
+  std::unique_ptr<HostKey> host_key(const uint64_t* src, bool device_src, uint32_t parts, uint32_t q_limbs,
+                                    uint64_t elt);
   void finish(Req& r, int status, const std::string& err);
 
   Context* ctx_;
@@ -134,6 +146,12 @@ class Server {
   bool building_ = false;     // the worker holds admitted requests outside the lock
   bool stop_ = false, worker_exited_ = false;
   ServerStats st_;
+  bool boot_ = false;  // bootstrap template (enable_bootstrap)
+  BootParams boot_bp_;
+  double boot_delta_ = 0, boot_em_ = 0, boot_si_ = 0;
+  std::vector<LtPtr> boot_ctos_, boot_stoc_;
+  std::vector<double> boot_coeffs_;
+  std::vector<uint64_t> boot_elts_;
   std::thread worker_, completer_;
 };
 

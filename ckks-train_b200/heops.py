@@ -197,6 +197,9 @@ def _declare(L):
     L.ckg_server_destroy.argtypes = [VP]
     L.ckg_server_add_owner.argtypes = [VP, U32P]
     L.ckg_server_add_key.argtypes = [VP, C.c_uint32, VP, C.c_int, C.c_uint32, C.c_uint32, C.c_uint64]
+    L.ckg_server_add_sse_keys.argtypes = [VP, C.c_uint32, VP, VP, C.c_int]
+    L.ckg_server_enable_bootstrap.argtypes = [VP, U32P, C.c_double]
+    L.ckg_server_submit_bootstrap.argtypes = [VP, C.c_uint32, VP, U64P]
     L.ckg_server_submit_mul.argtypes = [VP, C.c_uint32, VP, VP, U64P]
     L.ckg_server_submit_rotate.argtypes = [VP, C.c_uint32, VP, C.c_int32, U64P]
     L.ckg_server_submit_mul_plain.argtypes = [VP, C.c_uint32, VP, VP, U64P]
@@ -790,6 +793,21 @@ class Server:
         parts, two, limbs, n = shape
         assert two == 2 and n == self.ctx.n
         _check(lib().ckg_server_add_key(self.h, owner, VP(ptr), 1, parts, limbs - self.ctx.k, galois_elt))
+
+    def add_sse_keys(self, owner, to_sparse, to_dense):
+        """The owner's SSE keys (to_sparse (1, 2, 1 + k, N), to_dense (dnum, 2, L + 1 + k, N))."""
+        a = np.ascontiguousarray(to_sparse, np.uint64)
+        b = np.ascontiguousarray(to_dense, np.uint64)
+        _check(lib().ckg_server_add_sse_keys(self.h, owner, a.ctypes.data_as(VP), b.ctypes.data_as(VP), 0))
+
+    def add_sse_keys_device(self, owner, ptr_sparse, ptr_dense):
+        _check(lib().ckg_server_add_sse_keys(self.h, owner, VP(ptr_sparse), VP(ptr_dense), 1))
+
+    def enable_bootstrap(self, bp, delta):
+        _check(lib().ckg_server_enable_bootstrap(self.h, _bp(bp), delta))
+
+    def submit_bootstrap(self, owner, a):
+        return self._submit(lib().ckg_server_submit_bootstrap, owner, a.h, keep=(a,))
 
     def _submit(self, fn, owner, *args, keep=()):
         i = C.c_uint64()

@@ -316,7 +316,9 @@ CKG_API int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double del
  *   mul        Evaluator::mul then ::rescale (evaluator.rs:463-510), relinearization key;
  *   rotate     Evaluator::rotate (evaluator.rs:534-540), the step's Galois key;
  *   mul_plain  Evaluator::mul_plain then ::rescale (evaluator.rs:262-271, 498-510);
- *   matvec     matvec_plain with hoisted BSGS (linalg.rs:608-622), the step keys.
+ *   matvec     matvec_plain with hoisted BSGS (linalg.rs:608-622), the step keys;
+ *   bootstrap  Bootstrapper::bootstrap (bootstrapper.rs:385-473), one per flight, in its own
+ *              completion segment.
  * Each result is bit-identical to the op run on its own. ckg_server_result waits for one
  * request (timeout_ms < 0: no limit; CKG_TIMEOUT leaves it pending), returns its status
  * (the op's error text via ckg_last_error), its output and times_us = {submitted, admitted,
@@ -328,7 +330,7 @@ CKG_API int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double del
  * key_evictions, key_upload_bytes, key_bytes, peak_key_bytes, peak_device_bytes,
  * budget_waits, pending, hbm_budget. */
 typedef struct ckg_server ckg_server;
-enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVEC = 3 };
+enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVEC = 3, CKG_REQ_BOOTSTRAP = 4 };
 CKG_API int ckg_server_create(ckg_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t max_batch_ks, uint32_t max_inflight,
                               uint32_t flags, ckg_server** out);
 CKG_API void ckg_server_destroy(ckg_server* s);
@@ -336,6 +338,15 @@ CKG_API int ckg_server_add_owner(ckg_server* s, uint32_t* owner);
 /* key: the layout of ckg_key_upload; galois_elt 0 registers the relinearization key. */
 CKG_API int ckg_server_add_key(ckg_server* s, uint32_t owner, const uint64_t* key, int device_src, uint32_t parts,
                                uint32_t q_limbs, uint64_t galois_elt);
+/* The owner's SSE keys for its bootstrap requests (to_sparse: 1 part, 1 data limb; to_dense:
+ * dnum parts, L+1 data limbs; the layout of ckg_key_upload). */
+CKG_API int ckg_server_add_sse_keys(ckg_server* s, uint32_t owner, const uint64_t* to_sparse, const uint64_t* to_dense,
+                                    int device_src);
+/* Encodes the bootstrap stages and EvalMod series once (bp: 7 words, as ckg_boot_create) so
+ * bootstrap requests (bootstrapper.rs:385-473, the owner's relinearization, rotation,
+ * conjugation and SSE keys) can be served; inputs at level 0 and scale delta. */
+CKG_API int ckg_server_enable_bootstrap(ckg_server* s, const uint32_t* bp, double delta);
+CKG_API int ckg_server_submit_bootstrap(ckg_server* s, uint32_t owner, const ckg_ct* a, uint64_t* id);
 CKG_API int ckg_server_submit_mul(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_ct* b, uint64_t* id);
 CKG_API int ckg_server_submit_rotate(ckg_server* s, uint32_t owner, const ckg_ct* a, int32_t steps, uint64_t* id);
 CKG_API int ckg_server_submit_mul_plain(ckg_server* s, uint32_t owner, const ckg_ct* a, const ckg_pt* p, uint64_t* id);

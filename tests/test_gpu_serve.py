@@ -252,3 +252,57 @@ def test_serve_cancel_and_drain(owners, ckg):
     assert st["completed"] + st["cancelled"] == 12 and st["pending"] == 0
     assert srv.cancel(ids[0]) is False
     srv.close()
+
+
+def test_serve_bootstrap_requests(ckg, oracle):
+    """Bootstrap requests from two owners (each with its own relinearization, rotation,
+    conjugation and SSE keys) served beside rotations and HMults, on the reference's N = 2^10
+    bootstrap chain: every output equals the oracle's and each owner's OpCounter equals the
+    CPU's."""
+    O = oracle
+    q_bits = [54, 42, 42] + [34] * 4 + [58] * 7 + [56] * 4
+    delta = 2.0 ** 42
+    P = O.Params.from_bits(10, q_bits, [60, 60], 42, 9)
+    enc = O.Encoder(P)
+    ctx = ckg.Context(10, P.q, P.p, 9, scale=delta)
+    io = ckg.CudaEvaluator(ctx, None, [])
+    srv = ckg.Server(ctx, 2 << 30, max_batch_ks=32, max_inflight=2, ev=io)
+    srv.enable_bootstrap(ckg.BootParams(log_slots=9), delta)
+    owners = []
+    for o in range(2):
+        kg = O.KeyGenerator(P, 60 + o)
+        rk = kg.relin_key()
+        bs = O.Bootstrapper(P, kg, enc, 9)
+        oid = srv.add_owner()
+        srv.add_key(oid, rk.export())
+        for e, k in bs.galois_keys().items():
+            srv.add_key(oid, k.export(), e)
+        ts, td = bs.sse_keys()
+        srv.add_sse_keys(oid, ts.export(), td.export())
+        owners.append((kg, rk, bs, O.Evaluator(P, rk, bs.galois_keys())))
+    rng = np.random.default_rng(3)
+    reqs = []
+    for i in range(6):
+        o = i % 2
+        kg, rk, bs, ev = owners[o]
+        m = rng.uniform(-1, 1, P.n // 2)
+        ct0 = ev.mod_switch_to_level(O.encrypt_sk(ev, kg, 20 + i, enc.encode(m, delta, P.max_level), delta), 0)
+        g0 = io.upload_ct(ct0.data(), delta)
+        reqs.append(("boot", o, ct0, srv.submit_bootstrap(o, g0)))
+        x = random_ct(P, 200 + i, P.max_level - 2)
+        reqs.append(("rot", o, x, srv.submit_rotate(o, io.upload_ct(x, delta), 1)))
+    for kind, o, x, rid in reqs:
+        ct, _ = srv.result(rid, 300000)
+        kg, rk, bs, ev = owners[o]
+        if kind == "boot":
+            want = bs.bootstrap(ev, x)
+        else:
+            want = ev.rotate(ev.ct(x, delta), 1)
+        got, scale = io.download_ct(ct)
+        assert scale == want.scale and ct.level() == want.level
+        assert_same(got, want.data(), f"served {kind} owner {o}")
+    for o, (kg, rk, bs, ev) in enumerate(owners):
+        assert srv.owner_counter(o) == ev.counter(), f"owner {o} counter"
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    srv.close()
