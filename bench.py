@@ -59,6 +59,8 @@ SERVE_D = 64                 # BSGS mat-vec diagonals: baby 8, giant 8
 SERVE_BUDGET = 24 << 30      # HBM bytes for cached keys + queued work: about half the owners
 SERVE_REQUESTS = 1000
 SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
+SERVE_BOOT_OWNERS = 8        # n16_boot serving with bootstrap requests
+SERVE_BOOT_BUDGET = 96 << 30
 
 
 def load_package():
@@ -304,6 +306,9 @@ class Serving:
     (24, 18, 12 and 6 limbs; mat-vecs at 24 or 12 limbs against one shared 64-diagonal
     matrix per level)."""
 
+    params_text = "N=2^16, 24x50-bit q + 8x60-bit p, dnum 3"
+    mix_text = "5/8 single ops (HMult+relin+rescale | rotation), 3/8 64x64 BSGS plaintext mat-vec"
+
     def __init__(self, S, owners=SERVE_OWNERS, budget=SERVE_BUDGET, seed=7):
         ckg, torch = S.ckg, S.torch
         self.S, self.owners = S, owners
@@ -388,9 +393,7 @@ class Serving:
         span = (t[:, 1].max() - t[:, 0].min()) * 1e-6
         d = {k: st[k] - st0[k] for k in ("batches", "multi_owner_batches", "key_hits", "key_misses",
                                           "key_evictions", "key_upload_bytes", "budget_waits")}
-        return {"requests": requests, "owners": self.owners,
-                "mix": "5/8 single ops (HMult+relin+rescale | rotation), 3/8 64x64 BSGS plaintext mat-vec; "
-                       "bootstrap requests not served yet",
+        return {"requests": requests, "owners": self.owners, "params": self.params_text, "mix": self.mix_text,
                 "capacity_req_s": round(capacity, 2), "offered_req_s": round(rate, 2),
                 "throughput_req_s": round(requests / span, 2),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
@@ -406,6 +409,94 @@ class Serving:
 
     def close(self):
         self.srv.close()
+
+
+class BootServing(Serving):
+    """The serving loop on the n16_boot chain with bootstrap requests in the mix:
+    SERVE_BOOT_OWNERS owners, each with its own relinearization key, the 33 Galois keys of the
+    bootstrap (32 rotations + conjugation), the 3 more a 64x64 BSGS mat-vec needs and the two
+    SSE keys -- 38 keys of 288 MiB (about 11 GiB per owner, synthetic uniform key material) in
+    pinned host memory, all resident once warm within SERVE_BOOT_BUDGET. Requests: 1/4 HMult
+    +relin+rescale and 1/4 rotations at level 16 (the post-bootstrap level), 3/10 64x64 plaintext
+    mat-vecs at level 16, 1/5 full bootstraps of a level-0 input; Poisson arrivals."""
+
+    params_text = "n16_boot: N=2^16, 32 q primes + 4x60-bit p, dnum 8, BootParams::default_n16"
+    mix_text = "1/4 HMult+relin+rescale, 1/4 rotation, 3/10 64x64 BSGS plaintext mat-vec, 1/5 full SSE bootstrap"
+
+    def __init__(self, ckg, torch, device, owners=SERVE_BOOT_OWNERS, budget=SERVE_BOOT_BUDGET, seed=9):
+        self.owners = owners
+        self.rng = np.random.default_rng(seed)
+        q, p = ckg.primes_for_bits(16, BOOT_Q_BITS, BOOT_P_BITS)
+        self.ctx = ctx = ckg.Context(16, q, p, BOOT_DNUM, device=device)
+        n, k, L = 1 << 16, len(p), len(q) - 1
+        gen = torch.Generator(device=f"cuda:{device}")
+        gen.manual_seed(777 + device)
+        qall = torch.tensor(q + p, dtype=torch.int64, device=f"cuda:{device}")
+
+        def uniform(shape, qcol):
+            t = torch.randint(0, 1 << 62, shape, generator=gen, device=qall.device, dtype=torch.int64) % qcol
+            torch.cuda.synchronize()
+            return t
+
+        def key_tensor(parts, qlimbs):
+            shape = (parts, 2, qlimbs + k, n)
+            return uniform(shape, torch.cat([qall[:qlimbs], qall[len(q):]]).view(1, 1, -1, 1)), shape
+
+        self.ev = ckg.CudaEvaluator(ctx, None, [])
+        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=self.ev)
+        bp = ckg.BootParams()
+        self.srv.enable_bootstrap(bp, BOOT_DELTA)
+        boot_steps = ckg.boot_rotation_steps(bp)
+        self.steps = list(range(1, 8)) + [8 * j for j in range(1, 8)]
+        elts = sorted({galois_elt(n, st) for st in boot_steps + self.steps} | {2 * n - 1})
+        t0 = time.time()
+        nkeys = 0
+        for _ in range(owners):
+            o = self.srv.add_owner()
+            for e in [0] + elts:
+                t, shape = key_tensor(BOOT_DNUM, L + 1)
+                self.srv.add_key_device(o, t.data_ptr(), shape, e)
+                del t
+                nkeys += 1
+            ts, _ = key_tensor(1, 1)
+            td, _ = key_tensor(BOOT_DNUM, L + 1)
+            self.srv.add_sse_keys_device(o, ts.data_ptr(), td.data_ptr())
+            del ts, td
+            nkeys += 1
+        self.register_s = time.time() - t0
+        self.key_bytes = nkeys * BOOT_DNUM * 2 * (L + 1 + k) * n * 8 + owners * 2 * (1 + k) * n * 8
+
+        def ct(level):
+            t = uniform((2, level + 1, n), qall[: level + 1].view(1, -1, 1))
+            c = self.ev.upload_ct_device(t.data_ptr(), 2, level, BOOT_DELTA)
+            ctx.sync()
+            return c
+
+        self.level0 = [ct(0) for _ in range(owners)]
+        self.inputs = [[ct(16) for _ in range(2)] for _ in range(owners)]
+        diag = []
+        for _ in range(SERVE_D):
+            t = uniform((17, n), qall[:17].view(-1, 1))
+            diag.append(self.ev.upload_pt_device(t.data_ptr(), 16, BOOT_DELTA))
+            ctx.sync()
+        self.diag = diag
+
+    def request(self):
+        o = int(self.rng.integers(self.owners))
+        r = self.rng.random()
+        a = self.inputs[o][int(self.rng.integers(2))]
+        if r < 0.25:
+            return lambda: self.srv.submit_mul(o, a, a)
+        if r < 0.5:
+            st = self.steps[int(self.rng.integers(len(self.steps)))]
+            return lambda: self.srv.submit_rotate(o, a, st)
+        if r < 0.8:
+            return lambda: self.srv.submit_matvec(o, SERVE_D, 1, self.diag, a)
+        return lambda: self.srv.submit_bootstrap(o, self.level0[o])
+
+    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD):
+        out = super().measure(requests, load)
+        return out
 
 
 class BootBench:
@@ -449,10 +540,11 @@ class BootBench:
             self.to_dense.nbytes
         self.ev = ckg.CudaEvaluator(ctx, relin, [])
         t0 = time.time()
+        l0 = ckg.launch_count()
         self.bs = ckg.Bootstrapper.encoded(self.ev, bp, BOOT_DELTA, self.galois, self.to_sparse, self.to_dense)
         ctx.sync()
         self.setup_s = time.time() - t0
-        self.setup_launches = ckg.launch_count()
+        self.setup_launches = ckg.launch_count() - l0
         t = uniform((2, 1, n), qall[:1].view(1, 1, 1))
         self.ct = self.ev.upload_ct_device(t.data_ptr(), 2, 0, BOOT_DELTA)
         ctx.sync()
@@ -688,11 +780,15 @@ def main():
         return
     S = Setup(ckg, torch, local)
     if args.serve_only:
-        sv = Serving(S, owners=args.serve_owners)
+        sv = BootServing(ckg, torch, local)
         out = sv.measure(args.serve_requests)
         sv.close()
+        del sv
+        sv = Serving(S, owners=args.serve_owners)
+        out2 = sv.measure(args.serve_requests)
+        sv.close()
         if rank == 0:
-            print(json.dumps({"serving": out}))
+            print(json.dumps({"serving": out, "serving_spill": out2}))
         return
     if args.profile == "plain":
         P = Plain(S)
@@ -738,11 +834,15 @@ def main():
     if not args.no_boot:
         mix.batch = None
         boot = BootBench(ckg, torch, local).measure()
-    serving = None
+    serving = serving_spill = None
     if not args.no_serve:
         mix.batch = None
-        sv = Serving(S, owners=args.serve_owners)
+        sv = BootServing(ckg, torch, local)
         serving = sv.measure(args.serve_requests)
+        sv.close()
+        del sv
+        sv = Serving(S, owners=args.serve_owners)
+        serving_spill = sv.measure(args.serve_requests)
         sv.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -756,7 +856,8 @@ def main():
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
                 "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
-                "bootstrap": boot, "serving": serving, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "bootstrap": boot, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
+                "clocks": clk.summary()}
         print(json.dumps(line))
     mix.batch = None
     S.ctx.sync()
