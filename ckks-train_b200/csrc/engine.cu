@@ -162,6 +162,15 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
     c.r64 = (uint64_t)(((u128)1 << 64) % m.q);
     c.r64_s = m.shoup(c.r64);
     c.one_s = m.shoup(1);
+    c.qd = (double)m.q;
+    c.qinv = 1.0 / c.qd;
+    c.ninvd = (double)c.ninv;
+    c.wninvd = (double)c.wninv;
+  }
+  std::vector<double> twdf(np * n), twdi(np * n);
+  for (size_t i = 0; i < np * n; ++i) {
+    twdf[i] = (double)twf[i].x;  // exact below 2^53; used only for primes below 2^50
+    twdi[i] = (double)twi[i].x;
   }
   CKG_CUDA(cudaMalloc(&d_prime, np * sizeof(PrimeConst)));
   CKG_CUDA(cudaMalloc(&d_tw_fwd, np * n * sizeof(ulonglong2)));
@@ -169,7 +178,11 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
   CKG_CUDA(cudaMemcpy(d_prime, pc.data(), np * sizeof(PrimeConst), cudaMemcpyHostToDevice));
   CKG_CUDA(cudaMemcpy(d_tw_fwd, twf.data(), np * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
   CKG_CUDA(cudaMemcpy(d_tw_inv, twi.data(), np * n * sizeof(ulonglong2), cudaMemcpyHostToDevice));
-  dt = DevTables{d_prime, d_tw_fwd, d_tw_inv, (int)log_n};
+  CKG_CUDA(cudaMalloc(&d_twd_fwd, np * n * sizeof(double)));
+  CKG_CUDA(cudaMalloc(&d_twd_inv, np * n * sizeof(double)));
+  CKG_CUDA(cudaMemcpy(d_twd_fwd, twdf.data(), np * n * sizeof(double), cudaMemcpyHostToDevice));
+  CKG_CUDA(cudaMemcpy(d_twd_inv, twdi.data(), np * n * sizeof(double), cudaMemcpyHostToDevice));
+  dt = DevTables{d_prime, d_tw_fwd, d_tw_inv, d_twd_fwd, d_twd_inv, (int)log_n};
 
   // conversion tables
   std::vector<uint64_t> conv;
@@ -228,6 +241,8 @@ Context::~Context() {
   cudaFree(d_prime);
   cudaFree(d_tw_fwd);
   cudaFree(d_tw_inv);
+  cudaFree(d_twd_fwd);
+  cudaFree(d_twd_inv);
   cudaFree(d_conv);
 }
 

@@ -96,6 +96,8 @@ struct Context {
   PrimeConst* d_prime = nullptr;
   ulonglong2* d_tw_fwd = nullptr;
   ulonglong2* d_tw_inv = nullptr;
+  double* d_twd_fwd = nullptr;
+  double* d_twd_inv = nullptr;
   uint64_t* d_conv = nullptr;  // all conversion tables
   uint64_t* d_consts = nullptr;  // finish constants (Shoup pairs)
   std::vector<size_t> modup_off;    // [l * dnum + j] word offset into d_conv

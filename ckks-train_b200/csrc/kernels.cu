@@ -2,9 +2,10 @@
 // conversion (ModUp / ModDown / rescale), the key-switch inner product, the ModDown and
 // rescale finish, element-wise ops and the NTT-form automorphism.
 //
-// All arithmetic is 64-bit integer on the IMAD pipe; the only floating-point step is the
-// overflow estimate of exact base conversion, done with __dmul_rn / __dadd_rn so that no
-// multiply-add is contracted (crates/ckks-train-core/src/baseconv.rs:198-206).
+// Arithmetic is 64-bit integer on the IMAD pipe, except the NTT butterflies of primes below
+// 2^50, which run exactly on the FP64 pipe (see kF64Bound), and the overflow estimate of
+// exact base conversion, done with __dmul_rn / __dadd_rn so that no multiply-add is
+// contracted (crates/ckks-train-core/src/baseconv.rs:198-206).
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -79,6 +80,54 @@ CKG_DEV ulonglong2 ldtw(const ulonglong2* t, uint32_t i) { return __ldg(t + i); 
 
 CKG_DEV int pad_idx(int k) { return k + (k >> 4); }
 
+// FP64 butterflies for primes below 2^50, on the FP64 pipe instead of IMAD. Values are
+// exact integers held in doubles, signed and lazy: every butterfly input lies in (-2q, 2q).
+// w*y mod q: hi = fl(w y) and lo = fma(w, y, -hi) hold the exact product (|w y| < 2q^2 <
+// 2^101); k = rint(hi / q), taken with the 1.5 * 2^52 rounding constant (|hi / q| < 2^51), is
+// within 1.25 of w y / q, so fma(-k, q, hi) + lo = w y - k q is an integer below 2^51 in
+// magnitude and every step is exact. Inputs and outputs of a transform are canonical u64;
+// between its two passes the limb holds the raw doubles.
+constexpr uint64_t kF64Bound = 1ULL << 50;
+constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double kTwo52 = 4503599627370496.0;
+
+CKG_DEV double f64_of(uint64_t x) {  // exact for x < 2^52
+  return __dsub_rn(__longlong_as_double((long long)(x | 0x4330000000000000ULL)), kTwo52);
+}
+CKG_DEV uint64_t u64_of(double v) {  // v an integer in [0, 2^52)
+  return (uint64_t)__double_as_longlong(__dadd_rn(v, kTwo52)) & 0xFFFFFFFFFFFFFULL;
+}
+CKG_DEV double bits_dbl(uint64_t v) { return __longlong_as_double((long long)v); }
+CKG_DEV uint64_t dbl_bits(double v) { return (uint64_t)__double_as_longlong(v); }
+CKG_DEV double rint_f64(double v) { return __dsub_rn(__dadd_rn(v, kMagic), kMagic); }  // |v| < 2^51
+
+// w y mod q in (-1.25q, 1.25q) for |y| < 2q, 0 <= w < q.
+CKG_DEV double mulmod_f64(double y, double w, double q, double qinv) {
+  const double hi = __dmul_rn(y, w);
+  const double lo = __fma_rn(y, w, -hi);
+  const double k = rint_f64(__dmul_rn(hi, qinv));
+  return __dadd_rn(__fma_rn(-k, q, hi), lo);
+}
+// x - q rint(x / q): |x| < 4q -> |result| <= q/2 + 1.
+CKG_DEV double red_f64(double x, double q, double qinv) { return __fma_rn(-rint_f64(__dmul_rn(x, qinv)), q, x); }
+CKG_DEV uint64_t canon_u64(double x, double q, double qinv) {
+  const double r = red_f64(x, q, qinv);
+  return u64_of(r < 0.0 ? __dadd_rn(r, q) : r);
+}
+// Cooley-Tukey: outputs below 1.75q + 1.
+CKG_DEV void ct_bf_f64(double& x, double& y, double w, double q, double qinv) {
+  const double t = mulmod_f64(y, w, q, qinv);
+  const double xr = red_f64(x, q, qinv);
+  x = __dadd_rn(xr, t);
+  y = __dsub_rn(xr, t);
+}
+// Gentleman-Sande: outputs below 1.25q.
+CKG_DEV void gs_bf_f64(double& x, double& y, double w, double q, double qinv) {
+  const double xr = red_f64(x, q, qinv), yr = red_f64(y, q, qinv);
+  x = __dadd_rn(xr, yr);
+  y = mulmod_f64(__dsub_rn(xr, yr), w, q, qinv);
+}
+
 // Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
 template <int LOGS, bool LAZY>
 CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roots, uint64_t* sm) {
@@ -120,14 +169,59 @@ CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roo
   }
 }
 
+// The same pass with FP64 butterflies; writes the raw doubles for the row pass.
+template <int LOGS>
+CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm) {
+  constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
+  const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
+  const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
+  const int col = blockIdx.x * kCols + c;
+  double x[1 << E1];
+#pragma unroll
+  for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(ref.src[col + (size_t)kRow * (ts + TPS * j)]);
+#pragma unroll
+  for (int r = 0; r < E1; ++r) {
+    const int half = 1 << (E1 - 1 - r);
+#pragma unroll
+    for (int j = 0; j < (1 << E1); ++j)
+      if (!(j & half)) ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << r) + (j >> (E1 - r))), q, qinv);
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << E1); ++j) sm[(ts + TPS * j) * kCols + c] = dbl_bits(x[j]);
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int t2 = ts + TPS * v;
+    double y[1 << E2];
+#pragma unroll
+    for (int j = 0; j < (1 << E2); ++j) y[j] = bits_dbl(sm[((t2 << E2) + j) * kCols + c]);
+#pragma unroll
+    for (int r = E1; r < LOGS; ++r) {
+      const int half = 1 << (LOGS - 1 - r);
+#pragma unroll
+      for (int j = 0; j < (1 << E2); ++j)
+        if (!(j & half)) {
+          const int k = (t2 << E2) + j;
+          ct_bf_f64(y[j], y[j + half], __ldg(roots + (1u << r) + (k >> (LOGS - r))), q, qinv);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << E2); ++j) ref.dst[col + (size_t)kRow * ((t2 << E2) + j)] = dbl_bits(y[j]);
+  }
+}
+
 template <int LOGS, class B>
 __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
     k_ntt_fwd_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
   extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
   LimbRef ref = b.r[blockIdx.y];
   if (in_place) ref.src = ref.dst;
   const uint64_t q = __ldg(&pc[ref.prime].q);
+  if (q < kF64Bound) {
+    fwd_cols_body_f64<LOGS>(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), sm);
+    return;
+  }
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm);
   else fwd_cols_body<LOGS, false>(ref, q, roots, sm);
@@ -184,18 +278,66 @@ CKG_DEV void fwd_rows_body(const uint64_t* base, const PrimeConst* P, const ulon
   for (int i = 0; i < kRowsPerCta; ++i) store(i, threadIdx.x, sm[i * kRowPad + pad_idx(threadIdx.x)]);
 }
 
+// The row pass with FP64 butterflies over the raw doubles of the FP64 column pass.
+template <class Store>
+CKG_DEV void fwd_rows_body_f64(const uint64_t* base, const PrimeConst* P, const double* roots, int log_n,
+                               uint64_t* sm, Store store) {
+  const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
+  const int s0 = log_n - kRowLog;
+  const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
+  const uint32_t row = blockIdx.x * kRowsPerCta + rr;
+  const uint64_t* src = base + (size_t)row * kRow;
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = bits_dbl(src[t + 16 * j]);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int half = 1 << (3 - r);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & half))
+        ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, qinv);
+  }
+  uint64_t* srow = sm + rr * kRowPad;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) srow[pad_idx(t + 16 * j)] = dbl_bits(x[j]);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = bits_dbl(srow[pad_idx(16 * t + j)]);
+#pragma unroll
+  for (int r = 4; r < 8; ++r) {
+    const int half = 1 << (7 - r);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & half)) {
+        const int k = 16 * t + j;
+        ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, qinv);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = canon_u64(x[j], q, qinv);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kRowsPerCta; ++i) store(i, threadIdx.x, sm[i * kRowPad + pad_idx(threadIdx.x)]);
+}
+
 template <class B>
 __global__ void __launch_bounds__(256, 4)
     k_ntt_fwd_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
   const LimbRef ref = b.r[blockIdx.y];
   const uint64_t* src = in_place ? ref.dst : ref.src;
   const PrimeConst* P = pc + ref.prime;
-  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   uint64_t* dst = ref.dst + (size_t)blockIdx.x * kRowsPerCta * kRow;
   auto store = [&](int i, int col, uint64_t v) { dst[i * kRow + col] = v; };
-  if (__ldg(&P->q) < kLazyBound) fwd_rows_body<true>(src, P, roots, log_n, sm, store);
+  const uint64_t q = __ldg(&P->q);
+  if (q < kF64Bound) {
+    fwd_rows_body_f64(src, P, twd + ((size_t)ref.prime << log_n), log_n, sm, store);
+    return;
+  }
+  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+  if (q < kLazyBound) fwd_rows_body<true>(src, P, roots, log_n, sm, store);
   else fwd_rows_body<false>(src, P, roots, log_n, sm, store);
 }
 
@@ -205,7 +347,7 @@ __global__ void __launch_bounds__(256, 4)
 template <class B>
 __global__ void __launch_bounds__(256, 4)
     k_ntt_fwd_rows_finish(const __grid_constant__ B fb, const PrimeConst* __restrict__ pc,
-                          const ulonglong2* __restrict__ tw, int log_n) {
+                          const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
   const FinRef& r = fb.r[blockIdx.y];
   const PrimeConst* P = pc + r.prime;
@@ -218,15 +360,58 @@ __global__ void __launch_bounds__(256, 4)
     if (r.add) o = add_mod(o, r.add[r.add_perm ? __ldg(r.add_perm + g) : g], q);
     r.out[g] = o;
   };
-  if (q < kLazyBound) fwd_rows_body<true>(r.t, P, roots, log_n, sm, store);
+  if (q < kF64Bound) fwd_rows_body_f64(r.t, P, twd + ((size_t)r.prime << log_n), log_n, sm, store);
+  else if (q < kLazyBound) fwd_rows_body<true>(r.t, P, roots, log_n, sm, store);
   else fwd_rows_body<false>(r.t, P, roots, log_n, sm, store);
+}
+
+// Inverse row pass with FP64 butterflies: canonical input, raw doubles out.
+CKG_DEV void inv_rows_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, int log_n,
+                               uint64_t* sm) {
+  const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
+  const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
+  const uint32_t row = blockIdx.x * kRowsPerCta + rr;
+  uint64_t* srow = sm + rr * kRowPad;
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = f64_of(srow[pad_idx(16 * t + j)]);
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int d = 1 << u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & d)) {
+        const uint32_t k = 16 * t + j;
+        const uint32_t h = 1u << (log_n - 1 - u);
+        gs_bf_f64(x[j], x[j + d], __ldg(roots + h + (row << (7 - u)) + (k >> (u + 1))), q, qinv);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = dbl_bits(x[j]);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 16; ++j) x[j] = bits_dbl(srow[pad_idx(t + 16 * j)]);
+#pragma unroll
+  for (int u = 4; u < 8; ++u) {
+    const int d = 1 << (u - 4);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (!(j & d)) {
+        const uint32_t k = t + 16 * j;
+        const uint32_t h = 1u << (log_n - 1 - u);
+        gs_bf_f64(x[j], x[j + d], __ldg(roots + h + (row << (7 - u)) + (k >> (u + 1))), q, qinv);
+      }
+  }
+  uint64_t* dst = ref.dst + (size_t)row * kRow;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) dst[t + 16 * j] = dbl_bits(x[j]);
 }
 
 // Inverse row pass: GS stages u = 0..7 (pair distance 2^u) within 256-point rows.
 template <class B>
 __global__ void __launch_bounds__(256, 4)
     k_ntt_inv_rows(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
   __shared__ uint64_t sm[kRowsPerCta * kRowPad];
   LimbRef ref = b.r[blockIdx.y];
   if (in_place) ref.src = ref.dst;
@@ -236,6 +421,10 @@ __global__ void __launch_bounds__(256, 4)
 #pragma unroll
   for (int i = 0; i < kRowsPerCta; ++i) sm[i * kRowPad + pad_idx(threadIdx.x)] = src[i * kRow + threadIdx.x];
   __syncthreads();
+  if (q < kF64Bound) {
+    inv_rows_body_f64(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), log_n, sm);
+    return;
+  }
   const int t = threadIdx.x % 16, rr = threadIdx.x / 16;
   const uint32_t row = blockIdx.x * kRowsPerCta + rr;
   uint64_t* srow = sm + rr * kRowPad;
@@ -276,15 +465,76 @@ __global__ void __launch_bounds__(256, 4)
 
 // Inverse column pass: GS stages u = 8..logN-1 on 2^LOGS-point columns, N^-1 fused into
 // the last stage, output in [0, q).
+// Inverse column pass with FP64 butterflies over the raw doubles of the row pass; N^-1 in
+// the last stage, canonical output.
+template <int LOGS>
+CKG_DEV void inv_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm) {
+  constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
+  const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
+  const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
+  const int col = blockIdx.x * kCols + c;
+  double x[1 << F1];
+#pragma unroll
+  for (int j = 0; j < (1 << F1); ++j) x[j] = bits_dbl(ref.src[col + (size_t)kRow * ((ts << F1) + j)]);
+#pragma unroll
+  for (int v = 0; v < F1; ++v) {
+    const int d = 1 << v;
+#pragma unroll
+    for (int j = 0; j < (1 << F1); ++j)
+      if (!(j & d)) {
+        const uint32_t k = (ts << F1) + j;
+        gs_bf_f64(x[j], x[j + d], __ldg(roots + (1u << (LOGS - 1 - v)) + (k >> (v + 1))), q, qinv);
+      }
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << F1); ++j) sm[((ts << F1) + j) * kCols + c] = dbl_bits(x[j]);
+  __syncthreads();
+  const double ninv = __ldg(&P->ninvd), wninv = __ldg(&P->wninvd);
+#pragma unroll
+  for (int vv = 0; vv < V; ++vv) {
+    const int t2 = ts + TPS * vv;
+    double y[1 << F2];
+#pragma unroll
+    for (int j = 0; j < (1 << F2); ++j) y[j] = bits_dbl(sm[(t2 + (j << F1)) * kCols + c]);
+#pragma unroll
+    for (int v = F1; v < LOGS - 1; ++v) {
+      const int d = 1 << (v - F1);
+#pragma unroll
+      for (int j = 0; j < (1 << F2); ++j)
+        if (!(j & d)) {
+          const uint32_t k = t2 + (j << F1);
+          gs_bf_f64(y[j], y[j + d], __ldg(roots + (1u << (LOGS - 1 - v)) + (k >> (v + 1))), q, qinv);
+        }
+    }
+    uint64_t out[1 << F2];
+    {  // last stage: pairs (k, k + 2^(LOGS-1)), times N^-1
+      const int d = 1 << (F2 - 1);
+#pragma unroll
+      for (int j = 0; j < (1 << F2); ++j)
+        if (!(j & d)) {
+          const double xr = red_f64(y[j], q, qinv), yr = red_f64(y[j + d], q, qinv);
+          out[j] = canon_u64(mulmod_f64(__dadd_rn(xr, yr), ninv, q, qinv), q, qinv);
+          out[j + d] = canon_u64(mulmod_f64(__dsub_rn(xr, yr), wninv, q, qinv), q, qinv);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < (1 << F2); ++j) ref.dst[col + (size_t)kRow * (t2 + (j << F1))] = out[j];
+  }
+}
+
 template <int LOGS, class B>
 __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
     k_ntt_inv_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, int log_n, int in_place) {
+                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
   constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
   extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
   LimbRef ref = b.r[blockIdx.y];
   if (in_place) ref.src = ref.dst;
   const PrimeConst* P = pc + ref.prime;
+  if (__ldg(&P->q) < kF64Bound) {
+    inv_cols_body_f64<LOGS>(ref, P, twd + ((size_t)ref.prime << log_n), sm);
+    return;
+  }
   const uint64_t q = __ldg(&P->q), two_q = 2 * q;
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
@@ -685,10 +935,10 @@ void launch_cols(bool inverse, const B& b, int count, const DevTables& d, int in
   dim3 grid(kRow / kCols, count);
   if (!inverse) {
     if (smem > 48 * 1024) set_smem(k_ntt_fwd_cols<LOGS, B>, smem);
-    k_ntt_fwd_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_fwd, d.log_n, in_place);
+    k_ntt_fwd_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_fwd, d.twd_fwd, d.log_n, in_place);
   } else {
     if (smem > 48 * 1024) set_smem(k_ntt_inv_cols<LOGS, B>, smem);
-    k_ntt_inv_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_inv, d.log_n, in_place);
+    k_ntt_inv_cols<LOGS, B><<<grid, threads, smem, st>>>(b, d.prime, d.tw_inv, d.twd_inv, d.log_n, in_place);
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
@@ -720,9 +970,9 @@ void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStr
   const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), count);
   if (!inverse) {
     launch_cols_any(false, b, count, d, 0, st);
-    k_ntt_fwd_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.log_n, 1);
+    k_ntt_fwd_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.twd_fwd, d.log_n, 1);
   } else {
-    k_ntt_inv_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.log_n, 0);
+    k_ntt_inv_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.twd_inv, d.log_n, 0);
     launch_cols_any(true, b, count, d, 1, st);
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -830,7 +1080,7 @@ void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaSt
       b.r[i] = LimbRef{refs[off + i].t, const_cast<uint64_t*>(refs[off + i].t), refs[off + i].prime, 0};
     }
     launch_cols_any(false, b, cnt, d, 1, st);
-    k_ntt_fwd_rows_finish<FinBatch><<<dim3(rgrid.x, cnt), 256, 0, st>>>(fb, d.prime, d.tw_fwd, d.log_n);
+    k_ntt_fwd_rows_finish<FinBatch><<<dim3(rgrid.x, cnt), 256, 0, st>>>(fb, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
 }
@@ -845,7 +1095,7 @@ void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const Fi
   }
   launch_cols_any(false, LimbPtrs{count, 0, dev_cols}, count, d, 1, st);
   k_ntt_fwd_rows_finish<FinPtrs><<<dim3((1 << d.log_n) / (kRow * kRowsPerCta), count), 256, 0, st>>>(
-      FinPtrs{count, 0, dev_fin}, d.prime, d.tw_fwd, d.log_n);
+      FinPtrs{count, 0, dev_fin}, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -16,6 +16,8 @@ struct DevTables {
   const PrimeConst* prime;   // [n_primes]
   const ulonglong2* tw_fwd;  // [n_primes][N] (w, w') with roots[bitrev(i)] = psi^i
   const ulonglong2* tw_inv;  // [n_primes][N] inverse roots
+  const double* twd_fwd;     // [n_primes][N] the same roots as doubles (FP64 butterflies)
+  const double* twd_inv;
   int log_n;
 };
 

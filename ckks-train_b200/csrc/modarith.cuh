@@ -24,6 +24,8 @@ struct PrimeConst {
   uint64_t one_s;    // floor(2^64 / q): Shoup companion of 1 (reduces any u64 to [0, 2q))
   uint32_t b;        // bit length of q
   uint32_t pad;
+  double qd, qinv;     // q and fl(1/q) for the FP64 butterflies of primes below 2^50
+  double ninvd, wninvd;  // ninv and wninv as doubles (exact: < q < 2^50)
 };
 
 CKG_DEV uint64_t mul_shoup_lazy(uint64_t a, uint64_t w, uint64_t ws, uint64_t q) {
