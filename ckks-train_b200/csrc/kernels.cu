@@ -83,12 +83,11 @@ CKG_DEV int pad_idx(int k) { return k + (k >> 4); }
 // FP64 butterflies for primes below 2^50, on the FP64 pipe instead of IMAD. Values are
 // exact integers held in doubles, signed and lazy: every butterfly input lies in (-2q, 2q).
 // w*y mod q: hi = fl(w y) and lo = fma(w, y, -hi) hold the exact product (|w y| < 2q^2 <
-// 2^101); k = rint(hi / q), taken with the 1.5 * 2^52 rounding constant (|hi / q| < 2^51), is
-// within 1.25 of w y / q, so fma(-k, q, hi) + lo = w y - k q is an integer below 2^51 in
-// magnitude and every step is exact. Inputs and outputs of a transform are canonical u64;
+// 2^101); k = rint(hi / q) is within 1.25 of w y / q (|hi / q| < 2q < 2^51), so fma(-k, q, hi) + lo = w y - k q is an integer below 2^51 in
+// magnitude and every step is exact. (k = rint(hi / q), taken by the native rounding
+// instruction, is within 1.25 of w y / q because |hi / q| < 2q < 2^51.) Inputs and outputs of a transform are canonical u64;
 // between its two passes the limb holds the raw doubles.
 constexpr uint64_t kF64Bound = 1ULL << 50;
-constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
 constexpr double kTwo52 = 4503599627370496.0;
 
 CKG_DEV double f64_of(uint64_t x) {  // exact for x < 2^52
@@ -99,7 +98,7 @@ CKG_DEV uint64_t u64_of(double v) {  // v an integer in [0, 2^52)
 }
 CKG_DEV double bits_dbl(uint64_t v) { return __longlong_as_double((long long)v); }
 CKG_DEV uint64_t dbl_bits(double v) { return (uint64_t)__double_as_longlong(v); }
-CKG_DEV double rint_f64(double v) { return __dsub_rn(__dadd_rn(v, kMagic), kMagic); }  // |v| < 2^51
+CKG_DEV double rint_f64(double v) { return rint(v); }  // round to nearest integer (|v| < 2^51 here)
 
 // w y mod q in (-1.25q, 1.25q) for |y| < 2q, 0 <= w < q.
 CKG_DEV double mulmod_f64(double y, double w, double q, double qinv) {
@@ -354,15 +353,43 @@ __global__ void __launch_bounds__(256, 4)
   const uint64_t q = __ldg(&P->q);
   const ulonglong2* roots = tw + ((size_t)r.prime << log_n);
   const size_t base = (size_t)blockIdx.x * kRowsPerCta * kRow;
-  auto store = [&](int i, int col, uint64_t v) {
-    const size_t g = base + i * kRow + col;
-    uint64_t o = mul_shoup(sub_mod(r.x[g], v, q), r.c, r.c_s, q);
-    if (r.add) o = add_mod(o, r.add[r.add_perm ? __ldg(r.add_perm + g) : g], q);
-    r.out[g] = o;
-  };
-  if (q < kF64Bound) fwd_rows_body_f64(r.t, P, twd + ((size_t)r.prime << log_n), log_n, sm, store);
-  else if (q < kLazyBound) fwd_rows_body<true>(r.t, P, roots, log_n, sm, store);
-  else fwd_rows_body<false>(r.t, P, roots, log_n, sm, store);
+  auto keep = [](int, int, uint64_t) {};  // the transformed rows stay in shared memory
+  if (q < kF64Bound) fwd_rows_body_f64(r.t, P, twd + ((size_t)r.prime << log_n), log_n, sm, keep);
+  else if (q < kLazyBound) fwd_rows_body<true>(r.t, P, roots, log_n, sm, keep);
+  else fwd_rows_body<false>(r.t, P, roots, log_n, sm, keep);
+  // Finish, 8 rows at a time so their loads (x, the permutation, the gathered addend) are in
+  // flight together; x, add and perm are only read here and `out` is a separate buffer.
+  const uint64_t* __restrict__ xs = r.x;
+  const uint64_t* __restrict__ adds = r.add;
+  const uint32_t* __restrict__ pm = r.add_perm;
+  uint64_t* __restrict__ outp = r.out;
+  const uint64_t c = r.c, c_s = r.c_s;
+  const int col = threadIdx.x;
+#pragma unroll
+  for (int h = 0; h < kRowsPerCta; h += 8) {
+    uint64_t xv[8], av[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) xv[i] = __ldg(xs + base + (h + i) * kRow + col);
+    if (adds) {
+      if (pm) {
+        uint32_t pv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) pv[i] = __ldg(pm + base + (h + i) * kRow + col);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) av[i] = __ldg(adds + pv[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) av[i] = __ldg(adds + base + (h + i) * kRow + col);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t v = sm[(h + i) * kRowPad + pad_idx(col)];
+      uint64_t o = mul_shoup(sub_mod(xv[i], v, q), c, c_s, q);
+      if (adds) o = add_mod(o, av[i], q);
+      outp[base + (h + i) * kRow + col] = o;
+    }
+  }
 }
 
 // Inverse row pass with FP64 butterflies: canonical input, raw doubles out.
