@@ -782,31 +782,46 @@ __global__ void __launch_bounds__(256)
   const int key_limb = is_q ? i : job.key_q + (i - l - 1);
   const size_t key_limbs = (size_t)(job.key_q + ib.k);
   const uint32_t src_c = job.perm ? __ldg(job.perm + c) : (uint32_t)c;
-  // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits)
+  // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits).
+  // By-value lists (one op's jobs) load the words of up to 4 digits before their products so
+  // the loads overlap; the batched grid, whose many resident jobs already keep loads in
+  // flight, keeps one digit per step (measured faster there).
   uint64_t Ab = 0, B1b = 0, B2b = 0, Cb = 0, Aa = 0, B1a = 0, B2a = 0, Ca = 0;
-  for (int j = 0; j < job.ndig; ++j) {
-    const int start = j * ib.alpha;
-    const int end = min(start + ib.alpha, l + 1);
-    uint64_t d;
-    if (is_q && i >= start && i < end) {
-      d = job.in[((size_t)i << log_n) + src_c];
-    } else {
-      const int t = i < start ? i : i - (end - start);
-      d = job.conv[j][((size_t)t << log_n) + src_c];
+  constexpr int kChunk = kJobFast ? 1 : 4;
+  for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
+    uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int j = j0 + u;
+      if (j < job.ndig) {
+        const int start = j * ib.alpha;
+        const int end = min(start + ib.alpha, l + 1);
+        if (is_q && i >= start && i < end) {
+          dv[u] = __ldg(job.in + ((size_t)i << log_n) + src_c);
+        } else {
+          const int t = i < start ? i : i - (end - start);
+          dv[u] = __ldg(job.conv[j] + ((size_t)t << log_n) + src_c);
+        }
+        kbv[u] = __ldcs(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c);
+        kav[u] = __ldcs(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c);
+      }
     }
-    const uint64_t kb = __ldcs(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c);
-    const uint64_t ka = __ldcs(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c);
-    const uint32_t dl = (uint32_t)(d & kMask30), dh = (uint32_t)(d >> 30);
-    const uint32_t bl = (uint32_t)(kb & kMask30), bh = (uint32_t)(kb >> 30);
-    const uint32_t al = (uint32_t)(ka & kMask30), ah = (uint32_t)(ka >> 30);
-    Ab += (uint64_t)dl * bl;
-    B1b += (uint64_t)dl * bh;
-    B2b += (uint64_t)dh * bl;
-    Cb += (uint64_t)dh * bh;
-    Aa += (uint64_t)dl * al;
-    B1a += (uint64_t)dl * ah;
-    B2a += (uint64_t)dh * al;
-    Ca += (uint64_t)dh * ah;
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      if (j0 + u >= job.ndig) break;
+      const uint64_t d = dv[u], kb = kbv[u], ka = kav[u];
+      const uint32_t dl = (uint32_t)(d & kMask30), dh = (uint32_t)(d >> 30);
+      const uint32_t bl = (uint32_t)(kb & kMask30), bh = (uint32_t)(kb >> 30);
+      const uint32_t al = (uint32_t)(ka & kMask30), ah = (uint32_t)(ka >> 30);
+      Ab += (uint64_t)dl * bl;
+      B1b += (uint64_t)dl * bh;
+      B2b += (uint64_t)dh * bl;
+      Cb += (uint64_t)dh * bh;
+      Aa += (uint64_t)dl * al;
+      B1a += (uint64_t)dl * ah;
+      B2a += (uint64_t)dh * al;
+      Ca += (uint64_t)dh * ah;
+    }
   }
   const PrimeConst& P = pc[prime];
   uint64_t lo = Ab, hi = 0;
