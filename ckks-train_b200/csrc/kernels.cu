@@ -100,31 +100,40 @@ CKG_DEV double bits_dbl(uint64_t v) { return __longlong_as_double((long long)v);
 CKG_DEV uint64_t dbl_bits(double v) { return (uint64_t)__double_as_longlong(v); }
 CKG_DEV double rint_f64(double v) { return rint(v); }  // round to nearest integer (|v| < 2^51 here)
 
-// w y mod q in (-1.25q, 1.25q) for |y| < 2q, 0 <= w < q.
+// w y mod q, signed and exact, for |y| < 8q, 0 <= w < q < 2^50: |w y / q| < 2^53 and the
+// rounded quotient is within 0.5 + 3 |y| 2^-53 of it, so the result lies in (-3.5q, 3.5q),
+// and |hi - k q| + |lo| < 2^53 keeps every step exact.
 CKG_DEV double mulmod_f64(double y, double w, double q, double qinv) {
   const double hi = __dmul_rn(y, w);
   const double lo = __fma_rn(y, w, -hi);
   const double k = rint_f64(__dmul_rn(hi, qinv));
   return __dadd_rn(__fma_rn(-k, q, hi), lo);
 }
-// x - q rint(x / q): |x| < 4q -> |result| <= q/2 + 1.
+// x - q rint(x / q): |x| < 8q -> |result| <= q/2 + 1.
 CKG_DEV double red_f64(double x, double q, double qinv) { return __fma_rn(-rint_f64(__dmul_rn(x, qinv)), q, x); }
 CKG_DEV uint64_t canon_u64(double x, double q, double qinv) {
   const double r = red_f64(x, q, qinv);
   return u64_of(r < 0.0 ? __dadd_rn(r, q) : r);
 }
-// Cooley-Tukey: outputs below 1.75q + 1.
+// Cooley-Tukey. With RED the additive input is first reduced to [-q/2, q/2]; the passes set
+// RED on every other stage. With |t| <= (0.5 + 0.375 |y|/q) q (q < 2^50), a RED stage after
+// inputs below b q gives outputs below (1 + 0.375 b) q and a plain stage after inputs below
+// a q gives (1.375 a + 0.5) q: the pair settles at a = 2.45, b = 3.87, so every value stays
+// below 3.9q, inside the 8q that mulmod_f64 and red_f64 accept.
+template <bool RED>
 CKG_DEV void ct_bf_f64(double& x, double& y, double w, double q, double qinv) {
   const double t = mulmod_f64(y, w, q, qinv);
-  const double xr = red_f64(x, q, qinv);
+  const double xr = RED ? red_f64(x, q, qinv) : x;
   x = __dadd_rn(xr, t);
   y = __dsub_rn(xr, t);
 }
-// Gentleman-Sande: outputs below 1.25q.
+// Gentleman-Sande: the sum is reduced, the difference multiplied. From inputs below c q the
+// outputs stay below q/2 + 1 and (0.5 + 0.75 c) q, which settles at c = 2: values below 2q,
+// differences below 4q.
 CKG_DEV void gs_bf_f64(double& x, double& y, double w, double q, double qinv) {
-  const double xr = red_f64(x, q, qinv), yr = red_f64(y, q, qinv);
-  x = __dadd_rn(xr, yr);
-  y = mulmod_f64(__dsub_rn(xr, yr), w, q, qinv);
+  const double s = __dadd_rn(x, y), d = __dsub_rn(x, y);
+  x = red_f64(s, q, qinv);
+  y = mulmod_f64(d, w, q, qinv);
 }
 
 // Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
@@ -183,7 +192,10 @@ CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const do
     const int half = 1 << (E1 - 1 - r);
 #pragma unroll
     for (int j = 0; j < (1 << E1); ++j)
-      if (!(j & half)) ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << r) + (j >> (E1 - r))), q, qinv);
+      if (!(j & half)) {
+        if (r % 2 == 0) ct_bf_f64<true>(x[j], x[j + half], __ldg(roots + (1u << r) + (j >> (E1 - r))), q, qinv);
+        else ct_bf_f64<false>(x[j], x[j + half], __ldg(roots + (1u << r) + (j >> (E1 - r))), q, qinv);
+      }
   }
 #pragma unroll
   for (int j = 0; j < (1 << E1); ++j) sm[(ts + TPS * j) * kCols + c] = dbl_bits(x[j]);
@@ -201,7 +213,8 @@ CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const do
       for (int j = 0; j < (1 << E2); ++j)
         if (!(j & half)) {
           const int k = (t2 << E2) + j;
-          ct_bf_f64(y[j], y[j + half], __ldg(roots + (1u << r) + (k >> (LOGS - r))), q, qinv);
+          if (r % 2 == 0) ct_bf_f64<true>(y[j], y[j + half], __ldg(roots + (1u << r) + (k >> (LOGS - r))), q, qinv);
+          else ct_bf_f64<false>(y[j], y[j + half], __ldg(roots + (1u << r) + (k >> (LOGS - r))), q, qinv);
         }
     }
 #pragma unroll
@@ -295,7 +308,8 @@ CKG_DEV void fwd_rows_body_f64(const uint64_t* base, const PrimeConst* P, const 
 #pragma unroll
     for (int j = 0; j < 16; ++j)
       if (!(j & half))
-        ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, qinv);
+        if (r % 2 == 0) ct_bf_f64<true>(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, qinv);
+        else ct_bf_f64<false>(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (j >> (4 - r))), q, qinv);
   }
   uint64_t* srow = sm + rr * kRowPad;
 #pragma unroll
@@ -310,7 +324,8 @@ CKG_DEV void fwd_rows_body_f64(const uint64_t* base, const PrimeConst* P, const 
     for (int j = 0; j < 16; ++j)
       if (!(j & half)) {
         const int k = 16 * t + j;
-        ct_bf_f64(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, qinv);
+        if (r % 2 == 0) ct_bf_f64<true>(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, qinv);
+        else ct_bf_f64<false>(x[j], x[j + half], __ldg(roots + (1u << (s0 + r)) + (row << r) + (k >> (8 - r))), q, qinv);
       }
   }
 #pragma unroll
@@ -539,9 +554,8 @@ CKG_DEV void inv_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const do
 #pragma unroll
       for (int j = 0; j < (1 << F2); ++j)
         if (!(j & d)) {
-          const double xr = red_f64(y[j], q, qinv), yr = red_f64(y[j + d], q, qinv);
-          out[j] = canon_u64(mulmod_f64(__dadd_rn(xr, yr), ninv, q, qinv), q, qinv);
-          out[j + d] = canon_u64(mulmod_f64(__dsub_rn(xr, yr), wninv, q, qinv), q, qinv);
+          out[j] = canon_u64(mulmod_f64(__dadd_rn(y[j], y[j + d]), ninv, q, qinv), q, qinv);
+          out[j + d] = canon_u64(mulmod_f64(__dsub_rn(y[j], y[j + d]), wninv, q, qinv), q, qinv);
         }
     }
 #pragma unroll
