@@ -619,6 +619,66 @@ def timed(torch, ctx, fn, steps, warmup, dist=None):
     return ms, extra
 
 
+def stream_roofline(ops, n, k, alpha, ms_per_step, peaks):
+    """HBM fraction of the whole batched stream. Algorithmic bytes per op, inputs read once
+    and outputs written once (limbs of 8N bytes): HMult+relin+rescale 4(l+1) + 2l, rotation
+    2(l+1) + 2(l+1), PtMult+rescale 3(l+1) + 2l; plus each distinct key read once per chunk
+    (2 beta (l+1+k) limbs at the highest level that uses it there). Chunks follow the batch
+    builder: key-switching ops sorted by key, then the plaintext products, at most 128 ops
+    and 16 GiB of scratch per chunk (keys ordered here by Galois element, relinearization
+    first; the builder orders them by address, which moves at most one key group per chunk
+    boundary)."""
+    limb = 8 * n
+
+    def beta(l):
+        return (l + 1 + alpha - 1) // alpha
+
+    def conv_limbs(l):
+        return sum((l + 1) - min(alpha, l + 1 - j * alpha) + k for j in range(beta(l)))
+
+    def scratch_words(kind, l):
+        if kind == "pmul":
+            return 4 * (l + 1) * n
+        w = (3 if kind == "mul" else 1) * (l + 1) + (l + 1) + conv_limbs(l) + 2 * (l + 1 + k) + 2 * (k + l + 1)
+        return (w + (4 * (l + 1) if kind == "mul" else 0)) * n
+
+    total, ks, pm = 0, [], []
+    for kind, l, steps in ops:
+        if kind == "mul":
+            total += (4 * (l + 1) + 2 * l) * limb
+            ks.append((0, kind, l))
+        elif kind == "rot":
+            total += 4 * (l + 1) * limb
+            if steps % (n // 2):
+                ks.append((galois_elt(n, steps), kind, l))
+        else:
+            total += (3 * (l + 1) + 2 * l) * limb
+            pm.append((None, kind, l))
+    ks.sort(key=lambda x: x[0])
+    chunks, cur = [], 0
+    for key, kind, l in ks + pm:
+        w = scratch_words(kind, l)
+        if not chunks or len(chunks[-1]) >= 128 or (cur + w) * 8 > (16 << 30):
+            chunks.append([])
+            cur = 0
+        chunks[-1].append((key, l))
+        cur += w
+    key_bytes = 0
+    for ch in chunks:
+        top = {}
+        for key, l in ch:
+            if key is not None:
+                top[key] = max(top.get(key, -1), l)
+        key_bytes += sum(2 * beta(l) * (l + 1 + k) * limb for l in top.values())
+    total += key_bytes
+    peak = float(peaks.get("hbm_gbs") or 6650.0)
+    gbs = total / (ms_per_step * 1e-3) / 1e9
+    return {"scope": "whole batched stream, per step", "bound": "hbm", "alg_bytes": int(total),
+            "key_bytes": int(key_bytes), "chunks": len(chunks), "achieved": round(gbs, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(gbs / peak, 4),
+            "note": "bounded by the integer and FP64 pipes (NTT butterflies, base conversion), not by HBM"}
+
+
 def ntt_roofline(torch, S, peaks, limbs=768):
     """Forward + inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as in a
     batched stage), timed alone with CUDA events on the library's stream. Algorithmic bytes
@@ -830,6 +890,7 @@ def main():
                  "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
     roof = ntt_roofline(torch, S, peaks)
+    roof_stream = stream_roofline(rank_stream(rank, args.ops), S.n, S.ctx.k, S.ctx.alpha, ms / args.steps, peaks)
     boot = None
     if not args.no_boot:
         mix.batch = None
@@ -856,6 +917,7 @@ def main():
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
                 "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
+                "roofline_stream": roof_stream,
                 "bootstrap": boot, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line))
