@@ -584,6 +584,95 @@ class BootBench:
                 "data": "synthetic uniform key material and level-0 input; stages encoded by the library"}
 
 
+MLP_Q_BITS = [58] + [42] * 31   # n16_train (crates/ckks-train-ckks/src/params.rs:168-173)
+MLP_P_BITS = [58] * 4
+MLP_DNUM = 8
+MLP_DIMS = [196, 64, 10]
+
+
+class MlpBench:
+    """One encrypted MLP training step (config 4): the interactive trainer's SGD step
+    (crates/ckks-train-nn/src/trainer.rs) through the library's HeOps, on n16_train (N = 2^16,
+    58 + 31 x 42-bit q, 4 x 58-bit p, dnum 8, scale 2^42), Layout(2^15, 256, 64), 196 -> 64 -> 10
+    with Square, batch 64. The 53 keys (relinearization and 52 Galois keys, 288 MiB each) are
+    uniform key material and the weights, biases and batch uniform ciphertexts at the levels and
+    exact scales the client would encrypt them at: a step's time does not depend on the values.
+    Each step starts from the same network (the trainer leaves updated weights 9 levels lower)."""
+
+    def __init__(self, ckg, torch, device):
+        self.ckg, self.torch = ckg, torch
+        nn = ckg.nn
+        q, p = ckg.primes_for_bits(16, MLP_Q_BITS, MLP_P_BITS)
+        self.ctx = ctx = ckg.Context(16, q, p, MLP_DNUM, device=device, scale=2.0 ** 42)
+        n = 1 << 16
+        gen = torch.Generator(device=f"cuda:{device}")
+        gen.manual_seed(515151 + device)
+        qall = torch.tensor(q + p, dtype=torch.int64, device=f"cuda:{device}")
+
+        def uniform(shape, qcol):
+            t = torch.randint(0, 1 << 62, shape, generator=gen, device=qall.device, dtype=torch.int64) % qcol
+            torch.cuda.synchronize()
+            return t
+
+        def key(elt):
+            shape = (MLP_DNUM, 2, len(q) + len(p), n)
+            t = uniform(shape, qall.view(1, 1, -1, 1))
+            kk = ctx.upload_key_device(t.data_ptr(), shape, elt)
+            del t
+            return kk
+
+        self.layout = layout = nn.Layout(n // 2, 256, 64)
+        steps = nn.mlp_rotation_steps(MLP_DIMS, layout)
+        self.keys = [key(0)] + [key(galois_elt(n, s)) for s in steps]
+        self.ev = ev = ckg.CudaEvaluator(ctx, self.keys[0], self.keys[1:])
+        top, delta = len(q) - 1, 2.0 ** 42
+        self.cts = []
+
+        def ct(level, scale):
+            t = uniform((2, level + 1, n), qall[:level + 1].view(1, -1, 1))
+            c = ev.upload_ct_device(t.data_ptr(), 2, level, scale)
+            ctx.sync()
+            del t
+            self.cts.append(c)
+            return c
+
+        per_layer, (y_level, y_scale) = nn.Mlp.scales(ev, MLP_DIMS, top, delta)
+        self.layers = []
+        for i, (_, _, b_scale) in enumerate(per_layer):
+            sh = nn.LayerShape(MLP_DIMS[i + 1], MLP_DIMS[i], layout)
+            w = nn.EncWeights([ct(top, delta) for _ in range(sh.m)], MLP_DIMS[i + 1], MLP_DIMS[i], layout)
+            self.layers.append((w, ct(top, b_scale)))
+        self.x, self.y = ct(top, delta), ct(y_level, y_scale)
+        self.trace = None
+
+    def step(self):
+        nn = self.ckg.nn
+        mlp = nn.Mlp([(nn.Dense(w, b), nn.Square()) for w, b in self.layers])
+        tr = nn.Trainer(self.ev, self.layout, [nn.Sgd(0.05) for _ in self.layers])
+        tr.train_batch(mlp, self.x, self.y)
+        self.trace = tr.trace
+
+    def measure(self, steps=3, warmup=3):
+        ckg, torch = self.ckg, self.torch
+        self.step()
+        self.ctx.sync()
+        self.ev.reset_counter()
+        l0 = ckg.launch_count()
+        self.step()
+        self.ctx.sync()
+        launches = ckg.launch_count() - l0
+        c = self.ev.counter()
+        ms, _ = timed(torch, self.ctx, self.step, steps, warmup)
+        ks = c["rotations"] + c["relins"]
+        return {"ms": round(ms / steps, 3), "unit": "ms per training step (device events, back-to-back)",
+                "key_switches": int(ks), "keyswitch_per_s": round(ks * steps / (ms * 1e-3), 1),
+                "counts": c, "launches": int(launches),
+                "params": "n16_train: N=2^16, 58 + 31x42-bit q, 4x58-bit p, dnum 8, scale 2^42",
+                "network": "196 -> 64 -> 10, Square after each layer, SGD, batch 64, Layout(2^15, 256, 64)",
+                "levels": dict(self.trace), "keys": len(self.keys),
+                "data": "synthetic uniform key material and ciphertexts at the client's levels and scales"}
+
+
 def max_over_ranks(dist, ms, device="cuda"):
     """The slowest rank's time: every rank's device-measured milliseconds, max-reduced."""
     import torch
@@ -773,6 +862,8 @@ def main():
     ap.add_argument("--no-boot", action="store_true")
     ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
+    ap.add_argument("--no-mlp", action="store_true")
+    ap.add_argument("--mlp-only", action="store_true", help="measure the encrypted MLP training step only")
     ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
     ap.add_argument("--profile", default=None, choices=["batch", "plain", "boot"],
@@ -832,6 +923,11 @@ def main():
         for _ in range(args.warmup + 1):
             B.step()
         B.ctx.sync()
+        return
+    if args.mlp_only:
+        out = MlpBench(ckg, torch, local).measure()
+        if rank == 0:
+            print(json.dumps({"mlp_step": out}))
         return
     if args.boot_only:
         out = BootBench(ckg, torch, local).measure()
@@ -895,6 +991,12 @@ def main():
     if not args.no_boot:
         mix.batch = None
         boot = BootBench(ckg, torch, local).measure()
+    mlp_step = None
+    if not args.no_mlp:
+        mix.batch = None
+        mb = MlpBench(ckg, torch, local)
+        mlp_step = mb.measure()
+        del mb
     serving = serving_spill = None
     if not args.no_serve:
         mix.batch = None
@@ -918,7 +1020,7 @@ def main():
                 "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
                 "roofline_stream": roof_stream,
-                "bootstrap": boot, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
+                "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line))
     mix.batch = None

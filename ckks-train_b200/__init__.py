@@ -42,3 +42,4 @@ from .heops import (  # noqa: F401
     lib,
     primes_for_bits,
 )
+from . import nn  # noqa: F401,E402
