@@ -1,5 +1,6 @@
 // Device context set-up (prime constants, twiddle and conversion tables) and the
 // polynomial-level algorithms of the evaluator path. See engine.hpp for the layouts.
+#include <cmath>
 #include <cstring>
 
 #include "engine.hpp"
@@ -44,47 +45,104 @@ DevBufPtr Context::alloc(size_t words) {
 
 namespace {
 
-// Conversion table record (kernels.cuh ConvLayout) for sources `src` -> targets `dst`
-// (global prime indices): sum_j y_j [S/s_j]_t - e [S]_t - [h]_t with h = (S-1)/2.
+// Whether target t of a conversion from `src` can take the FP64-assisted form (kernels.cu,
+// k_bconv_f64): V = sum_j y_j w_tj + e (t - [S]_t) + (t - [h]_t) is computed mod 2^64 on the
+// integer pipe, its quotient K = V / t is estimated as A = sum_j fl(y_j) fl(w_tj / t) + e fl(..)
+// + fl(..) by an FP64 FMA chain, and r = V - rint(A) t must stay inside the signed 64-bit range
+// with room to spare. With T_j = y_j w_tj / t < s_j: each term's representation error is at most
+// s_j (e1 + e2) (plus e1 e2), where fl(w_tj / t) carries e2 = 2^-53 (3 2^-53 when t >= 2^53, as
+// w_tj and t are rounded first) and fl(y_j) e1 = 0 (2^-53 when s_j > 2^53); each of the n + 2
+// roundings of the chain is at most half an ulp of A_max = sum_j s_j + 17, the two constant
+// terms add 17 2^-52, and rint 1/2. Their sum bounds |K - rint(A)|, and t times it must be at
+// most 2^62. `two_stage` is set unless the estimate alone is within 1/2, where r already lies in
+// (-t, t).
+bool conv_f64_form(const std::vector<HostMod>& mods, const std::vector<uint32_t>& src, uint32_t t, bool* two_stage) {
+  const uint64_t q = mods[t].q;
+  if (src.empty() || src.size() > (size_t)kMaxSrcF64 || q < (1ULL << 30)) return false;
+  const int e2 = q >= (1ULL << 53) ? 3 : 1;
+  long double sum = 0, rep = 0;
+  for (uint32_t s : src) {
+    const long double v = (long double)mods[s].q;
+    sum += v;
+    rep += v * (e2 + (mods[s].q > (1ULL << 53) ? 1 : 0));
+  }
+  const long double amax = (sum + 17 + 64) * (1 + ldexpl(1.0L, -40));
+  const long double ulp = ldexpl(1.0L, ilogbl(amax) - 52);
+  const long double eta = rep * ldexpl(1.0L, -53) + (long double)(src.size() + 2) * ulp / 2 + 17 * ldexpl(1.0L, -52) +
+                          ldexpl(1.0L, -30);
+  *two_stage = eta >= 0.5L;
+  return (eta + 0.5L) * (long double)q <= ldexpl(1.0L, 62);
+}
+
+// Conversion table (kernels.cuh ConvLayout) for sources `src` -> targets `dst` (global prime
+// indices): sum_j y_j [S/s_j]_t - e [S]_t - [h]_t with h = (S-1)/2. Targets that allow it get the
+// FP64-assisted record and come first.
 std::vector<uint64_t> conv_table(const std::vector<HostMod>& mods, const std::vector<uint32_t>& src,
                                  const std::vector<uint32_t>& dst) {
   std::vector<uint64_t> w;
   const size_t ns = src.size();
+  auto bits = [](double v) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    return b;
+  };
+  w.push_back(0);  // FP64-assisted record count, set below
   for (size_t j = 0; j < ns; ++j) {
     const HostMod& m = mods[src[j]];
     uint64_t qhat = 1;
     for (size_t i = 0; i < ns; ++i)
       if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
     uint64_t qhinv = m.inv(qhat);
-    double inv = 1.0 / (double)m.q;
-    uint64_t inv_bits;
-    memcpy(&inv_bits, &inv, 8);
     w.push_back(src[j]);
     w.push_back(qhinv);
     w.push_back(m.shoup(qhinv));
     w.push_back(m.q >> 1);
-    w.push_back(inv_bits);
+    w.push_back(bits(1.0 / (double)m.q));
   }
-  for (uint32_t t : dst) {
+  std::vector<std::pair<size_t, bool>> order;  // (output position, two_stage); FP64 records first
+  std::vector<size_t> exact;
+  for (size_t o = 0; o < dst.size(); ++o) {
+    bool two = false;
+    if (conv_f64_form(mods, src, dst[o], &two)) order.push_back({o, two});
+    else exact.push_back(o);
+  }
+  w[0] = order.size();
+  for (size_t o : exact) order.push_back({o, false});
+  for (size_t r = 0; r < order.size(); ++r) {
+    const bool f64 = r < w[0];
+    const size_t o = order[r].first;
+    const uint32_t t = dst[o];
     const HostMod& m = mods[t];
     uint64_t S = 1 % m.q;
     for (uint32_t s : src) S = m.mul(S, mods[s].q % m.q);
     // h = (S - 1)/2 mod t = (S - 1) * 2^-1
     uint64_t h = m.mul(m.sub(S, 1 % m.q), (m.q + 1) / 2);
     const uint64_t r64 = (uint64_t)(((u128)1 << 64) % m.q);
-    w.push_back(t);
-    w.push_back(m.q - S);
-    w.push_back(m.q - h);
-    w.push_back(m.q);
-    w.push_back(r64);
-    w.push_back(m.shoup(r64));
-    w.push_back(m.shoup(1));
-    w.push_back(0);
+    std::vector<uint64_t> qh(ns);
     for (size_t j = 0; j < ns; ++j) {
       uint64_t qhat = 1 % m.q;
       for (size_t i = 0; i < ns; ++i)
         if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
-      w.push_back((qhat & ((1ULL << 30) - 1)) | ((qhat >> 30) << 32));
+      qh[j] = qhat;
+    }
+    w.push_back(t);
+    w.push_back(m.q - S);
+    w.push_back(m.q - h);
+    w.push_back(m.q);
+    if (f64) {
+      w.push_back(bits(1.0 / (double)m.q));
+      w.push_back(bits((double)(m.q - S) / (double)m.q));
+      w.push_back(bits((double)(m.q - h) / (double)m.q));
+      w.push_back(o | ((uint64_t)order[r].second << 32));
+      for (size_t j = 0; j < ns; ++j) w.push_back(qh[j]);
+      for (size_t j = 0; j < ns; ++j) w.push_back(bits((double)qh[j] / (double)m.q));
+    } else {
+      w.push_back(r64);
+      w.push_back(m.shoup(r64));
+      w.push_back(m.shoup(1));
+      w.push_back(o);
+      for (size_t j = 0; j < ns; ++j) w.push_back((qh[j] & ((1ULL << 30) - 1)) | ((qh[j] >> 30) << 32));
+      for (size_t j = 0; j < ns; ++j) w.push_back(0);
     }
   }
   return w;

@@ -701,71 +701,144 @@ CKG_DEV uint64_t reduce128_rec(uint64_t hi, uint64_t lo, const uint64_t* rec) {
 
 constexpr uint64_t kMask30 = (1ULL << 30) - 1;
 
+// f64(v) rounded to nearest (ties to even), on the FP64 pipe: both 32-bit halves are exact
+// doubles (2^52 + x - 2^52), and one FMA rounds hi 2^32 + lo once. Equal to __ull2double_rn.
+CKG_DEV double u64_to_f64_rn(uint64_t v) {
+  const double hi = __dsub_rn(__hiloint2double(0x43300000, (int)(uint32_t)(v >> 32)), 4503599627370496.0);
+  const double lo = __dsub_rn(__hiloint2double(0x43300000, (int)(uint32_t)v), 4503599627370496.0);
+  return __fma_rn(hi, 4294967296.0, lo);
+}
+
+// One pass over the sources, then every target record of the job's table. Each thread converts
+// kBconvU coefficients (c, c + 256, ...). y_j = [(x_j + h_j) qhat_j^-1]_{s_j} stays in registers; the
+// overflow estimate is e = floor(sum_j f64(y_j) f64(1/s_j)) (0 for one source). NS is the source
+// count (1..8), or 0 for more sources, which have exact records only.
+//
+// FP64-assisted records (the first `head` of the table; the host admits a target only when the
+// bound below holds): V = sum_j y_j w_tj + e (t - [S]_t) + (t - [h]_t) is summed mod 2^64 with
+// 64-bit multiply-adds, its quotient by t is estimated by an FP64 FMA chain over f64(y_j) and
+// f64(w_tj / t), and r = V - k t (k = rint of the estimate) is exact as a signed 64-bit value
+// since |V / t - k| t <= 2^62. A second rounded quotient of f64(r) brings r into (-t, t)
+// (records flagged two_stage), and one conditional add into [0, t).
+//
+// Exact records: y_j split into 30-bit halves, so every product is a 32x32->64 multiply-add
+// into one of four 64-bit accumulators (A = lo*lo, B1 = lo*hi, B2 = hi*lo, C = hi*hi, each
+// < 16 * 2^60), assembled into 128 bits and reduced once.
+constexpr int kBconvU = 1;  // coefficients per thread (registers: one y_j per source each)
+
 template <int NS, class B>
 __global__ void __launch_bounds__(256)
     k_bconv(const __grid_constant__ B cb, const PrimeConst* __restrict__ pc, int n) {
-  __shared__ uint64_t sd[kMaxDst * (8 + kMaxSrc)];
+  constexpr int K = NS > 0 ? NS : kMaxSrc;
+  __shared__ uint64_t sd[kMaxDst * (8 + 2 * kMaxSrc)];
   const ConvJob& job = cb.j[blockIdx.y];
+  const uint64_t* tab = job.table;
+  const int head = (int)__ldg(tab);
   const int n_src = NS > 0 ? NS : cb.n_src;
   const int dw = ConvLayout::dst_words(n_src);
-  const uint64_t* tab = job.table;
+  const uint64_t* src_tab = tab + ConvLayout::kHeadWords;
   {
-    const uint64_t* dtab = tab + ConvLayout::kSrcWords * n_src;
+    const uint64_t* dtab = src_tab + ConvLayout::kSrcWords * n_src;
     for (int i = threadIdx.x; i < dw * job.n_dst; i += blockDim.x) sd[i] = __ldg(dtab + i);
   }
-  const int c0 = blockIdx.x * 512 + threadIdx.x;
-  bool ok[2] = {c0 < n, c0 + 256 < n};
-  uint32_t ylo[2][kMaxSrc], yhi[2][kMaxSrc];
-  double f[2] = {0.0, 0.0};
+  constexpr int U = kBconvU;
+  const int c0 = blockIdx.x * (256 * U) + threadIdx.x;
+  bool ok[U];
 #pragma unroll
-  for (int j = 0; j < kMaxSrc; ++j) {
-    if (j < n_src) {
-      const uint64_t* s = tab + ConvLayout::kSrcWords * j;
-      const uint32_t p = (uint32_t)__ldg(s);
-      const uint64_t q = __ldg(&pc[p].q), h = __ldg(s + 3), w = __ldg(s + 1), ws = __ldg(s + 2);
-      const double inv = __longlong_as_double((long long)__ldg(s + 4));
+  for (int u = 0; u < U; ++u) ok[u] = c0 + 256 * u < n;
+  uint64_t y[U][K];
+  uint64_t e[U];
+  {
+    double f[U];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const uint64_t x = ok[u] ? job.src[j * job.src_stride + c0 + 256 * u] : 0;
-        const uint64_t yj = mul_shoup(add_mod(x, h, q), w, ws, q);
-        ylo[u][j] = (uint32_t)(yj & kMask30);
-        yhi[u][j] = (uint32_t)(yj >> 30);
-        const double prod = __dmul_rn(__ull2double_rn(yj), inv);
-        f[u] = j == 0 ? prod : __dadd_rn(f[u], prod);
+    for (int j = 0; j < K; ++j) {
+      if (j < n_src) {
+        const uint64_t* s = src_tab + ConvLayout::kSrcWords * j;
+        const uint32_t p = (uint32_t)__ldg(s);
+        const uint64_t q = __ldg(&pc[p].q), h = __ldg(s + 3), w = __ldg(s + 1), ws = __ldg(s + 2);
+        const double inv = __longlong_as_double((long long)__ldg(s + 4));
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const uint64_t x = ok[u] ? job.src[j * job.src_stride + c0 + 256 * u] : 0;
+          const uint64_t yj = mul_shoup(add_mod(x, h, q), w, ws, q);
+          y[u][j] = yj;
+          const double prod = __dmul_rn(u64_to_f64_rn(yj), inv);
+          f[u] = j == 0 ? prod : __dadd_rn(f[u], prod);
+        }
       }
     }
+#pragma unroll
+    for (int u = 0; u < U; ++u) e[u] = n_src > 1 ? (uint64_t)floor(f[u]) : 0;
   }
-  uint64_t e[2];
-#pragma unroll
-  for (int u = 0; u < 2; ++u) e[u] = n_src > 1 ? (uint64_t)floor(f[u]) : 0;
   __syncthreads();
-  for (int t = 0; t < job.n_dst; ++t) {
+  for (int t = 0; t < (NS > 0 ? head : 0); ++t) {
     const uint64_t* d = sd + dw * t;
-    uint64_t A[2] = {0, 0}, B1[2] = {0, 0}, B2[2] = {0, 0}, Cc[2] = {0, 0};
+    uint64_t S[U];
+    double Af[U];
 #pragma unroll
-    for (int j = 0; j < kMaxSrc; ++j) {
+    for (int u = 0; u < U; ++u) S[u] = 0, Af[u] = 0.0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const uint64_t w = d[8 + j];
+      const double wq = __longlong_as_double((long long)d[8 + n_src + j]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        S[u] += y[u][j] * w;
+        Af[u] = __fma_rn(u64_to_f64_rn(y[u][j]), wq, Af[u]);
+      }
+    }
+    const uint64_t negS = d[1], negH = d[2], q = d[3];
+    const double qinv = __longlong_as_double((long long)d[4]);
+    const double nS = __longlong_as_double((long long)d[5]), nH = __longlong_as_double((long long)d[6]);
+    const uint64_t meta = d[7];
+    const size_t out = (size_t)(uint32_t)meta * job.dst_stride;
+    const bool two_stage = (meta >> 32) != 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t V = S[u] + e[u] * negS + negH;
+      const double A = __dadd_rn(__fma_rn((double)e[u], nS, Af[u]), nH);
+      const uint64_t k = (uint64_t)__double2ll_rn(A);
+      int64_t r = (int64_t)(V - k * q);
+      if (two_stage) {
+        // |r| <= 2^62: the rounded quotient of f64(r) is within 1 of r / t's nearest integer
+        const double rq = __dmul_rn(__ll2double_rn(r), qinv);
+        r -= __double2ll_rn(rq) * (int64_t)q;
+      }
+      if (r < 0) r += (int64_t)q;
+      if (ok[u]) job.dst[out + c0 + 256 * u] = (uint64_t)r;
+    }
+  }
+  for (int t = head; t < job.n_dst; ++t) {
+    const uint64_t* d = sd + dw * t;
+    uint64_t A[U], B1[U], B2[U], Cc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) A[u] = B1[u] = B2[u] = Cc[u] = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
       if (j < n_src) {
         const uint64_t w = d[8 + j];
         const uint32_t wl = (uint32_t)w, wh = (uint32_t)(w >> 32);
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          A[u] += (uint64_t)ylo[u][j] * wl;
-          B1[u] += (uint64_t)ylo[u][j] * wh;
-          B2[u] += (uint64_t)yhi[u][j] * wl;
-          Cc[u] += (uint64_t)yhi[u][j] * wh;
+        for (int u = 0; u < U; ++u) {
+          const uint32_t yl = (uint32_t)(y[u][j] & kMask30), yh = (uint32_t)(y[u][j] >> 30);
+          A[u] += (uint64_t)yl * wl;
+          B1[u] += (uint64_t)yl * wh;
+          B2[u] += (uint64_t)yh * wl;
+          Cc[u] += (uint64_t)yh * wh;
         }
       }
     }
     const uint64_t negS = d[1], negH = d[2];
+    const size_t out = (size_t)(uint32_t)d[7] * job.dst_stride;
 #pragma unroll
-    for (int u = 0; u < 2; ++u) {
+    for (int u = 0; u < U; ++u) {
       uint64_t lo = A[u], hi = 0;
       add128(hi, lo, B1[u] >> 34, B1[u] << 30);
       add128(hi, lo, B2[u] >> 34, B2[u] << 30);
       add128(hi, lo, Cc[u] >> 4, Cc[u] << 60);
       add128(hi, lo, 0, e[u] * negS);  // e < 16, so e * (t - [S]_t) < 2^64
       add128(hi, lo, 0, negH);
-      if (ok[u]) job.dst[t * job.dst_stride + c0 + 256 * u] = reduce128_rec(hi, lo, d);
+      if (ok[u]) job.dst[out + c0 + 256 * u] = reduce128_rec(hi, lo, d);
     }
   }
 }
@@ -1037,11 +1110,15 @@ void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStr
 template <class B>
 void bconv_launch(const DevTables& d, const B& cb, int count, int n_src, cudaStream_t st) {
   const int n = 1 << d.log_n;
-  dim3 grid((n + 511) / 512, count);
+  dim3 grid((n + 256 * kBconvU - 1) / (256 * kBconvU), count);
   switch (n_src) {
     case 1: k_bconv<1, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
     case 2: k_bconv<2, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 3: k_bconv<3, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
     case 4: k_bconv<4, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 5: k_bconv<5, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 6: k_bconv<6, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
+    case 7: k_bconv<7, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
     case 8: k_bconv<8, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
     default: k_bconv<0, B><<<grid, 256, 0, st>>>(cb, d.prime, n); break;
   }

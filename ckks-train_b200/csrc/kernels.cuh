@@ -66,15 +66,25 @@ struct ConvBatch {
 };
 
 // Table record (u64 words):
+//   header, 1 word: the number of leading dst records in the FP64-assisted form
 //   src block, 5 words per source j: prime, qhat_inv, qhat_inv_shoup, half_j, bits(1.0/s_j)
-//   dst block, (8 + n_src) words per target t: prime, (t - [S]_t), (t - [h]_t), t, [2^64]_t,
-//   its Shoup companion, floor(2^64/t), pad, then w_tj = [S/s_j]_t split into 30-bit halves
-//   (low half in bits 0..29, high half in bits 32..61)
+//   dst block, (8 + 2 n_src) words per target t, in one of two forms:
+//   - exact: prime, (t - [S]_t), (t - [h]_t), t, [2^64]_t, its Shoup companion, floor(2^64/t),
+//     out, then w_tj = [S/s_j]_t split into 30-bit halves (low half in bits 0..29, high half in
+//     bits 32..61), then n_src unused words;
+//   - FP64-assisted: prime, (t - [S]_t), (t - [h]_t), t, bits(1/t), bits((t - [S]_t)/t),
+//     bits((t - [h]_t)/t), out | two_stage << 32, then w_tj whole, then bits(w_tj / t);
+//   `out` is the target's limb position in the job's output (records may be reordered).
 struct ConvLayout {
+  static constexpr int kHeadWords = 1;
   static constexpr int kSrcWords = 5;
-  static __host__ __device__ int dst_words(int n_src) { return 8 + n_src; }
-  static __host__ __device__ int size(int n_src, int n_dst) { return kSrcWords * n_src + dst_words(n_src) * n_dst; }
+  static __host__ __device__ int dst_words(int n_src) { return 8 + 2 * n_src; }
+  static __host__ __device__ int size(int n_src, int n_dst) {
+    return kHeadWords + kSrcWords * n_src + dst_words(n_src) * n_dst;
+  }
 };
+// FP64-assisted records serve at most this many sources (kernel register arrays).
+constexpr int kMaxSrcF64 = 8;
 
 // Key-switch inner product of one level-l polynomial (module docs of keyswitch.cu).
 constexpr int kMaxDigits = 16;
