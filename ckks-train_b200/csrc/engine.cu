@@ -74,6 +74,22 @@ bool conv_f64_form(const std::vector<HostMod>& mods, const std::vector<uint32_t>
   return (eta + 0.5L) * (long double)q <= ldexpl(1.0L, 62);
 }
 
+// The inner product's FP64-assisted form for outputs modulo q (kernels.cu k_inner_product):
+// with d_j, k_j < q < 2^50 exact in f64, A = sum_j d_j fl(fl(k_j) fl(1/q)) by FMA is within
+// delta of V / q (each term's factor carries 2^-52 relative, each of the beta roundings half an
+// ulp of A_max = beta q, rint 1/2). Returns the offset ceil(delta) that makes
+// x = V - rint(A) q + ceil(delta) q nonnegative, or 0 when A_max >= 2^52 or x could reach 2^53.
+uint32_t ip_f64_offset(uint64_t q, uint32_t beta) {
+  if (q >= (1ULL << 50)) return 0;
+  const long double amax = (long double)beta * q * (1 + ldexpl(1.0L, -40)) + 64;
+  if (amax >= ldexpl(1.0L, 52)) return 0;
+  const long double ulp = ldexpl(1.0L, ilogbl(amax) - 52);
+  const long double delta = (long double)beta * q * ldexpl(1.0L, -52) + beta * ulp / 2 + 0.5L + ldexpl(1.0L, -30);
+  const long double off = ceill(delta);
+  if ((off + delta) * q >= ldexpl(1.0L, 53)) return 0;
+  return (uint32_t)off;
+}
+
 // Conversion table (kernels.cuh ConvLayout) for sources `src` -> targets `dst` (global prime
 // indices): sum_j y_j [S/s_j]_t - e [S]_t - [h]_t with h = (S-1)/2. Targets that allow it get the
 // FP64-assisted record and come first.
@@ -224,6 +240,7 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
     c.qinv = 1.0 / c.qd;
     c.ninvd = (double)c.ninv;
     c.wninvd = (double)c.wninv;
+    c.ip_off = ip_f64_offset(m.q, dnum);
   }
   std::vector<double> twdf(np * n), twdi(np * n);
   for (size_t i = 0; i < np * n; ++i) {

@@ -843,6 +843,22 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// f64(v) for v < 2^52, exact: the bits of 2^52 + v minus 2^52.
+CKG_DEV double f64_small(uint64_t v) {
+  return __dsub_rn(__longlong_as_double((long long)(v | 0x4330000000000000ULL)), 4503599627370496.0);
+}
+// rint(x) as an integer for 0 <= x < 2^52: 2^52 + x rounds to an integer in [2^52, 2^53).
+CKG_DEV uint64_t rint_small(double x) {
+  return (uint64_t)__double_as_longlong(__dadd_rn(x, 4503599627370496.0)) - 0x4330000000000000ULL;
+}
+// The FP64-assisted inner-product result: S = V mod 2^64, A ~ V / q within delta < off, base =
+// off q: x = S - rint(A) q + base is V + (off - k) q in [0, (off + delta) q) < 2^53.
+CKG_DEV uint64_t ip_finish_f64(uint64_t S, double A, uint64_t q, double q_d, double qinv, uint64_t base) {
+  const uint64_t x = S - rint_small(A) * q + base;
+  const int64_t r = (int64_t)(x - rint_small(__dmul_rn(u64_to_f64_rn(x), qinv)) * q);
+  return (uint64_t)(r < 0 ? r + (int64_t)q : r);
+}
+
 // ------------------------------------------------------------------------------------
 // Key-switch inner product (crates/ckks-train-ckks/src/keyswitch.rs:230-309): for every
 // limb i of Q_l * P, out_b = sum_j d_j * b_j and out_a = sum_j d_j * a_j, accumulated
@@ -852,7 +868,7 @@ __global__ void __launch_bounds__(256)
 // ------------------------------------------------------------------------------------
 
 template <class B>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 8 : 1)
     k_inner_product(const __grid_constant__ B ib, const PrimeConst* __restrict__ pc, int log_n) {
   const int n = 1 << log_n;
   // By-value lists: grid (coefficient blocks, limbs, jobs). Device-resident lists (the
@@ -869,14 +885,11 @@ __global__ void __launch_bounds__(256)
   const int key_limb = is_q ? i : job.key_q + (i - l - 1);
   const size_t key_limbs = (size_t)(job.key_q + ib.k);
   const uint32_t src_c = job.perm ? __ldg(job.perm + c) : (uint32_t)c;
-  // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits).
   // By-value lists (one op's jobs) load the words of up to 4 digits before their products so
   // the loads overlap; the batched grid, whose many resident jobs already keep loads in
   // flight, keeps one digit per step (measured faster there).
-  uint64_t Ab = 0, B1b = 0, B2b = 0, Cb = 0, Aa = 0, B1a = 0, B2a = 0, Ca = 0;
   constexpr int kChunk = kJobFast ? 1 : 4;
-  for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
-    uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+  auto load = [&](int j0, uint64_t* dv, uint64_t* kbv, uint64_t* kav) {
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       const int j = j0 + u;
@@ -893,6 +906,41 @@ __global__ void __launch_bounds__(256)
         kav[u] = __ldcs(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c);
       }
     }
+  };
+  const PrimeConst& P = pc[prime];
+  const size_t o = ((size_t)i << log_n) + c;
+  if (P.ip_off) {
+    // FP64-assisted (data primes below 2^50 whose digit sums allow it, PrimeConst::ip_off):
+    // S = sum_j d_j k_j mod 2^64 on the integer pipe; A = sum_j d_j fl(k_j / q) by FMA, within
+    // delta < ip_off of the quotient, so x = S - rint(A) q + ip_off q lies in [0, 2^53); a
+    // second rounded quotient of x (exact in f64) brings it into (-q, q), one add into [0, q).
+    const double q_d = P.qd, qinv = P.qinv;
+    uint64_t Sb = 0, Sa = 0;
+    double Ab = 0.0, Aa = 0.0;
+    for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
+      uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+      load(j0, dv, kbv, kav);
+#pragma unroll
+      for (int u = 0; u < kChunk; ++u) {
+        if (j0 + u >= job.ndig) break;
+        const uint64_t d = dv[u], kb = kbv[u], ka = kav[u];
+        Sb += d * kb;
+        Sa += d * ka;
+        const double dd = f64_small(d);
+        Ab = __fma_rn(dd, __dmul_rn(f64_small(kb), qinv), Ab);
+        Aa = __fma_rn(dd, __dmul_rn(f64_small(ka), qinv), Aa);
+      }
+    }
+    const uint64_t q = P.q, base = (uint64_t)P.ip_off * q;
+    job.out_b[o] = ip_finish_f64(Sb, Ab, q, q_d, qinv, base);
+    job.out_a[o] = ip_finish_f64(Sa, Aa, q, q_d, qinv, base);
+    return;
+  }
+  // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits).
+  uint64_t Ab = 0, B1b = 0, B2b = 0, Cb = 0, Aa = 0, B1a = 0, B2a = 0, Ca = 0;
+  for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
+    uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+    load(j0, dv, kbv, kav);
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       if (j0 + u >= job.ndig) break;
@@ -910,18 +958,17 @@ __global__ void __launch_bounds__(256)
       Ca += (uint64_t)dh * ah;
     }
   }
-  const PrimeConst& P = pc[prime];
   uint64_t lo = Ab, hi = 0;
   add128(hi, lo, B1b >> 34, B1b << 30);
   add128(hi, lo, B2b >> 34, B2b << 30);
   add128(hi, lo, Cb >> 4, Cb << 60);
-  job.out_b[((size_t)i << log_n) + c] = reduce128(hi, lo, P);
+  job.out_b[o] = reduce128(hi, lo, P);
   lo = Aa;
   hi = 0;
   add128(hi, lo, B1a >> 34, B1a << 30);
   add128(hi, lo, B2a >> 34, B2a << 30);
   add128(hi, lo, Ca >> 4, Ca << 60);
-  job.out_a[((size_t)i << log_n) + c] = reduce128(hi, lo, P);
+  job.out_a[o] = reduce128(hi, lo, P);
 }
 
 // ------------------------------------------------------------------------------------

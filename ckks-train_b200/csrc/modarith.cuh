@@ -23,7 +23,7 @@ struct PrimeConst {
   uint64_t r64_s;
   uint64_t one_s;    // floor(2^64 / q): Shoup companion of 1 (reduces any u64 to [0, 2q))
   uint32_t b;        // bit length of q
-  uint32_t pad;
+  uint32_t ip_off;   // nonzero: the inner product may take its FP64-assisted form (kernels.cu)
   double qd, qinv;     // q and fl(1/q) for the FP64 butterflies of primes below 2^50
   double ninvd, wninvd;  // ninv and wninv as doubles (exact: < q < 2^50)
 };

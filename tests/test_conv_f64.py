@@ -1,5 +1,6 @@
-"""The FP64-assisted form of exact base conversion (kernels.cu k_bconv_f64, admitted per target
-by engine.cu conv_f64_form), replayed in exact arithmetic on the CPU: FMA and every rounding
+"""The FP64-assisted forms of exact base conversion (kernels.cu k_bconv, admitted per target by
+engine.cu conv_f64_form) and of the key-switch inner product (k_inner_product, admitted per
+prime by engine.cu ip_f64_offset), replayed in exact arithmetic on the CPU: FMA and every rounding
 emulated with Fractions (float(Fraction) rounds to nearest even), on the prime chains of the
 configurations and with the sources at their extremes. For every admitted target the residual
 r = V - rint(A) t must stay within the admission bound, and the second rounded quotient plus
@@ -107,3 +108,48 @@ def test_fp64_assisted_conversion_bound(ckg, name):
     assert seen["f64"] > 0
     if name == "cfg2":  # data-prime targets of ModUp and the rescale are admitted, 60-bit ones not
         assert seen["exact"] > 0 and seen["two_stage"] > 0
+
+
+def ip_offset(q, beta):
+    """engine.cu ip_f64_offset."""
+    if q >= 2 ** 50:
+        return 0
+    amax = beta * q * (1 + 2.0 ** -40) + 64
+    if amax >= 2.0 ** 52:
+        return 0
+    ulp = 2.0 ** (math.floor(math.log2(amax)) - 52)
+    delta = beta * q * 2.0 ** -52 + beta * ulp / 2 + 0.5 + 2.0 ** -30
+    off = math.ceil(delta)
+    return 0 if (off + delta) * q >= 2.0 ** 53 else off
+
+
+@pytest.mark.parametrize("name", sorted(CHAINS))
+def test_fp64_assisted_inner_product(ckg, name):
+    """k_inner_product's FP64-assisted form (ip_finish_f64) replayed exactly: for every admitted
+    prime and digit count up to dnum, extreme and random digits and key words give V mod q."""
+    log_n, qb, pb, dnum = CHAINS[name]
+    q, p = ckg.primes_for_bits(log_n, qb, pb)
+    rng = np.random.default_rng(9)
+    admitted_primes = 0
+    for prime in sorted(set(q) | set(p)):
+        off = ip_offset(prime, dnum)
+        if not off:
+            continue
+        admitted_primes += 1
+        qinv = fl(Fraction(1) / Fraction(prime))
+        for beta in range(1, dnum + 1):
+            trials = [([prime - 1] * beta, [prime - 1] * beta),
+                      ([int(x) % prime for x in rng.integers(0, 2 ** 62, beta)],
+                       [int(x) % prime for x in rng.integers(0, 2 ** 62, beta)])]
+            for ds, ks in trials:
+                V = sum(d * k for d, k in zip(ds, ks))
+                A = 0.0
+                for d, k in zip(ds, ks):
+                    A = fma(float(d), fl(Fraction(float(k)) * Fraction(qinv)), A)
+                assert 0 <= A < 2 ** 52
+                x = V - rint(A) * prime + off * prime
+                assert 0 <= x < 2 ** 53
+                r = x - rint(fl(Fraction(float(x)) * Fraction(qinv))) * prime
+                assert -prime < r < prime
+                assert (r + prime if r < 0 else r) == V % prime
+    assert admitted_primes > 0
