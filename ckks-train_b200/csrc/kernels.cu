@@ -80,13 +80,12 @@ CKG_DEV ulonglong2 ldtw(const ulonglong2* t, uint32_t i) { return __ldg(t + i); 
 
 CKG_DEV int pad_idx(int k) { return k + (k >> 4); }
 
-// FP64 butterflies for primes below 2^50, on the FP64 pipe instead of IMAD. Values are
-// exact integers held in doubles, signed and lazy: every butterfly input lies in (-2q, 2q).
-// w*y mod q: hi = fl(w y) and lo = fma(w, y, -hi) hold the exact product (|w y| < 2q^2 <
-// 2^101); k = rint(hi / q) is within 1.25 of w y / q (|hi / q| < 2q < 2^51), so fma(-k, q, hi) + lo = w y - k q is an integer below 2^51 in
-// magnitude and every step is exact. (k = rint(hi / q), taken by the native rounding
-// instruction, is within 1.25 of w y / q because |hi / q| < 2q < 2^51.) Inputs and outputs of a transform are canonical u64;
-// between its two passes the limb holds the raw doubles.
+// FP64 butterflies for primes below 2^50, on the FP64 pipe instead of IMAD. Values are exact
+// integers held in doubles, signed and lazy (bounds at mulmod_f64 and ct_bf_f64 / gs_bf_f64).
+// w*y mod q: hi = fl(w y) and lo = fma(w, y, -hi) hold the exact product; k = rint(hi / q) by the
+// native rounding instruction; fma(-k, q, hi) + lo = w y - k q is then an integer below 2^53 in
+// magnitude and every step is exact. Inputs and outputs of a transform are canonical u64; between
+// its two passes the limb holds the raw doubles.
 constexpr uint64_t kF64Bound = 1ULL << 50;
 constexpr double kTwo52 = 4503599627370496.0;
 
