@@ -206,11 +206,26 @@ class Mix:
                 host.append((ta.cpu().pin_memory(), None if tb is None else tb.cpu().pin_memory()))
             del ta, tb
         self.host = host
+        self.chunk_items = None
         self.batch, self.outputs = self.make_batch(self.inputs)
         self.ks = self.batch.key_switches()
 
+    def tune(self, ntt_wave=None, chunk_items=None, reps=3):
+        """The library's autotuner on this stream (NTT limb wave x chunk size), or the given
+        settings. Tuning replays run before any timed region."""
+        if ntt_wave is None or chunk_items is None:
+            out = self.batch.autotune(reps)
+        else:
+            self.S.ctx.ntt_wave = ntt_wave
+            self.batch.chunk_items = chunk_items
+            out = {"ntt_wave": ntt_wave, "chunk_items": chunk_items, "trials": []}
+        self.chunk_items = out["chunk_items"]
+        return out
+
     def make_batch(self, inputs):
         b = self.S.ckg.Batch(self.S.ev)
+        if self.chunk_items:
+            b.chunk_items = self.chunk_items
         outs = []
         for kind, a, extra, steps in inputs:
             if kind == "mul":
@@ -863,6 +878,8 @@ def main():
     ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
     ap.add_argument("--no-mlp", action="store_true")
+    ap.add_argument("--ntt-wave", type=int, default=None, help="fixed NTT limb wave (with --chunk-items; default: autotune)")
+    ap.add_argument("--chunk-items", type=int, default=None, help="fixed batch chunk size (with --ntt-wave)")
     ap.add_argument("--mlp-only", action="store_true", help="measure the encrypted MLP training step only")
     ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
@@ -953,6 +970,7 @@ def main():
         S.ctx.sync()
         return
     mix = Mix(S, rank_stream(rank, args.ops), keep_host=not args.no_e2e and args.profile is None)
+    tuning = mix.tune(args.ntt_wave, args.chunk_items)
     l0 = ckg.launch_count()
     mix.batch.capture_graph()
     launches_per_step = ckg.launch_count() - l0
@@ -1017,7 +1035,10 @@ def main():
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64",
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
-                "config": dict(config, key_switches_per_step=int(mix.ks)), "e2e": e2e,
+                "config": dict(config, key_switches_per_step=int(mix.ks),
+                               autotune={"ntt_wave": tuning["ntt_wave"], "chunk_items": tuning["chunk_items"],
+                                         "trials_ms": [[w, c, round(m, 3)] for w, c, m in tuning["trials"]]}),
+                "e2e": e2e,
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
                 "roofline_stream": roof_stream,
                 "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,

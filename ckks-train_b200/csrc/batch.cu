@@ -8,8 +8,8 @@ namespace ckg {
 
 namespace {
 
-// Upper bounds of one chunk: items and scratch bytes. Chunks run one after another on
-// the context's stream and reuse one scratch region.
+// Upper bounds of one chunk: items (the default; Batch::set_chunk_items) and scratch bytes.
+// Chunks run one after another on the context's stream and reuse one scratch region.
 constexpr size_t kChunkItems = 128;
 constexpr size_t kChunkScratchBytes = (size_t)16 << 30;
 
@@ -49,12 +49,77 @@ struct Batch::Stage {
   int ip_max_limbs = 0;
 };
 
-Batch::Batch(Evaluator* ev) : ev_(ev), ctx_(ev->ctx()) {}
+Batch::Batch(Evaluator* ev) : ev_(ev), ctx_(ev->ctx()), chunk_items_(kChunkItems) {}
 
-Batch::~Batch() {
+Batch::~Batch() { reset(); }
+
+void Batch::reset() {
   if (exec_) cudaGraphExecDestroy(exec_);
   if (graph_) cudaGraphDestroy(graph_);
+  exec_ = nullptr;
+  graph_ = nullptr;
   for (auto* s : chunks_) delete s;
+  chunks_.clear();
+  desc_.reset();
+  scratch_.reset();
+  built_ = false;
+}
+
+void Batch::set_chunk_items(size_t items) {
+  if (items < 1 || items > 4096) throw Error(ST_INVALID_PARAMS, "chunk size must be in 1..=4096");
+  if (items != chunk_items_) reset();
+  chunk_items_ = items;
+}
+
+std::vector<Batch::Trial> Batch::autotune(int reps) {
+  static const int kWaves[] = {0, 32, 64, 128, 256};
+  static const int kChunks[] = {64, 128, 256};
+  if (reps < 1 || reps > 100) throw Error(ST_INVALID_PARAMS, "reps must be in 1..=100");
+  Context& c = *ctx_;
+  c.activate();
+  const int wave0 = c.dt.ntt_wave;
+  std::vector<Trial> trials;
+  cudaEvent_t e0, e1;
+  CKG_CUDA(cudaEventCreate(&e0));
+  CKG_CUDA(cudaEventCreate(&e1));
+  try {
+    for (int chunk : kChunks) {
+      set_chunk_items((size_t)chunk);
+      for (int wave : kWaves) {
+        reset();
+        c.dt.ntt_wave = wave;
+        build();
+        CKG_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        issue();
+        cudaError_t err = cudaStreamEndCapture(c.stream, &graph_);
+        if (err != cudaSuccess) throw_cuda(err, "cudaStreamEndCapture");
+        CKG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+        CKG_CUDA(cudaGraphLaunch(exec_, c.stream));
+        CKG_CUDA(cudaEventRecord(e0, c.stream));
+        for (int r = 0; r < reps; ++r) CKG_CUDA(cudaGraphLaunch(exec_, c.stream));
+        CKG_CUDA(cudaEventRecord(e1, c.stream));
+        CKG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        CKG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        trials.push_back({wave, chunk, ms / reps});
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    reset();
+    c.dt.ntt_wave = wave0;
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const Trial* best = &trials[0];
+  for (const Trial& t : trials)
+    if (t.ms < best->ms) best = &t;
+  reset();
+  c.dt.ntt_wave = best->ntt_wave;
+  chunk_items_ = (size_t)best->chunk_items;
+  return trials;
 }
 
 Ct Batch::mul_relin_rescale(const Ct& a, const Ct& b, Evaluator* ev) {  // evaluator.rs:463-510
@@ -155,7 +220,7 @@ void Batch::build() {
   size_t cur = 0;
   for (size_t idx : order) {
     const size_t w = item_words(items_[idx]);
-    if (chunks.empty() || chunks.back().size() >= kChunkItems || (cur + w) * 8 > kChunkScratchBytes) {
+    if (chunks.empty() || chunks.back().size() >= chunk_items_ || (cur + w) * 8 > kChunkScratchBytes) {
       chunks.emplace_back();
       cur = 0;
     }

@@ -31,6 +31,20 @@ class Batch {
   uint64_t key_switches() const;
   size_t size() const { return items_.size(); }
 
+  // Tuning. The chunk size (ops per launch sequence; default 128) applies at the next build
+  // and drops a built batch and its graph. autotune() times every (NTT limb wave, chunk size)
+  // pair of the grid below on this batch's own ops (`reps` graph replays each, after one
+  // warm-up; no OpCounter change), leaves the fastest wave on the context and the fastest chunk
+  // size on the batch (unbuilt), and returns every trial.
+  struct Trial {
+    int ntt_wave;
+    int chunk_items;
+    float ms;
+  };
+  void set_chunk_items(size_t items);
+  size_t chunk_items() const { return chunk_items_; }
+  std::vector<Trial> autotune(int reps);
+
   enum Kind { MUL = 0, ROT = 1, PMUL = 2 };
   // Device working words of one op (its share of the batch scratch) on a level-`level`,
   // `ncomp`-component input.
@@ -50,11 +64,13 @@ class Batch {
   void build();
   void issue();
   void count_ops();
+  void reset();  // drops the graph, work lists and scratch (the ops stay)
 
   Evaluator* ev_;
   Context* ctx_;
   std::vector<Item> items_;
   bool built_ = false;
+  size_t chunk_items_;
   DevBufPtr scratch_;
   DevBufPtr desc_;
   std::vector<Stage*> chunks_;

@@ -548,6 +548,37 @@ int ckg_batch_launch_graph(ckg_batch* b) {
 
 uint64_t ckg_batch_key_switches(const ckg_batch* b) { return b && b->b ? b->b->key_switches() : 0; }
 
+int ckg_ctx_set_ntt_wave(ckg_ctx* ctx, int32_t limbs) {
+  CKG_API_BEGIN
+  if (limbs < 0 || limbs > 65536) throw Error(CKG_INVALID_PARAMS, "NTT wave must be in 0..=65536 limbs");
+  ctx_of(ctx).dt.ntt_wave = limbs;
+  CKG_API_END
+}
+
+int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx) { return ctx && ctx->c ? ctx->c->dt.ntt_wave : -1; }
+
+int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items) {
+  CKG_API_BEGIN
+  if (items < 1) throw Error(CKG_INVALID_PARAMS, "chunk size must be positive");
+  batch_of(b).set_chunk_items((size_t)items);
+  CKG_API_END
+}
+
+int32_t ckg_batch_chunk_items(const ckg_batch* b) { return b && b->b ? (int32_t)b->b->chunk_items() : -1; }
+
+int ckg_batch_autotune(ckg_batch* b, int32_t reps, int32_t* trials, int32_t max_trials, int32_t* n_trials) {
+  CKG_API_BEGIN
+  if (!n_trials || (max_trials > 0 && !trials)) throw Error(CKG_INVALID_PARAMS, "null output");
+  const auto t = batch_of(b).autotune(reps);
+  *n_trials = (int32_t)t.size();
+  for (size_t i = 0; i < t.size() && (int32_t)i < max_trials; ++i) {
+    trials[3 * i] = t[i].ntt_wave;
+    trials[3 * i + 1] = t[i].chunk_items;
+    trials[3 * i + 2] = (int32_t)(t[i].ms * 1000.0f + 0.5f);
+  }
+  CKG_API_END
+}
+
 // ---- bootstrapping ------------------------------------------------------------------------
 
 static BootParams boot_params_of(const uint32_t* bp) {

@@ -1190,8 +1190,14 @@ void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse
   }
 }
 
+// Device lists go in waves of d.ntt_wave limbs: a wave's column pass and row pass run back to
+// back, so the intermediate limbs can stay in L2 between them.
 void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st) {
-  ntt_passes(d, LimbPtrs{count, 0, dev_refs}, count, inverse, st);
+  const int wave = d.ntt_wave > 0 ? d.ntt_wave : count;
+  for (int off = 0; off < count; off += wave) {
+    const int c = std::min(wave, count - off);
+    ntt_passes(d, LimbPtrs{c, 0, dev_refs + off}, c, inverse, st);
+  }
 }
 
 void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st) {
@@ -1272,10 +1278,14 @@ void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const Fi
     launch_finish_ptr(d, dev_fin, count, st);
     return;
   }
-  launch_cols_any(false, LimbPtrs{count, 0, dev_cols}, count, d, 1, st);
-  k_ntt_fwd_rows_finish<FinPtrs><<<dim3((1 << d.log_n) / (kRow * kRowsPerCta), count), 256, 0, st>>>(
-      FinPtrs{count, 0, dev_fin}, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
+  const int wave = d.ntt_wave > 0 ? d.ntt_wave : count;
+  for (int off = 0; off < count; off += wave) {
+    const int c = std::min(wave, count - off);
+    launch_cols_any(false, LimbPtrs{c, 0, dev_cols + off}, c, d, 1, st);
+    k_ntt_fwd_rows_finish<FinPtrs><<<dim3((1 << d.log_n) / (kRow * kRowsPerCta), c), 256, 0, st>>>(
+        FinPtrs{c, 0, dev_fin + off}, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
 }
 
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {

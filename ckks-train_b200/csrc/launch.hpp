@@ -19,6 +19,7 @@ struct DevTables {
   const double* twd_fwd;     // [n_primes][N] the same roots as doubles (FP64 butterflies)
   const double* twd_inv;
   int log_n;
+  int ntt_wave;  // limbs per column + row launch pair of device-list transforms (0: all at once)
 };
 
 void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st);

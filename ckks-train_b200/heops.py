@@ -165,6 +165,13 @@ def _declare(L):
         getattr(L, name).argtypes = [VP]
     L.ckg_batch_key_switches.argtypes = [VP]
     L.ckg_batch_key_switches.restype = C.c_uint64
+    L.ckg_ctx_set_ntt_wave.argtypes = [VP, C.c_int32]
+    L.ckg_ctx_ntt_wave.argtypes = [VP]
+    L.ckg_ctx_ntt_wave.restype = C.c_int32
+    L.ckg_batch_set_chunk_items.argtypes = [VP, C.c_int32]
+    L.ckg_batch_chunk_items.argtypes = [VP]
+    L.ckg_batch_chunk_items.restype = C.c_int32
+    L.ckg_batch_autotune.argtypes = [VP, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
     DP = C.POINTER(C.c_double)
     L.ckg_boot_mul_const.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
     L.ckg_boot_add_const.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
@@ -277,6 +284,15 @@ class Context:
 
     def sync(self):
         _check(lib().ckg_ctx_sync(self.h))
+
+    @property
+    def ntt_wave(self):
+        """Limbs per column + row launch pair of the batched transforms (0: all at once)."""
+        return lib().ckg_ctx_ntt_wave(self.h)
+
+    @ntt_wave.setter
+    def ntt_wave(self, limbs):
+        _check(lib().ckg_ctx_set_ntt_wave(self.h, int(limbs)))
 
     def digit_ranges(self, level):
         """keyswitch::digit_ranges (crates/ckks-train-ckks/src/keyswitch.rs:68-74)."""
@@ -744,6 +760,24 @@ class Batch:
 
     def key_switches(self):
         return lib().ckg_batch_key_switches(self.h)
+
+    @property
+    def chunk_items(self):
+        return lib().ckg_batch_chunk_items(self.h)
+
+    @chunk_items.setter
+    def chunk_items(self, items):
+        _check(lib().ckg_batch_set_chunk_items(self.h, int(items)))
+
+    def autotune(self, reps=3):
+        """Times the (NTT limb wave, chunk size) grid on this batch's ops and keeps the fastest
+        (include/ckg.h, "tuning"). Returns {"ntt_wave", "chunk_items", "trials": [(wave,
+        chunk, ms per replay)]}."""
+        buf = (C.c_int32 * 96)()
+        n = C.c_int32()
+        _check(lib().ckg_batch_autotune(self.h, int(reps), buf, 32, C.byref(n)))
+        trials = [(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2] / 1000.0) for i in range(min(n.value, 32))]
+        return {"ntt_wave": self.ev.ctx.ntt_wave, "chunk_items": self.chunk_items, "trials": trials}
 
 
 SERVER_STATS = ("submitted", "completed", "failed", "cancelled", "batches", "multi_owner_batches",

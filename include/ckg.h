@@ -228,6 +228,22 @@ CKG_API int ckg_batch_capture_graph(ckg_batch* b);
 CKG_API int ckg_batch_launch_graph(ckg_batch* b);
 CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
 
+/* ---- tuning (no reference counterpart) ---------------------------------------------------
+ * Two launch-shape knobs, both bit-neutral (every choice computes the same words):
+ * - the NTT limb wave of a context: device-list transforms run as column + row launch pairs
+ *   over waves of this many limbs, so the intermediate can stay in L2 (0: one pair for all);
+ * - the chunk size of a batch: key-switching ops per launch sequence (default 128).
+ * ckg_batch_autotune times every pair of the grid {0, 32, 64, 128, 256} x {64, 128, 256} on
+ * the batch's own ops (`reps` graph replays each after a warm-up, no OpCounter change), keeps
+ * the fastest: the wave on the context, the chunk size on the batch (rebuilt at its next
+ * run or capture). `trials` receives 3 words per trial (wave, chunk size, microseconds per
+ * replay), at most `max_trials` of them; `n_trials` the count. */
+CKG_API int ckg_ctx_set_ntt_wave(ckg_ctx* ctx, int32_t limbs);
+CKG_API int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx);
+CKG_API int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items);
+CKG_API int32_t ckg_batch_chunk_items(const ckg_batch* b);
+CKG_API int ckg_batch_autotune(ckg_batch* b, int32_t reps, int32_t* trials, int32_t max_trials, int32_t* n_trials);
+
 /* ---- bootstrapping ---------------------------------------------------------------------
  * The device side of the reference's bootstrap (crates/ckks-train-ckks/src/bootstrap/): the
  * BootstrapArithmetic ops (poly.rs:453-486), ModRaise with sparse-secret encapsulation

@@ -41,9 +41,11 @@ def _mix(env, seed, count):
     return ops
 
 
-def _run_mix(env, ops, graph):
+def _run_mix(env, ops, graph, chunk=None, tune=False):
     P, gpu, cpu = env.P, env.gpu, env.cpu
     batch = env.ckg.Batch(gpu)
+    if chunk:
+        batch.chunk_items = chunk
     want, got = [], []
     cpu.reset_counter()
     gpu.reset_counter()
@@ -62,6 +64,12 @@ def _run_mix(env, ops, graph):
             pt = P.random_q(s + 900, level)
             want.append(cpu.rescale(cpu.mul_plain(a_c, pt, env.scale)))
             got.append(batch.mul_plain_rescale(a_g, gpu.upload_pt(pt, env.scale)))
+    if tune:
+        before = gpu.counter()
+        rep = batch.autotune(1)
+        assert gpu.counter() == before, "tuning counted ops"
+        assert len(rep["trials"]) == 15 and rep["ntt_wave"] in (0, 32, 64, 128, 256)
+        assert rep["chunk_items"] in (64, 128, 256) and batch.chunk_items == rep["chunk_items"]
     if graph:
         batch.capture_graph()
         batch.launch_graph()
@@ -115,3 +123,22 @@ def test_batch_errors_before_work(env):
         with pytest.raises(env.ckg.LevelMismatch):
             batch.mul_relin_rescale(a, b)
     assert batch.key_switches() == 0
+
+
+def test_batch_tuning_is_bit_neutral(env):
+    """Every NTT limb wave and chunk size computes the same words; the autotuner counts no ops
+    and leaves its choice on the context and the batch (include/ckg.h, "tuning")."""
+    ops = _mix(env, 17, 40)
+    ctx = env.gpu.ctx
+    wave0 = ctx.ntt_wave
+    try:
+        for wave, chunk in [(0, 128), (8, 3), (32, 7), (1, 1)]:
+            ctx.ntt_wave = wave
+            _run_mix(env, ops, wave % 2 == 0, chunk=chunk)
+        _run_mix(env, ops, True, tune=True)
+        with pytest.raises(env.ckg.InvalidParams):
+            ctx.ntt_wave = -1
+        with pytest.raises(env.ckg.InvalidParams):
+            env.ckg.Batch(env.gpu).chunk_items = 0
+    finally:
+        ctx.ntt_wave = wave0
