@@ -41,5 +41,8 @@ from .heops import (  # noqa: F401
     launch_count,
     lib,
     primes_for_bits,
+    seal_decode,
+    seal_encode,
+    seal_parms_id,
 )
 from . import nn  # noqa: F401,E402

@@ -7,6 +7,7 @@
 #include "../../include/ckg.h"
 #include "bootsetup.hpp"
 #include "handles.hpp"
+#include "seal.hpp"
 
 using namespace ckg;
 
@@ -400,6 +401,10 @@ int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, doub
   check_launch();
   CKG_API_END
 }
+void ckg_pt_info(const ckg_pt* pt, uint32_t* level, double* scale) {
+  if (level) *level = pt->p->level;
+  if (scale) *scale = pt->p->scale;
+}
 ckg_pt* ckg_pt_clone(const ckg_pt* pt) { return new ckg_pt{pt->p}; }
 void ckg_pt_free(ckg_pt* pt) { delete pt; }
 
@@ -576,6 +581,100 @@ int ckg_batch_autotune(ckg_batch* b, int32_t reps, int32_t* trials, int32_t max_
     trials[3 * i + 1] = t[i].chunk_items;
     trials[3 * i + 2] = (int32_t)(t[i].ms * 1000.0f + 0.5f);
   }
+  CKG_API_END
+}
+
+// ---- SEAL wire format -----------------------------------------------------------------------
+
+static uint64_t ring_degree(uint32_t log_n) {
+  if (log_n < 1 || log_n > 17) throw Error(CKG_INVALID_PARAMS, "log_n outside [1, 17]");
+  return 1ULL << log_n;
+}
+
+int ckg_seal_parms_id(uint32_t log_n, const uint64_t* m, uint32_t count, uint64_t out[4]) {
+  CKG_API_BEGIN
+  if (!out || (count && !m)) throw Error(CKG_INVALID_PARAMS, "null argument");
+  const auto id = seal::parms_id(ring_degree(log_n), m, count);
+  memcpy(out, id.data(), 32);
+  CKG_API_END
+}
+
+uint64_t ckg_seal_bytes(uint32_t log_n, uint32_t ncomp, uint32_t level) {
+  if (log_n < 1 || log_n > 17) return 0;
+  return ncomp ? seal::ct_bytes(1ULL << log_n, ncomp, level + 1) : seal::pt_bytes(1ULL << log_n, level + 1);
+}
+
+int ckg_seal_encode(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* words, uint32_t ncomp,
+                    uint32_t level, double scale, uint8_t* out, uint64_t cap, uint64_t* len) {
+  CKG_API_BEGIN
+  const uint64_t n = ring_degree(log_n);
+  if (!q || !words || !len) throw Error(CKG_INVALID_PARAMS, "null argument");
+  if (level >= nq) throw Error(CKG_INVALID_PARAMS, "level above max_level");
+  if (ncomp > 16) throw Error(CKG_INVALID_PARAMS, "a SEAL ciphertext has at most 16 components");
+  *len = ncomp ? seal::ct_bytes(n, ncomp, level + 1) : seal::pt_bytes(n, level + 1);
+  if (!out || cap < *len) throw Error(CKG_INVALID_PARAMS, "output buffer holds " + std::to_string(cap) +
+                                                              " bytes, the object needs " + std::to_string(*len));
+  if (ncomp) seal::encode_ct(n, q, words, ncomp, level, scale, out);
+  else seal::encode_pt(n, q, words, level, scale, out);
+  CKG_API_END
+}
+
+int ckg_seal_decode(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* p, uint32_t np,
+                    const uint8_t* bytes, uint64_t len, int plaintext, uint64_t* words, uint64_t cap,
+                    uint64_t* nwords, uint32_t* ncomp, uint32_t* level, double* scale) {
+  CKG_API_BEGIN
+  const uint64_t n = ring_degree(log_n);
+  if (!q || !nq || (np && !p) || !nwords) throw Error(CKG_INVALID_PARAMS, "null argument");
+  auto r = plaintext ? seal::decode_pt(n, q, nq, p, np, bytes, len) : seal::decode_ct(n, q, nq, p, np, bytes, len);
+  *nwords = r.words.size();
+  if (!words || cap < r.words.size())
+    throw Error(CKG_INVALID_PARAMS, "output buffer holds " + std::to_string(cap) + " words, the object has " +
+                                        std::to_string(r.words.size()));
+  memcpy(words, r.words.data(), r.words.size() * 8);
+  if (ncomp) *ncomp = r.ncomp;
+  if (level) *level = r.level;
+  if (scale) *scale = r.scale;
+  CKG_API_END
+}
+
+static seal::Parsed parse_for(const Context& c, const uint8_t* bytes, uint64_t len, bool plaintext) {
+  const uint64_t* q = c.primes.data();
+  const uint64_t* p = c.primes.data() + c.nq;
+  return plaintext ? seal::decode_pt(c.n, q, c.nq, p, c.k, bytes, len) : seal::decode_ct(c.n, q, c.nq, p, c.k, bytes, len);
+}
+
+int ckg_ct_from_seal(ckg_eval* ev, const uint8_t* bytes, uint64_t len, ckg_ct** out) {
+  CKG_API_BEGIN
+  Evaluator& e = ev_of(ev);
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  auto r = parse_for(*e.ctx(), bytes, len, false);
+  return emit(e.upload(r.words.data(), false, r.ncomp, r.level, r.scale), out);
+  CKG_API_END
+}
+
+int ckg_pt_from_seal(ckg_eval* ev, const uint8_t* bytes, uint64_t len, ckg_pt** out) {
+  CKG_API_BEGIN
+  Evaluator& e = ev_of(ev);
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  auto r = parse_for(*e.ctx(), bytes, len, true);
+  *out = new ckg_pt{e.upload_pt(r.words.data(), false, r.level, r.scale)};
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_ct_to_seal(const ckg_ct* ct, uint8_t* out, uint64_t cap, uint64_t* len) {
+  CKG_API_BEGIN
+  const Ct& c = ct_of(ct);
+  if (!len) throw Error(CKG_INVALID_PARAMS, "null length");
+  const Context& x = *c->ctx;
+  *len = seal::ct_bytes(x.n, c->ncomp, c->level + 1);
+  if (!out || cap < *len) throw Error(CKG_INVALID_PARAMS, "output buffer holds " + std::to_string(cap) +
+                                                              " bytes, the ciphertext needs " + std::to_string(*len));
+  if (c->ncomp > 16) throw Error(CKG_INVALID_PARAMS, "a SEAL ciphertext has at most 16 components");
+  std::vector<uint64_t> words((size_t)c->ncomp * (c->level + 1) * x.n);
+  copy_out(c, words.data(), cudaMemcpyDeviceToHost);
+  CKG_CUDA(cudaStreamSynchronize(x.stream));
+  seal::encode_ct(x.n, x.primes.data(), words.data(), c->ncomp, c->level, c->scale, out);
   CKG_API_END
 }
 

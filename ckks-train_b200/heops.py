@@ -172,6 +172,20 @@ def _declare(L):
     L.ckg_batch_chunk_items.argtypes = [VP]
     L.ckg_batch_chunk_items.restype = C.c_int32
     L.ckg_batch_autotune.argtypes = [VP, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
+    U8P = C.POINTER(C.c_uint8)
+    L.ckg_seal_parms_id.argtypes = [C.c_uint32, U64P, C.c_uint32, U64P]
+    L.ckg_seal_bytes.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+    L.ckg_seal_bytes.restype = C.c_uint64
+    L.ckg_seal_encode.argtypes = [C.c_uint32, U64P, C.c_uint32, U64P, C.c_uint32, C.c_uint32, C.c_double, U8P,
+                                  C.c_uint64, C.POINTER(C.c_uint64)]
+    L.ckg_seal_decode.argtypes = [C.c_uint32, U64P, C.c_uint32, U64P, C.c_uint32, U8P, C.c_uint64, C.c_int, U64P,
+                                  C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_double)]
+    L.ckg_ct_from_seal.argtypes = [VP, U8P, C.c_uint64, C.POINTER(VP)]
+    L.ckg_pt_from_seal.argtypes = [VP, U8P, C.c_uint64, C.POINTER(VP)]
+    L.ckg_ct_to_seal.argtypes = [VP, U8P, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.ckg_pt_info.argtypes = [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]
+    L.ckg_pt_info.restype = None
     DP = C.POINTER(C.c_double)
     L.ckg_boot_mul_const.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
     L.ckg_boot_add_const.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
@@ -571,6 +585,29 @@ class CudaEvaluator:
 
     upload_pt_owned = upload_pt
 
+    def ct_from_seal(self, data):
+        """Parse SEAL 4.1 ciphertext bytes and upload them (load_ciphertext)."""
+        buf, bp = _u8(data)
+        return self._ct(lib().ckg_ct_from_seal, bp, len(buf))
+
+    def pt_from_seal(self, data):
+        """Parse SEAL 4.1 plaintext bytes and upload them (load_plaintext)."""
+        buf, bp = _u8(data)
+        h = VP()
+        _check(lib().ckg_pt_from_seal(self.h, bp, len(buf), C.byref(h)))
+        lv, sc = C.c_uint32(), C.c_double()
+        lib().ckg_pt_info(h, C.byref(lv), C.byref(sc))
+        return Plaintext(self, h, lv.value, sc.value)
+
+    def ct_to_seal(self, ct):
+        """SEAL 4.1 bytes of a device ciphertext (save_ciphertext)."""
+        n, l, _ = ct.info()
+        size = lib().ckg_seal_bytes(self.ctx.log_n, n, l)
+        out = np.zeros(size, np.uint8)
+        ln = C.c_uint64()
+        _check(lib().ckg_ct_to_seal(ct.h, out.ctypes.data_as(C.POINTER(C.c_uint8)), size, C.byref(ln)))
+        return out.tobytes()
+
     def upload_pt_device(self, ptr, level, scale):
         h = VP()
         _check(lib().ckg_pt_upload_device(self.h, VP(ptr), level, scale, C.byref(h)))
@@ -936,6 +973,47 @@ def encode_complex_host(log_n, q, values, scale, level):
     _check(lib().ckg_encode_complex_host(log_n, _p64(qa), len(qa), flat.ctypes.data_as(C.POINTER(C.c_double)),
                                          len(flat) // 2, scale, level, _p64(out)))
     return out
+
+
+def _u8(data):
+    buf = np.frombuffer(bytes(data), np.uint8)
+    return buf, buf.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+def seal_parms_id(log_n, moduli):
+    """SEAL's parms_id of the moduli at ring degree 2^log_n (include/ckg.h, "SEAL 4.1 wire format")."""
+    m = np.ascontiguousarray(moduli, np.uint64)
+    out = np.zeros(4, np.uint64)
+    _check(lib().ckg_seal_parms_id(log_n, _p64(m), len(m), _p64(out)))
+    return [int(x) for x in out]
+
+
+def seal_encode(log_n, q, words, level, scale, plaintext=False):
+    """SEAL 4.1 bytes of NTT-form words over q[0..level] (ncomp x (level+1) x N for a
+    ciphertext, (level+1) x N for a plaintext)."""
+    qa = np.ascontiguousarray(q, np.uint64)
+    w = np.ascontiguousarray(words, np.uint64)
+    ncomp = 0 if plaintext else w.shape[0]
+    n = C.c_uint64()
+    size = lib().ckg_seal_bytes(log_n, ncomp, level)
+    out = np.zeros(size, np.uint8)
+    _check(lib().ckg_seal_encode(log_n, _p64(qa), len(qa), _p64(w), ncomp, level, scale,
+                                 out.ctypes.data_as(C.POINTER(C.c_uint8)), size, C.byref(n)))
+    return out.tobytes()
+
+
+def seal_decode(log_n, q, p, data, plaintext=False):
+    """Parse SEAL 4.1 bytes against the primes: (words, level, scale), words shaped like
+    seal_encode's input. Raises InvalidParams for anything malformed."""
+    qa, pa = np.ascontiguousarray(q, np.uint64), np.ascontiguousarray(p, np.uint64)
+    buf, bp = _u8(data)
+    cap = max(len(buf) // 8, 1)
+    words = np.zeros(cap, np.uint64)
+    nw, nc, lv, sc = C.c_uint64(), C.c_uint32(), C.c_uint32(), C.c_double()
+    _check(lib().ckg_seal_decode(log_n, _p64(qa), len(qa), _p64(pa), len(pa), bp, len(buf), int(plaintext),
+                                 _p64(words), cap, C.byref(nw), C.byref(nc), C.byref(lv), C.byref(sc)))
+    w = words[:nw.value].reshape((-1, lv.value + 1, 1 << log_n))
+    return (w[0] if plaintext else w), lv.value, sc.value
 
 
 def boot_rotation_steps(bp):

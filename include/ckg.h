@@ -176,6 +176,7 @@ CKG_API int ckg_eval_owns(const ckg_eval* ev, const ckg_ct* ct);
 
 CKG_API int ckg_pt_upload(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
 CKG_API int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, double scale, ckg_pt** out);
+CKG_API void ckg_pt_info(const ckg_pt* pt, uint32_t* level, double* scale);
 CKG_API ckg_pt* ckg_pt_clone(const ckg_pt* pt);
 CKG_API void ckg_pt_free(ckg_pt* pt);
 
@@ -243,6 +244,38 @@ CKG_API int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx);
 CKG_API int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items);
 CKG_API int32_t ckg_batch_chunk_items(const ckg_batch* b);
 CKG_API int ckg_batch_autotune(ckg_batch* b, int32_t reps, int32_t* trials, int32_t max_trials, int32_t* n_trials);
+
+/* ---- SEAL 4.1 wire format (crates/ckks-train-ckks/src/seal_compat.rs) ------------------
+ * Ciphertexts and plaintexts serialized as Microsoft SEAL 4.1 writes them with
+ * compr_mode_type::none (layout at seal_compat.rs:11-33): requests that arrive as bytes are
+ * parsed on the host and uploaded, results are written back byte-identical to SEAL's own
+ * save. Interop needs SEAL's parameters (ring degree and primes in SEAL's order, SEAL's last
+ * prime as the single special prime). Reading treats the bytes as untrusted, as
+ * seal_compat.rs:313-455 does: every length is checked against the bytes present, the
+ * parms_id must name a data level of the parameters (not the key level), ciphertexts must be
+ * in NTT form with 2..16 components and correction factor 1, scales positive and finite,
+ * every residue reduced, nothing trailing; compressed and seeded objects are rejected. All
+ * failures are CKG_INVALID_PARAMS with a message.
+ * Functions marked host need no GPU; they take the data primes q[0..nq) and the special
+ * primes p[0..np) of the parameters. */
+/* host: SEAL's parms_id of the moduli m[0..count) at ring degree 2^log_n (seal_compat.rs:86-109). */
+CKG_API int ckg_seal_parms_id(uint32_t log_n, const uint64_t* m, uint32_t count, uint64_t out[4]);
+/* host: serialized length of a ciphertext (ncomp > 0) or a plaintext (ncomp = 0) at `level`. */
+CKG_API uint64_t ckg_seal_bytes(uint32_t log_n, uint32_t ncomp, uint32_t level);
+/* host: serialize NTT-form words (component-major, limb, coefficient) at `level`; `cap` bytes
+ * in `out`, `*len` receives the length (also when `cap` is too small). ncomp = 0: a plaintext. */
+CKG_API int ckg_seal_encode(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* words, uint32_t ncomp,
+                            uint32_t level, double scale, uint8_t* out, uint64_t cap, uint64_t* len);
+/* host: parse a ciphertext (plaintext = 0) or plaintext (plaintext = 1); `cap` words in
+ * `words`, `*nwords` receives the word count (also when `cap` is too small). */
+CKG_API int ckg_seal_decode(uint32_t log_n, const uint64_t* q, uint32_t nq, const uint64_t* p, uint32_t np,
+                            const uint8_t* bytes, uint64_t len, int plaintext, uint64_t* words, uint64_t cap,
+                            uint64_t* nwords, uint32_t* ncomp, uint32_t* level, double* scale);
+/* The same through the device: parse and upload (load_ciphertext / load_plaintext), and
+ * download and serialize (save_ciphertext). */
+CKG_API int ckg_ct_from_seal(ckg_eval* ev, const uint8_t* bytes, uint64_t len, ckg_ct** out);
+CKG_API int ckg_pt_from_seal(ckg_eval* ev, const uint8_t* bytes, uint64_t len, ckg_pt** out);
+CKG_API int ckg_ct_to_seal(const ckg_ct* ct, uint8_t* out, uint64_t cap, uint64_t* len);
 
 /* ---- bootstrapping ---------------------------------------------------------------------
  * The device side of the reference's bootstrap (crates/ckks-train-ckks/src/bootstrap/): the
