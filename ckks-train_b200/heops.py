@@ -670,6 +670,25 @@ class CudaEvaluator:
         _check(lib().ckg_hoisted_rotate(self.h, ct.h, st, len(steps), outs))
         return [Ciphertext(self, VP(outs[i])) for i in range(len(steps))]
 
+    def rotate_many(self, items):
+        """rotate(ct, steps) for independent (ct, steps) pairs, as one batched launch sequence
+        (results and OpCounter those of the single calls)."""
+        if len(items) < 2:
+            return [self.rotate(c, s) for c, s in items]
+        b = Batch(self)
+        outs = [b.rotate(c, s) for c, s in items]
+        b.run()
+        return outs
+
+    def mul_rescale_many(self, pairs):
+        """rescale(mul(a, b)) for independent pairs, as one batched launch sequence."""
+        if len(pairs) < 2:
+            return [self.rescale(self.mul(a, b)) for a, b in pairs]
+        bt = Batch(self)
+        outs = [bt.mul_relin_rescale(a, b) for a, b in pairs]
+        bt.run()
+        return outs
+
     def matvec_plain(self, d, stride, entries, x):
         arr = (VP * len(entries))(*[e.h for e in entries])
         return self._ct(lib().ckg_matvec_plain, d, stride, arr, x.h)

@@ -21,7 +21,10 @@ The evaluator needs: `params()` (with `q`, `n`), `add`, `sub`, `mul`, `mul_lazy`
 `rescale`, `rotate`, `hoisted_rotate`, `mod_switch_to_level`, `mul_plain`, `mul_plain_to_scale`,
 `matvec_enc(d, stride, entries, x)`, `exact_product_scale`, `target_plain_scale`,
 `encode(values, scale, level)`, `has_galois_key`, `has_relin_key`, `owns`; ciphertexts need
-`level()`, `scale()`, `size()`.
+`level()`, `scale()`, `size()`. Where the reference loops over independent ciphertexts (the m
+diagonals of a weight gradient, the transpose's entries), an evaluator that also offers
+`rotate_many` / `mul_rescale_many` (CudaEvaluator: one batched launch sequence) gets each round
+at once; every ciphertext still sees its reference op sequence, so results and counts are the same.
 """
 
 import math
@@ -351,7 +354,9 @@ class EncWeights:
         _check_keys(ev, transpose_rotation_steps(self.d_out, self.d_in, layout))
         plan = zip(transpose_sources(self.d_out, self.d_in, layout),
                    rotations_for_transpose(self.d_out, self.d_in, layout))
-        entries = [self.entries[c] if a == 0 else ev.rotate(self.entries[c], a) for c, a in plan]
+        plan = list(plan)
+        moved = iter(_rotate_all(ev, [(self.entries[c], a) for c, a in plan if a != 0]))
+        entries = [self.entries[c] if a == 0 else next(moved) for c, a in plan]
         return EncWeights(entries, self.d_in, self.d_out, layout)
 
 
@@ -383,21 +388,43 @@ def _first_period_plaintext(ev, layout, period, c, scale, level):
     return ev.encode(mask, scale, level)
 
 
+def _rotate_all(ev, items):
+    """rotate(ct, steps) for every (ct, steps) pair. An evaluator with `rotate_many` runs the
+    independent rotations as one batched launch sequence; the results and counts are those of
+    the single rotations."""
+    if hasattr(ev, "rotate_many"):
+        return ev.rotate_many(items)
+    return [ev.rotate(c, s) for c, s in items]
+
+
+def _mul_rescale_all(ev, pairs):
+    """rescale(mul(a, b)) for every pair, batched where the evaluator offers `mul_rescale_many`."""
+    if hasattr(ev, "mul_rescale_many"):
+        return ev.mul_rescale_many(pairs)
+    return [ev.rescale(ev.mul(a, b)) for a, b in pairs]
+
+
+def _batch_sum_consts_all(ev, vs, masks, target, layout):
+    """_batch_sum_consts for several independent ciphertexts, each rotation round batched over
+    them (every ciphertext sees the op sequence of _batch_sum_consts)."""
+    reduce, replicate = _lane_steps(layout)
+    for s in reduce:
+        rs = _rotate_all(ev, [(v, s) for v in vs])
+        vs = [ev.add(v, r) for v, r in zip(vs, rs)]
+    outs = []
+    for mask in masks:
+        os_ = [ev.rescale(ev.mul_plain_to_scale(v, mask, target)) for v in vs]
+        for s in replicate:
+            rs = _rotate_all(ev, [(o, s) for o in os_])
+            os_ = [ev.add(o, r) for o, r in zip(os_, rs)]
+        outs.append(os_)
+    return outs
+
+
 def _batch_sum_consts(ev, v, masks, target, layout):
     """Reduce (log2 B rotations), per mask a ct-pt product landing on `target` and a rescale,
     then replicate (log2 B rotations) (dense.rs:917-947)."""
-    reduce, replicate = _lane_steps(layout)
-    for s in reduce:
-        r = ev.rotate(v, s)
-        v = ev.add(v, r)
-    outs = []
-    for mask in masks:
-        out = ev.rescale(ev.mul_plain_to_scale(v, mask, target))
-        for s in replicate:
-            r = ev.rotate(out, s)
-            out = ev.add(out, r)
-        outs.append(out)
-    return outs
+    return [out[0] for out in _batch_sum_consts_all(ev, [v], masks, target, layout)]
 
 
 class Dense:
@@ -473,12 +500,9 @@ class Dense:
         a = ev.mod_switch_to_level(a_prev, level)
         a_rot = ev.hoisted_rotate(a, [k2 * b for k2 in range(sh.baby)])
         d_rot = ev.hoisted_rotate(delta, [-(sh.baby * k1 * b) for k1 in range(sh.giant)])
-        entries = [[] for _ in cs]
-        for e in range(sh.m):
-            p = ev.rescale(ev.mul(d_rot[e // sh.baby], a_rot[e % sh.baby]))
-            for out, value in zip(entries, _batch_sum_consts(ev, p, masks, target, layout)):
-                out.append(value)
-        return entries
+        # the m diagonals are independent: each takes dense.rs's sequence, the rounds batched
+        ps = _mul_rescale_all(ev, [(d_rot[e // sh.baby], a_rot[e % sh.baby]) for e in range(sh.m)])
+        return _batch_sum_consts_all(ev, ps, masks, target, layout)
 
     def bias_grad_scaled(self, ev, delta, layout, c):
         """c sum_b delta_b in canonical form at exactly the bias scale, one level below delta
