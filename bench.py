@@ -1005,18 +1005,21 @@ def main():
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
     roof = ntt_roofline(torch, S, peaks)
     roof_stream = stream_roofline(rank_stream(rank, args.ops), S.n, S.ctx.k, S.ctx.alpha, ms / args.steps, peaks)
+    # The bootstrap, training-step and serving figures are single-GPU measurements: a run on N > 1
+    # GPUs (one replica per rank) reports the batched stream only.
+    single = world == 1
     boot = None
-    if not args.no_boot:
+    if not args.no_boot and single:
         mix.batch = None
         boot = BootBench(ckg, torch, local).measure()
     mlp_step = None
-    if not args.no_mlp:
+    if not args.no_mlp and single:
         mix.batch = None
         mb = MlpBench(ckg, torch, local)
         mlp_step = mb.measure()
         del mb
     serving = serving_spill = None
-    if not args.no_serve:
+    if not args.no_serve and single:
         mix.batch = None
         sv = BootServing(ckg, torch, local)
         serving = sv.measure(args.serve_requests)
