@@ -86,6 +86,13 @@ int ckg_ctx_sync(ckg_ctx* ctx) {
   Context& c = ctx_of(ctx);
   c.activate();
   CKG_CUDA(cudaStreamSynchronize(c.stream));
+  c.sync_transfers();
+  CKG_API_END
+}
+
+int ckg_ctx_join_transfers(ckg_ctx* ctx) {
+  CKG_API_BEGIN
+  ctx_of(ctx).join_transfers();
   CKG_API_END
 }
 
@@ -401,6 +408,31 @@ int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, doub
   check_launch();
   CKG_API_END
 }
+int ckg_ct_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t ncomp, uint32_t level, double scale,
+                          ckg_ct** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  return emit(ev_of(ev).upload_overlapped(host, ncomp, level, scale), out);
+  CKG_API_END
+}
+
+int ckg_pt_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  *out = new ckg_pt{ev_of(ev).upload_pt_overlapped(host, level, scale)};
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_ct_download_overlap(const ckg_ct* ct, uint64_t* host) {
+  CKG_API_BEGIN
+  const Ct& c = ct_of(ct);
+  if (!host) throw Error(CKG_INVALID_PARAMS, "null host buffer");
+  const size_t words = (size_t)(c->level + 1) * c->ctx->n;
+  c->ctx->download_overlapped(c->buf, c->comp(0), words, c->comp_stride, c->ncomp, host);
+  CKG_API_END
+}
+
 void ckg_pt_info(const ckg_pt* pt, uint32_t* level, double* scale) {
   if (level) *level = pt->p->level;
   if (scale) *scale = pt->p->scale;

@@ -27,12 +27,92 @@ DevBuf::~DevBuf() {
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
+  for (cudaEvent_t e : waits) {
+    cudaStreamWaitEvent(sres->s, e, 0);
+    cudaEventDestroy(e);
+  }
   if (pooled) cudaFreeAsync(p, sres->s);
   else cudaFree(p);
   if (cur != device) cudaSetDevice(cur);
 }
 
 void Context::activate() const { CKG_CUDA(cudaSetDevice(device)); }
+
+void Context::transfer_streams() {
+  for (StreamPtr* sp : {&xfer_in, &xfer_out}) {
+    if (*sp) continue;
+    auto r = std::make_shared<StreamRes>();
+    r->device = device;
+    CKG_CUDA(cudaStreamCreateWithFlags(&r->s, cudaStreamNonBlocking));
+    r->own = true;
+    *sp = r;
+  }
+}
+
+namespace {
+// `to` waits for the work queued on `from` so far.
+void stream_after(cudaStream_t to, cudaStream_t from) {
+  cudaEvent_t e;
+  CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaError_t err = cudaEventRecord(e, from);
+  if (err == cudaSuccess) err = cudaStreamWaitEvent(to, e, 0);
+  cudaEventDestroy(e);
+  if (err != cudaSuccess) throw_cuda(err, "cudaStreamWaitEvent");
+}
+}  // namespace
+
+DevBufPtr Context::upload_overlapped(const uint64_t* host, size_t words) {
+  activate();
+  transfer_streams();
+  auto b = std::make_shared<DevBuf>();
+  b->sres = sres;  // freed in compute order, after every use there
+  b->device = device;
+  b->words = words;
+  if (!words) return b;
+  CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, xfer_in->s));
+  CKG_CUDA(cudaMemcpyAsync(b->p, host, words * 8, cudaMemcpyHostToDevice, xfer_in->s));
+  stream_after(stream, xfer_in->s);
+  return b;
+}
+
+void Context::download_overlapped(const DevBufPtr& buf, const uint64_t* dev, size_t row_words, size_t pitch_words,
+                                  size_t rows, uint64_t* host) {
+  activate();
+  transfer_streams();
+  stream_after(xfer_out->s, stream);  // the data is final once the compute stream gets here
+  if (pitch_words == row_words)
+    CKG_CUDA(cudaMemcpyAsync(host, dev, rows * row_words * 8, cudaMemcpyDeviceToHost, xfer_out->s));
+  else
+    CKG_CUDA(cudaMemcpy2DAsync(host, row_words * 8, dev, pitch_words * 8, row_words * 8, rows,
+                               cudaMemcpyDeviceToHost, xfer_out->s));
+  // the buffer's free waits for this copy; finished earlier copies are dropped from the list
+  auto& w = buf->waits;
+  for (size_t i = 0; i < w.size();) {
+    if (cudaEventQuery(w[i]) == cudaSuccess) {
+      cudaEventDestroy(w[i]);
+      w[i] = w.back();
+      w.pop_back();
+    } else {
+      ++i;
+    }
+  }
+  cudaEvent_t e;
+  CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CKG_CUDA(cudaEventRecord(e, xfer_out->s));
+  w.push_back(e);
+}
+
+void Context::join_transfers() {
+  activate();
+  if (xfer_in) stream_after(stream, xfer_in->s);
+  if (xfer_out) stream_after(stream, xfer_out->s);
+}
+
+void Context::sync_transfers() {
+  activate();
+  if (xfer_in) CKG_CUDA(cudaStreamSynchronize(xfer_in->s));
+  if (xfer_out) CKG_CUDA(cudaStreamSynchronize(xfer_out->s));
+}
 
 DevBufPtr Context::alloc(size_t words) {
   auto b = std::make_shared<DevBuf>();

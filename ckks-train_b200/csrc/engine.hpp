@@ -63,6 +63,9 @@ struct DevBuf {
   uint64_t* p = nullptr;
   size_t words = 0;
   StreamPtr sres;
+  // Copies still reading the buffer on other streams (overlapped downloads): the free on
+  // `sres` waits for them.
+  std::vector<cudaEvent_t> waits;
   int device = 0;
   bool pooled = true;
   DevBuf() = default;
@@ -121,6 +124,17 @@ struct Context {
   uint64_t* d_xhalf = nullptr;
   DevBufPtr alloc(size_t words);                            // stream-ordered, on `stream`
   void activate() const;                                    // makes `device` current
+
+  // Overlapped host transfers: an upload stream and a download stream beside `stream`
+  // (created on first use). Buffers they fill are allocated on the upload stream and freed on
+  // `stream`, which waits for the copy before its first use.
+  StreamPtr xfer_in, xfer_out;
+  void transfer_streams();
+  DevBufPtr upload_overlapped(const uint64_t* host, size_t words);
+  void download_overlapped(const DevBufPtr& buf, const uint64_t* dev, size_t row_words, size_t pitch_words,
+                           size_t rows, uint64_t* host);
+  void join_transfers();  // `stream` waits for every transfer queued so far
+  void sync_transfers();  // the host waits for them
 };
 
 // ---- polynomial-level algorithms (all asynchronous on ctx.stream) -------------------

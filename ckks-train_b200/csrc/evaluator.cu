@@ -92,6 +92,32 @@ Ct Evaluator::upload(const uint64_t* src, bool device_src, uint32_t ncomp, uint3
   return c;
 }
 
+Ct Evaluator::upload_overlapped(const uint64_t* host, uint32_t ncomp, uint32_t level, double scale) {
+  if (ncomp < 2) throw Error(ST_INVALID_PARAMS, "a ciphertext needs at least 2 components");
+  if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+  if (!host) throw Error(ST_INVALID_PARAMS, "null host buffer");
+  check_ct_scale(scale);
+  auto c = std::make_shared<CtObj>();
+  c->ctx = ctx_;
+  c->ncomp = ncomp;
+  c->level = level;
+  c->scale = scale;
+  c->comp_stride = (size_t)(level + 1) * ctx_->n;
+  c->buf = ctx_->upload_overlapped(host, ncomp * c->comp_stride);
+  return c;
+}
+
+Pt Evaluator::upload_pt_overlapped(const uint64_t* host, uint32_t level, double scale) {
+  if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+  if (!host) throw Error(ST_INVALID_PARAMS, "null host buffer");
+  auto p = std::make_shared<PtObj>();
+  p->ctx = ctx_;
+  p->level = level;
+  p->scale = scale;
+  p->buf = ctx_->upload_overlapped(host, (size_t)(level + 1) * ctx_->n);
+  return p;
+}
+
 Pt Evaluator::upload_pt(const uint64_t* src, bool device_src, uint32_t level, double scale) {
   if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
   ctx_->activate();

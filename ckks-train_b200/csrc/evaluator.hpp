@@ -90,6 +90,9 @@ class Evaluator {
 
   Ct upload(const uint64_t* src, bool device_src, uint32_t ncomp, uint32_t level, double scale);
   Pt upload_pt(const uint64_t* src, bool device_src, uint32_t level, double scale);
+  // The same from host memory on the context's upload stream (Context::upload_overlapped).
+  Ct upload_overlapped(const uint64_t* host, uint32_t ncomp, uint32_t level, double scale);
+  Pt upload_pt_overlapped(const uint64_t* host, uint32_t level, double scale);
 
   Ct add(const Ct& a, const Ct& b) { return add_sub(a, b, false); }
   Ct sub(const Ct& a, const Ct& b) { return add_sub(a, b, true); }

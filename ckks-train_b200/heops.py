@@ -186,6 +186,10 @@ def _declare(L):
     L.ckg_ct_to_seal.argtypes = [VP, U8P, C.c_uint64, C.POINTER(C.c_uint64)]
     L.ckg_pt_info.argtypes = [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_double)]
     L.ckg_pt_info.restype = None
+    L.ckg_ct_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_pt_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
+    L.ckg_ct_download_overlap.argtypes = [VP, VP]
+    L.ckg_ctx_join_transfers.argtypes = [VP]
     DP = C.POINTER(C.c_double)
     L.ckg_boot_mul_const.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
     L.ckg_boot_add_const.argtypes = [VP, VP, C.c_double, C.POINTER(VP)]
@@ -298,6 +302,10 @@ class Context:
 
     def sync(self):
         _check(lib().ckg_ctx_sync(self.h))
+
+    def join_transfers(self):
+        """The context's stream waits for every overlapped transfer queued so far."""
+        _check(lib().ckg_ctx_join_transfers(self.h))
 
     @property
     def ntt_wave(self):
@@ -572,6 +580,23 @@ class CudaEvaluator:
         h = VP()
         _check(lib().ckg_pt_upload(self.h, C.cast(VP(ptr), U64P), level, scale, C.byref(h)))
         return Plaintext(self, h, level, scale)
+
+    def upload_ct_overlap(self, ptr, ncomp, level, scale):
+        """upload_ct from a pinned host address on the context's upload stream (include/ckg.h,
+        "overlapped host transfers")."""
+        h = VP()
+        _check(lib().ckg_ct_upload_overlap(self.h, C.cast(VP(ptr), U64P), ncomp, level, scale, C.byref(h)))
+        return Ciphertext(self, h)
+
+    def upload_pt_overlap(self, ptr, level, scale):
+        h = VP()
+        _check(lib().ckg_pt_upload_overlap(self.h, C.cast(VP(ptr), U64P), level, scale, C.byref(h)))
+        return Plaintext(self, h, level, scale)
+
+    def download_ct_overlap(self, ct, ptr):
+        """Queues the copy of `ct` to the pinned host address `ptr` on the download stream;
+        complete after ctx.sync()."""
+        _check(lib().ckg_ct_download_overlap(ct.h, VP(ptr)))
 
     def download_ct_async(self, ct, ptr):
         """Queues the copy of `ct` to the host address `ptr`; complete after ctx.sync()."""

@@ -177,6 +177,21 @@ CKG_API int ckg_eval_owns(const ckg_eval* ev, const ckg_ct* ct);
 CKG_API int ckg_pt_upload(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
 CKG_API int ckg_pt_upload_device(ckg_eval* ev, const uint64_t* dev, uint32_t level, double scale, ckg_pt** out);
 CKG_API void ckg_pt_info(const ckg_pt* pt, uint32_t* level, double* scale);
+
+/* Overlapped host transfers (no reference counterpart). The same uploads and downloads on two
+ * transfer streams of the context, so the uploads of the next batch, the compute of this one
+ * and the downloads of the last one run at once, both PCIe directions included. Host memory
+ * should be pinned (else the copies are staged and do not overlap) and must stay untouched
+ * until its copy completes. Work queued on the context after an upload waits for that upload;
+ * a download copies the ciphertext as queued work leaves it, and the ciphertext's memory is
+ * not reused before the copy ends, even if its handle is freed at once.
+ * ckg_ctx_join_transfers makes the context's stream wait for every transfer queued so far
+ * (record a completion event after it); ckg_ctx_sync also waits for them on the host. */
+CKG_API int ckg_ct_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t ncomp, uint32_t level, double scale,
+                                  ckg_ct** out);
+CKG_API int ckg_pt_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
+CKG_API int ckg_ct_download_overlap(const ckg_ct* ct, uint64_t* host);
+CKG_API int ckg_ctx_join_transfers(ckg_ctx* ctx);
 CKG_API ckg_pt* ckg_pt_clone(const ckg_pt* pt);
 CKG_API void ckg_pt_free(ckg_pt* pt);
 

@@ -1,0 +1,74 @@
+"""Overlapped host transfers (include/ckg.h, "overlapped host transfers"): uploads on the
+context's upload stream, downloads on its download stream. Results equal the plain uploads and
+downloads and the oracle's, work queued after an upload sees its data, and a ciphertext whose
+handle is freed right after its download is not overwritten before the copy ends."""
+
+import numpy as np
+import pytest
+
+from gpu_util import assert_same, random_ct, torch_dev
+from test_gpu_eval import Env
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env(ckg, oracle):
+    return Env(ckg, oracle, "small", [1, 2])
+
+
+def _pinned(arr):
+    torch = torch_dev()
+    return torch.from_numpy(np.ascontiguousarray(arr, np.uint64).view(np.int64)).pin_memory()
+
+
+def _empty_pinned(shape):
+    torch = torch_dev()
+    return torch.empty(shape, dtype=torch.int64).pin_memory()
+
+
+def test_overlapped_batch_matches_oracle(env):
+    ckg, P, gpu, cpu = env.ckg, env.P, env.gpu, env.cpu
+    L = P.max_level
+    ins = [random_ct(P, 10 + i, L) for i in range(6)]
+    host_in = [_pinned(a) for a in ins]
+    pt = P.random_q(77, L)
+    host_pt = _pinned(pt)
+    outs_host = [_empty_pinned((2, L, P.n)), _empty_pinned((2, L + 1, P.n)), _empty_pinned((2, L, P.n))]
+    for step in range(3):  # the same host buffers every step, as a pipelined client would use them
+        g = [gpu.upload_ct_overlap(h.data_ptr(), 2, L, env.scale) for h in host_in]
+        gp = gpu.upload_pt_overlap(host_pt.data_ptr(), L, env.scale)
+        b = ckg.Batch(gpu)
+        res = [b.mul_relin_rescale(g[0], g[1]), b.rotate(g[2], 1), b.mul_plain_rescale(g[3], gp)]
+        b.run()
+        for r, h in zip(res, outs_host):
+            gpu.download_ct_overlap(r, h.data_ptr())
+        del res, g, b  # handles go at once: the copies still read the right memory
+    env.ctx.sync()
+    c = [cpu.ct(a, env.scale) for a in ins]
+    want = [cpu.rescale(cpu.mul(c[0], c[1])), cpu.rotate(c[2], 1), cpu.rescale(cpu.mul_plain(c[3], pt, env.scale))]
+    for w, h, what in zip(want, outs_host, ("mul", "rotate", "mul_plain")):
+        assert_same(h.numpy().view(np.uint64), w.data(), what)
+
+
+def test_freed_handles_are_not_overwritten_early(env):
+    """A result downloaded and dropped at once, then much more work allocating and writing
+    device memory: the host copy still holds the result."""
+    ckg, P, gpu = env.ckg, env.P, env.gpu
+    L = P.max_level
+    a = random_ct(P, 5, L)
+    host = _empty_pinned((2, L + 1, P.n))
+    ga = gpu.upload_ct(a, env.scale)
+    r = gpu.rotate(ga, 2)
+    want = gpu.download_ct(r)[0]
+    gpu.download_ct_overlap(r, host.data_ptr())
+    del r
+    junk = [gpu.rotate(gpu.upload_ct(random_ct(P, 100 + i, L), env.scale), 1) for i in range(8)]
+    env.ctx.join_transfers()
+    env.ctx.sync()
+    assert_same(host.numpy().view(np.uint64), want, "overlapped download")
+    assert len(junk) == 8
+    with pytest.raises(ckg.InvalidParams):
+        gpu.upload_ct_overlap(0, 2, L, env.scale)
+    with pytest.raises(ckg.InvalidParams):
+        gpu.upload_ct_overlap(host.data_ptr(), 1, L, env.scale)
