@@ -861,48 +861,80 @@ CKG_DEV uint64_t ip_finish_f64(uint64_t S, double A, uint64_t q, double q_d, dou
 // ------------------------------------------------------------------------------------
 // Key-switch inner product (crates/ckks-train-ckks/src/keyswitch.rs:230-309): for every
 // limb i of Q_l * P, out_b = sum_j d_j * b_j and out_a = sum_j d_j * a_j, accumulated
-// exactly in 128 bits and reduced once. Digit j's limb i is the input polynomial's limb
-// when prime i belongs to digit j, else the converted limb; with a Galois permutation
-// every digit word is read at perm[c] (hoisted rotation).
+// exactly and reduced once. Digit j's limb i is the input polynomial's limb when prime i
+// belongs to digit j, else the converted limb; with a Galois permutation every digit word is
+// read at perm[c] (hoisted rotation). Each thread computes two adjacent coefficients (c, c + 1)
+// with 16-byte loads and stores, so the job, limb and digit addressing is shared by both; a job
+// whose buffers are not all 16-byte aligned (the input may be a caller's pointer) reads and
+// writes the pair as two words.
 // ------------------------------------------------------------------------------------
 
+CKG_DEV bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+CKG_DEV ulonglong2 ld_pair(const uint64_t* p, bool vec) {
+  return vec ? __ldg(reinterpret_cast<const ulonglong2*>(p)) : make_ulonglong2(__ldg(p), __ldg(p + 1));
+}
+CKG_DEV ulonglong2 ldcs_pair(const uint64_t* p, bool vec) {
+  return vec ? __ldcs(reinterpret_cast<const ulonglong2*>(p)) : make_ulonglong2(__ldcs(p), __ldcs(p + 1));
+}
+CKG_DEV void st_pair(uint64_t* p, uint64_t x, uint64_t y, bool vec) {
+  if (vec) {
+    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(x, y);
+  } else {
+    p[0] = x;
+    p[1] = y;
+  }
+}
+
 template <class B>
-__global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 8 : 1)
+__global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 4 : 1)
     k_inner_product(const __grid_constant__ B ib, const PrimeConst* __restrict__ pc, int log_n) {
   const int n = 1 << log_n;
-  // By-value lists: grid (coefficient blocks, limbs, jobs). Device-resident lists (the
-  // batched path, jobs sorted by key): grid (jobs, coefficient blocks, limbs), so the jobs
+  // By-value lists: grid (coefficient-pair blocks, limbs, jobs). Device-resident lists (the
+  // batched path, jobs sorted by key): grid (jobs, coefficient-pair blocks, limbs), so the jobs
   // that share a key read the same key block back to back and it is served from L2.
   constexpr bool kJobFast = std::is_same<B, IpPtrs>::value;
   const IpJob& job = ib.j[kJobFast ? blockIdx.x : blockIdx.z];
   const int i = kJobFast ? blockIdx.z : blockIdx.y;  // limb of Q_l * P: 0..l data, l+1..l+k special
-  const int c = (kJobFast ? blockIdx.y : blockIdx.x) * blockDim.x + threadIdx.x;
+  const int c = 2 * ((kJobFast ? blockIdx.y : blockIdx.x) * blockDim.x + threadIdx.x);
   const int l = job.level;
   if (c >= n || i > l + ib.k) return;
   const bool is_q = i <= l;
   const uint32_t prime = is_q ? i : (ib.L + 1) + (i - l - 1);
   const int key_limb = is_q ? i : job.key_q + (i - l - 1);
   const size_t key_limbs = (size_t)(job.key_q + ib.k);
-  const uint32_t src_c = job.perm ? __ldg(job.perm + c) : (uint32_t)c;
+  const bool gather = job.perm != nullptr;
+  uint32_t s0 = (uint32_t)c, s1 = (uint32_t)c + 1;
+  if (gather) {
+    s0 = __ldg(job.perm + c);
+    s1 = __ldg(job.perm + c + 1);
+  }
+  const bool vin = !gather && aligned16(job.in);
+  const bool vkey = aligned16(job.key);
+  const bool vout = aligned16(job.out_b) && aligned16(job.out_a);
   // By-value lists (one op's jobs) load the words of up to 4 digits before their products so
   // the loads overlap; the batched grid, whose many resident jobs already keep loads in
   // flight, keeps one digit per step (measured faster there).
   constexpr int kChunk = kJobFast ? 1 : 4;
-  auto load = [&](int j0, uint64_t* dv, uint64_t* kbv, uint64_t* kav) {
+  auto load = [&](int j0, ulonglong2* dv, ulonglong2* kbv, ulonglong2* kav) {
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       const int j = j0 + u;
       if (j < job.ndig) {
         const int start = j * ib.alpha;
         const int end = min(start + ib.alpha, l + 1);
+        const uint64_t* base;
+        bool vec;
         if (is_q && i >= start && i < end) {
-          dv[u] = __ldg(job.in + ((size_t)i << log_n) + src_c);
+          base = job.in + ((size_t)i << log_n);
+          vec = vin;
         } else {
           const int t = i < start ? i : i - (end - start);
-          dv[u] = __ldg(job.conv[j] + ((size_t)t << log_n) + src_c);
+          base = job.conv[j] + ((size_t)t << log_n);
+          vec = !gather && aligned16(job.conv[j]);
         }
-        kbv[u] = __ldcs(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c);
-        kav[u] = __ldcs(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c);
+        dv[u] = gather ? make_ulonglong2(__ldg(base + s0), __ldg(base + s1)) : ld_pair(base + c, vec);
+        kbv[u] = ldcs_pair(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c, vkey);
+        kav[u] = ldcs_pair(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c, vkey);
       }
     }
   };
@@ -914,60 +946,72 @@ __global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 8 : 1)
     // delta < ip_off of the quotient, so x = S - rint(A) q + ip_off q lies in [0, 2^53); a
     // second rounded quotient of x (exact in f64) brings it into (-q, q), one add into [0, q).
     const double q_d = P.qd, qinv = P.qinv;
-    uint64_t Sb = 0, Sa = 0;
-    double Ab = 0.0, Aa = 0.0;
+    uint64_t Sb0 = 0, Sa0 = 0, Sb1 = 0, Sa1 = 0;
+    double Ab0 = 0.0, Aa0 = 0.0, Ab1 = 0.0, Aa1 = 0.0;
     for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
-      uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+      ulonglong2 dv[kChunk], kbv[kChunk], kav[kChunk];
       load(j0, dv, kbv, kav);
 #pragma unroll
       for (int u = 0; u < kChunk; ++u) {
         if (j0 + u >= job.ndig) break;
-        const uint64_t d = dv[u], kb = kbv[u], ka = kav[u];
-        Sb += d * kb;
-        Sa += d * ka;
-        const double dd = f64_small(d);
-        Ab = __fma_rn(dd, __dmul_rn(f64_small(kb), qinv), Ab);
-        Aa = __fma_rn(dd, __dmul_rn(f64_small(ka), qinv), Aa);
+        const ulonglong2 d = dv[u], kb = kbv[u], ka = kav[u];
+        Sb0 += d.x * kb.x;
+        Sa0 += d.x * ka.x;
+        Sb1 += d.y * kb.y;
+        Sa1 += d.y * ka.y;
+        const double dd0 = f64_small(d.x), dd1 = f64_small(d.y);
+        Ab0 = __fma_rn(dd0, __dmul_rn(f64_small(kb.x), qinv), Ab0);
+        Aa0 = __fma_rn(dd0, __dmul_rn(f64_small(ka.x), qinv), Aa0);
+        Ab1 = __fma_rn(dd1, __dmul_rn(f64_small(kb.y), qinv), Ab1);
+        Aa1 = __fma_rn(dd1, __dmul_rn(f64_small(ka.y), qinv), Aa1);
       }
     }
     const uint64_t q = P.q, base = (uint64_t)P.ip_off * q;
-    job.out_b[o] = ip_finish_f64(Sb, Ab, q, q_d, qinv, base);
-    job.out_a[o] = ip_finish_f64(Sa, Aa, q, q_d, qinv, base);
+    st_pair(job.out_b + o, ip_finish_f64(Sb0, Ab0, q, q_d, qinv, base), ip_finish_f64(Sb1, Ab1, q, q_d, qinv, base),
+            vout);
+    st_pair(job.out_a + o, ip_finish_f64(Sa0, Aa0, q, q_d, qinv, base), ip_finish_f64(Sa1, Aa1, q, q_d, qinv, base),
+            vout);
     return;
   }
   // 30-bit halves: four 64-bit accumulators per output, each < 16 * 2^60 (at most 16 digits).
-  uint64_t Ab = 0, B1b = 0, B2b = 0, Cb = 0, Aa = 0, B1a = 0, B2a = 0, Ca = 0;
+  uint64_t acc[2][2][4] = {};  // [coefficient][b, a][lo*lo, lo*hi, hi*lo, hi*hi]
   for (int j0 = 0; j0 < job.ndig; j0 += kChunk) {
-    uint64_t dv[kChunk], kbv[kChunk], kav[kChunk];
+    ulonglong2 dv[kChunk], kbv[kChunk], kav[kChunk];
     load(j0, dv, kbv, kav);
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       if (j0 + u >= job.ndig) break;
-      const uint64_t d = dv[u], kb = kbv[u], ka = kav[u];
-      const uint32_t dl = (uint32_t)(d & kMask30), dh = (uint32_t)(d >> 30);
-      const uint32_t bl = (uint32_t)(kb & kMask30), bh = (uint32_t)(kb >> 30);
-      const uint32_t al = (uint32_t)(ka & kMask30), ah = (uint32_t)(ka >> 30);
-      Ab += (uint64_t)dl * bl;
-      B1b += (uint64_t)dl * bh;
-      B2b += (uint64_t)dh * bl;
-      Cb += (uint64_t)dh * bh;
-      Aa += (uint64_t)dl * al;
-      B1a += (uint64_t)dl * ah;
-      B2a += (uint64_t)dh * al;
-      Ca += (uint64_t)dh * ah;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const uint64_t d = e ? dv[u].y : dv[u].x, kb = e ? kbv[u].y : kbv[u].x, ka = e ? kav[u].y : kav[u].x;
+        const uint32_t dl = (uint32_t)(d & kMask30), dh = (uint32_t)(d >> 30);
+        const uint32_t bl = (uint32_t)(kb & kMask30), bh = (uint32_t)(kb >> 30);
+        const uint32_t al = (uint32_t)(ka & kMask30), ah = (uint32_t)(ka >> 30);
+        acc[e][0][0] += (uint64_t)dl * bl;
+        acc[e][0][1] += (uint64_t)dl * bh;
+        acc[e][0][2] += (uint64_t)dh * bl;
+        acc[e][0][3] += (uint64_t)dh * bh;
+        acc[e][1][0] += (uint64_t)dl * al;
+        acc[e][1][1] += (uint64_t)dl * ah;
+        acc[e][1][2] += (uint64_t)dh * al;
+        acc[e][1][3] += (uint64_t)dh * ah;
+      }
     }
   }
-  uint64_t lo = Ab, hi = 0;
-  add128(hi, lo, B1b >> 34, B1b << 30);
-  add128(hi, lo, B2b >> 34, B2b << 30);
-  add128(hi, lo, Cb >> 4, Cb << 60);
-  job.out_b[o] = reduce128(hi, lo, P);
-  lo = Aa;
-  hi = 0;
-  add128(hi, lo, B1a >> 34, B1a << 30);
-  add128(hi, lo, B2a >> 34, B2a << 30);
-  add128(hi, lo, Ca >> 4, Ca << 60);
-  job.out_a[o] = reduce128(hi, lo, P);
+  uint64_t r[2][2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e)
+#pragma unroll
+    for (int ba = 0; ba < 2; ++ba) {
+      const uint64_t* a = acc[e][ba];
+      uint64_t lo = a[0], hi = 0;
+      add128(hi, lo, a[1] >> 34, a[1] << 30);
+      add128(hi, lo, a[2] >> 34, a[2] << 30);
+      add128(hi, lo, a[3] >> 4, a[3] << 60);
+      r[e][ba] = reduce128(hi, lo, P);
+    }
+  st_pair(job.out_b + o, r[0][0], r[1][0], vout);
+  st_pair(job.out_a + o, r[0][1], r[1][1], vout);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1231,7 +1275,7 @@ void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJ
       ib.j[i] = jobs[off + i];
       max_limbs = std::max(max_limbs, jobs[off + i].level + 1 + k);
     }
-    k_inner_product<IpBatch><<<dim3((n + 255) / 256, max_limbs, ib.count), 256, 0, st>>>(ib, d.prime, d.log_n);
+    k_inner_product<IpBatch><<<dim3((n / 2 + 255) / 256, max_limbs, ib.count), 256, 0, st>>>(ib, d.prime, d.log_n);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
 }
@@ -1240,7 +1284,7 @@ void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const
                               int max_limbs, cudaStream_t st) {
   if (!count) return;
   const int n = 1 << d.log_n;
-  k_inner_product<IpPtrs><<<dim3(count, (n + 255) / 256, max_limbs), 256, 0, st>>>(IpPtrs{count, alpha, L, k, dev_jobs},
+  k_inner_product<IpPtrs><<<dim3(count, (n / 2 + 255) / 256, max_limbs), 256, 0, st>>>(IpPtrs{count, alpha, L, k, dev_jobs},
                                                                                   d.prime, d.log_n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }

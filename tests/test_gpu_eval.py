@@ -69,6 +69,26 @@ def test_key_switch_raw(env):
         assert_same(from_dev(oa), wa, f"key_switch a level {level}")
 
 
+def test_key_switch_raw_unaligned(env):
+    """Caller buffers one word off a 16-byte boundary (tensor slices at odd offsets): the input's
+    own-digit limbs take the word-pair loads of the inner product, and the outputs are written
+    at odd word offsets, with the aligned call's result."""
+    P, ctx = env.P, env.ctx
+    level = P.max_level
+    d = P.random_q(900, level)
+    n_words = d.size
+    dd = to_dev(np.concatenate([np.zeros(1, np.uint64), d.ravel()]))
+    out = empty_dev((2 * n_words + 4,))
+    assert ptr(dd) % 16 == 0 and ptr(out) % 16 == 0
+    ob, oa = ptr(out) + 8, ptr(out) + 8 * (n_words + 3)
+    ctx.key_switch(env.d_rk, ptr(dd) + 8, level, ob, oa)
+    ctx.sync()
+    got = from_dev(out)
+    wb, wa = env.rk.key_switch(d)
+    assert_same(got[1:1 + n_words].reshape(d.shape), wb, "unaligned key_switch b")
+    assert_same(got[n_words + 3:2 * n_words + 3].reshape(d.shape), wa, "unaligned key_switch a")
+
+
 def test_arithmetic_ops(env):
     P = env.P
     L = P.max_level
