@@ -406,6 +406,16 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
+// 8-byte asynchronous global -> shared copy (cp.async, no register staging) and the wait for
+// all of this thread's copies.
+CKG_DEV void cp_async8(void* smem, const void* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+CKG_DEV void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Inverse row pass with FP64 butterflies: canonical input, raw doubles out.
 CKG_DEV void inv_rows_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, int log_n,
                                uint64_t* sm) {
@@ -416,6 +426,21 @@ CKG_DEV void inv_rows_body_f64(const LimbRef& ref, const PrimeConst* P, const do
   double x[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) x[j] = f64_of(srow[pad_idx(16 * t + j)]);
+  // The row's words are in registers: its shared-memory slot now takes the twiddles of stages
+  // 0-3, 128 >> u words for stage u at [256 - (256 >> u), ...), loaded in one batch of 15 per
+  // thread instead of one dependent round of global loads per stage; tw_idx spreads each stage's
+  // stride-(8 >> u) reads over the banks.
+  // The copies are asynchronous (cp.async), so they hold no registers while in flight.
+  auto tw_idx = [](int w) { return w + (w >> 3); };  // < 272 for w < 240
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 15; ++i) {
+    const int u = i < 8 ? 0 : i < 12 ? 1 : i < 14 ? 2 : 3;
+    const int w = t + 16 * i, m = w - (256 - (256 >> u));
+    cp_async8(srow + tw_idx(w), roots + (1u << (log_n - 1 - u)) + (row << (7 - u)) + m);
+  }
+  cp_async_wait_all();
+  __syncwarp();
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const int d = 1 << u;
@@ -423,10 +448,11 @@ CKG_DEV void inv_rows_body_f64(const LimbRef& ref, const PrimeConst* P, const do
     for (int j = 0; j < 16; ++j)
       if (!(j & d)) {
         const uint32_t k = 16 * t + j;
-        const uint32_t h = 1u << (log_n - 1 - u);
-        gs_bf_f64(x[j], x[j + d], __ldg(roots + h + (row << (7 - u)) + (k >> (u + 1))), q, qinv);
+        const double w = bits_dbl(srow[tw_idx((256 - (256 >> u)) + (k >> (u + 1)))]);
+        gs_bf_f64(x[j], x[j + d], w, q, qinv);
       }
   }
+  __syncwarp();  // every thread of the row has read its twiddles
 #pragma unroll
   for (int j = 0; j < 16; ++j) srow[pad_idx(16 * t + j)] = dbl_bits(x[j]);
   __syncwarp();
