@@ -789,6 +789,43 @@ def stream_roofline(ops, n, k, alpha, ms_per_step, peaks):
             "note": "bounded by the integer and FP64 pipes (NTT butterflies, base conversion), not by HBM"}
 
 
+def pcie_ceiling(torch, h2d_bytes, d2h_bytes, ms_per_step, nbytes=1 << 30):
+    """The host link's bound on the e2e step: 1 GiB pinned <-> device copies timed with CUDA
+    events, each direction alone and both at once on two streams (as the e2e step overlaps
+    them). bound_ms_per_step = the step's larger direction at the concurrent per-direction rate."""
+    h_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(up, down, reps=3):
+        best = None
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            evs = []
+            for on, st, fn in ((up, s_in, lambda: d_in.copy_(h_in, non_blocking=True)),
+                               (down, s_out, lambda: h_out.copy_(d_out, non_blocking=True))):
+                if on:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(st)
+                    with torch.cuda.stream(st):
+                        fn()
+                    b.record(st)
+                    evs.append((a, b))
+            torch.cuda.synchronize()
+            ms = max(a.elapsed_time(b) for a, b in evs)
+            best = ms if best is None else min(best, ms)
+        return nbytes / (best * 1e-3) / 1e9
+
+    h2d, d2h, both = run(True, False), run(False, True), run(True, True)
+    bound = max(h2d_bytes, d2h_bytes) / (both * 1e9) * 1e3
+    del h_in, h_out, d_in, d_out
+    return {"h2d_gbs": round(h2d, 1), "d2h_gbs": round(d2h, 1), "concurrent_gbs_each_way": round(both, 1),
+            "bound_ms_per_step": round(bound, 1), "frac": round(bound / ms_per_step, 3),
+            "how": "1 GiB pinned copies, CUDA events, best of 3; both directions at once on two streams"}
+
+
 def ntt_roofline(torch, S, peaks, limbs=768):
     """Forward + inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as in a
     batched stage), timed alone with CUDA events on the library's stream. Algorithmic bytes
@@ -996,6 +1033,8 @@ def main():
         e2e = {"value": round(mix.ks * steps_e * world / (ms_e * 1e-3), 2), "unit": unit,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": round(ms_e / steps_e, 3)}
+        if rank == 0:  # no collective inside: the other ranks skip it
+            e2e["host_link"] = pcie_ceiling(torch, h2d, d2h, ms_e / steps_e)
     plain = None
     if not args.no_plain:
         P = Plain(S)
