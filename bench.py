@@ -826,17 +826,33 @@ def pcie_ceiling(torch, h2d_bytes, d2h_bytes, ms_per_step, nbytes=1 << 30):
             "how": "1 GiB pinned copies, CUDA events, best of 3; both directions at once on two streams"}
 
 
+# DRAM bytes (read + write) per 768-limb transform of ntt_roofline, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --profile ntt`: its twelve
+# launches (three 256-limb chunks, a column and a row pass each, forward then inverse) summed
+# and halved.
+NTT_TRAFFIC_PER_TRANSFORM = 1358850304
+
+
+def ntt_pair(torch, ctx, n, limbs=768):
+    """One forward and one inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as
+    in a batched stage), in place; returns (buffer, primes) for more rounds."""
+    buf = torch.randint(0, 1 << 40, (limbs, n), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    nprimes = len(ctx.q) + ctx.k
+    primes = [i % nprimes for i in range(limbs)]
+    ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, False)
+    ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, True)
+    return buf, primes
+
+
 def ntt_roofline(torch, S, peaks, limbs=768):
     """Forward + inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as in a
     batched stage), timed alone with CUDA events on the library's stream. Algorithmic bytes
     per transform: every limb read and written once (both passes together)."""
     ctx = S.ctx
-    buf = torch.randint(0, 1 << 40, (limbs, S.n), dtype=torch.int64, device="cuda")
-    torch.cuda.synchronize()
-    nprimes = len(ctx.q) + ctx.k
-    primes = [i % nprimes for i in range(limbs)]
+    buf, primes = ntt_pair(torch, ctx, S.n, limbs)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    for _ in range(3):
+    for _ in range(2):
         ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, False)
         ctx.ntt(buf.data_ptr(), buf.data_ptr(), primes, True)
     ctx.sync()
@@ -854,7 +870,8 @@ def ntt_roofline(torch, S, peaks, limbs=768):
     peak = peaks.get("hbm_gbs", 6650.0)
     return {"kernel": f"ntt forward/inverse, {limbs} limbs of N=2^16 per transform (2 passes)", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": None, "ms_per_transform": round(ms, 4), "alg_bytes": alg,
+            "traffic": NTT_TRAFFIC_PER_TRANSFORM if limbs == 768 else None,
+            "ms_per_transform": round(ms, 4), "alg_bytes": alg,
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback"}
 
 
@@ -926,7 +943,7 @@ def main():
     ap.add_argument("--mlp-only", action="store_true", help="measure the encrypted MLP training step only")
     ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
-    ap.add_argument("--profile", default=None, choices=["batch", "plain", "boot"],
+    ap.add_argument("--profile", default=None, choices=["batch", "plain", "boot", "ntt"],
                     help="run the set-up and `warmup` + 1 step of one path, print nothing (for ncu)")
     args = ap.parse_args()
 
@@ -978,6 +995,11 @@ def main():
     except Exception:
         pass
 
+    if args.profile == "ntt":  # the roofline's 768-limb forward + inverse transform pair, once
+        ctx = ckg.Context.from_bits(LOG_N, Q_BITS, P_BITS, DNUM, device=local, scale_bits=50)
+        ntt_pair(torch, ctx, ctx.n)
+        ctx.sync()
+        return
     if args.profile == "boot":
         B = BootBench(ckg, torch, local)
         for _ in range(args.warmup + 1):
