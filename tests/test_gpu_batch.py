@@ -142,3 +142,15 @@ def test_batch_tuning_is_bit_neutral(env):
             env.ckg.Batch(env.gpu).chunk_items = 0
     finally:
         ctx.ntt_wave = wave0
+
+
+@pytest.fixture(scope="module")
+def env_cfg2(ckg, oracle):
+    """The benchmark's own parameters: N = 2^16, 24 x 50-bit + 8 x 60-bit primes, dnum 3."""
+    return Env(ckg, oracle, "cfg2", [1, -1, 2, 4, 8])
+
+
+def test_batch_matches_oracle_cfg2(env_cfg2):
+    """A 48-op mix at random levels of the full-size parameters, replayed from a CUDA graph in
+    chunks of 16 ops: every coefficient equals the oracle's, levels, scales and counters too."""
+    _run_mix(env_cfg2, _mix(env_cfg2, 23, 48), True, chunk=16)
