@@ -252,13 +252,17 @@ void Batch::build() {
       sp += limbs * N;
       return p;
     };
+    // Rescale by the last prime: INTT of limb l, its centred lift to every other prime, NTT and
+    // finish. With two-pass transforms (N >= 2^12) the column pass reads the lift straight from the
+    // coefficient-form limb (LimbRef::aux = l + 1), so the lifted limbs are never written out.
+    const bool fuse_lift = c.log_n >= 12;
     auto rescale_poly = [&](const uint64_t* poly, uint32_t l, uint64_t* out) {
       uint64_t* last = carve(1 + l);
       uint64_t* T = last + N;
       intt_last.push_back(LimbRef{poly + (size_t)l * N, last, l, 0});
-      rs_conv.push_back(ConvJob{last, T, c.d_conv + c.rescale_off[l], N, N, (int)l, 0});
+      if (!fuse_lift) rs_conv.push_back(ConvJob{last, T, c.d_conv + c.rescale_off[l], N, N, (int)l, 0});
       for (uint32_t i = 0; i < l; ++i) {
-        fwd_rs.push_back(LimbRef{T + i * N, T + i * N, i, 0});
+        fwd_rs.push_back(fuse_lift ? LimbRef{last, T + i * N, i, l + 1} : LimbRef{T + i * N, T + i * N, i, 0});
         fin_rs.push_back(FinRef{poly + i * N, T + i * N, nullptr, nullptr, out + i * N, c.qlinv[l][i].first,
                                 c.qlinv[l][i].second, i, 0});
       }

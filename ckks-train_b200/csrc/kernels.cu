@@ -135,9 +135,20 @@ CKG_DEV void gs_bf_f64(double& x, double& y, double w, double q, double qinv) {
   y = mulmod_f64(d, w, q, qinv);
 }
 
+// The centred lift of x in [0, ql) to prime q: x when x <= (ql - 1) / 2, else x - ql, reduced
+// mod q (one_s = floor(2^64 / q)). It equals the one-source exact base conversion of the rescale
+// (x + h mod ql, lifted, minus h with h = (ql - 1) / 2; crates/ckks-train-core/src/baseconv.rs:258-291).
+CKG_DEV uint64_t centred_lift(uint64_t x, uint64_t ql, uint64_t q, uint64_t one_s) {
+  const bool neg = x > (ql >> 1);
+  const uint64_t m = neg ? ql - x : x;
+  const uint64_t r = csub(mul_shoup_lazy(m, 1, one_s, q), q);
+  return neg && r ? q - r : r;
+}
+
 // Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
 template <int LOGS, bool LAZY>
-CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roots, uint64_t* sm) {
+CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roots, uint64_t* sm, uint64_t lift_q,
+                           uint64_t one_s) {
   constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
   const uint64_t two_q = 2 * q;
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
@@ -145,6 +156,10 @@ CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roo
   uint64_t x[1 << E1];
 #pragma unroll
   for (int j = 0; j < (1 << E1); ++j) x[j] = ref.src[col + (size_t)kRow * (ts + TPS * j)];
+  if (lift_q) {
+#pragma unroll
+    for (int j = 0; j < (1 << E1); ++j) x[j] = centred_lift(x[j], lift_q, q, one_s);
+  }
 #pragma unroll
   for (int r = 0; r < E1; ++r) {
     const int half = 1 << (E1 - 1 - r);
@@ -178,14 +193,22 @@ CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roo
 
 // The same pass with FP64 butterflies; writes the raw doubles for the row pass.
 template <int LOGS>
-CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm) {
+CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm,
+                               uint64_t lift_q) {
   constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
   const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
   const int col = blockIdx.x * kCols + c;
   double x[1 << E1];
+  if (lift_q) {
+    const uint64_t qi = __ldg(&P->q), one_s = __ldg(&P->one_s);
 #pragma unroll
-  for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(ref.src[col + (size_t)kRow * (ts + TPS * j)]);
+    for (int j = 0; j < (1 << E1); ++j)
+      x[j] = f64_of(centred_lift(ref.src[col + (size_t)kRow * (ts + TPS * j)], lift_q, qi, one_s));
+  } else {
+#pragma unroll
+    for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(ref.src[col + (size_t)kRow * (ts + TPS * j)]);
+  }
 #pragma unroll
   for (int r = 0; r < E1; ++r) {
     const int half = 1 << (E1 - 1 - r);
@@ -227,15 +250,19 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
                    const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
   extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
   LimbRef ref = b.r[blockIdx.y];
-  if (in_place) ref.src = ref.dst;
+  // aux = p + 1: src is a limb of prime p in coefficient form, read through its centred lift
+  // (the rescale's one-source conversion fused into the load; never in place).
+  const uint64_t lift_q = ref.aux ? __ldg(&pc[ref.aux - 1].q) : 0;
+  if (in_place && !ref.aux) ref.src = ref.dst;
   const uint64_t q = __ldg(&pc[ref.prime].q);
   if (q < kF64Bound) {
-    fwd_cols_body_f64<LOGS>(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), sm);
+    fwd_cols_body_f64<LOGS>(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), sm, lift_q);
     return;
   }
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
-  if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm);
-  else fwd_cols_body<LOGS, false>(ref, q, roots, sm);
+  const uint64_t one_s = __ldg(&pc[ref.prime].one_s);
+  if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm, lift_q, one_s);
+  else fwd_cols_body<LOGS, false>(ref, q, roots, sm, lift_q, one_s);
 }
 
 // Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
