@@ -445,6 +445,9 @@ void rescale_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l
   if (!np) return;
   if (l < 1) throw Error(ST_NO_LEVELS_LEFT, "cannot rescale at level 0");
   auto scratch = c.alloc(np * (1 + l) * N);
+  // With two-pass transforms (N >= 2^12) the NTT's column pass reads the centred lift of the last
+  // limb itself (LimbRef::aux = l + 1); smaller rings run the one-source conversion first.
+  const bool fuse_lift = c.log_n >= 12;
   std::vector<LimbRef> refs;
   std::vector<ConvJob> jobs;
   for (size_t i = 0; i < np; ++i) {
@@ -453,18 +456,19 @@ void rescale_many(Context& c, const std::vector<const uint64_t*>& in, uint32_t l
     jobs.push_back(ConvJob{last, last + N, c.d_conv + c.rescale_off[l], N, N});
   }
   ntt_limbs(c, refs, true);
-  launch_bconv(c.dt, jobs.data(), (int)jobs.size(), 1, (int)l, c.stream);
+  if (!fuse_lift) launch_bconv(c.dt, jobs.data(), (int)jobs.size(), 1, (int)l, c.stream);
   refs.clear();
   std::vector<FinRef> fin;
   for (size_t i = 0; i < np; ++i) {
+    const uint64_t* last = scratch->p + i * (1 + l) * N;
     uint64_t* t = scratch->p + i * (1 + l) * N + N;
     for (uint32_t j = 0; j < l; ++j) {
-      refs.push_back(LimbRef{t + j * N, t + j * N, j, 0});
+      refs.push_back(LimbRef{last, t + j * N, j, l + 1});
       fin.push_back(FinRef{in[i] + j * N, t + j * N, nullptr, nullptr, out[i] + j * N, c.qlinv[l][j].first,
                            c.qlinv[l][j].second, j, 0});
     }
   }
-  launch_ntt_finish(c.dt, fin.data(), (int)fin.size(), c.stream);
+  launch_ntt_finish(c.dt, fin.data(), (int)fin.size(), c.stream, fuse_lift ? refs.data() : nullptr);
 }
 
 void mod_down_many(Context& c, const std::vector<ModDownJob>& jobs, uint32_t l) {

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <stdexcept>
 #include <vector>
 #include <type_traits>
 
@@ -1342,7 +1343,8 @@ void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
-void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {
+void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st, const LimbRef* cols) {
+  if (cols && d.log_n <= 11) throw std::logic_error("launch_ntt_finish: explicit column passes need N >= 2^12");
   if (d.log_n <= 11) {  // small transforms: separate NTT and finish
     std::vector<LimbRef> lr(count);
     for (int i = 0; i < count; ++i) lr[i] = LimbRef{refs[i].t, const_cast<uint64_t*>(refs[i].t), refs[i].prime, 0};
@@ -1359,7 +1361,7 @@ void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaSt
     fb.count = cnt;
     for (int i = 0; i < cnt; ++i) {
       fb.r[i] = refs[off + i];
-      b.r[i] = LimbRef{refs[off + i].t, const_cast<uint64_t*>(refs[off + i].t), refs[off + i].prime, 0};
+      b.r[i] = cols ? cols[off + i] : LimbRef{refs[off + i].t, const_cast<uint64_t*>(refs[off + i].t), refs[off + i].prime, 0};
     }
     launch_cols_any(false, b, cnt, d, 1, st);
     k_ntt_fwd_rows_finish<FinBatch><<<dim3(rgrid.x, cnt), 256, 0, st>>>(fb, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);

@@ -28,7 +28,10 @@ void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJ
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
 // Forward NTT of each FinRef's t (in place for the column pass) fused with its finish:
 // out = (x - NTT(t)) * c (+ add). `dev_cols` holds the matching in-place LimbRefs of t.
-void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st);
+// `cols`, when given, are the column passes' own refs (one per FinRef, N >= 2^12), e.g. a
+// centred-lift load (LimbRef::aux); by default each column pass runs in place on the FinRef's t.
+void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st,
+                       const LimbRef* cols = nullptr);
 void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const FinRef* dev_fin, int count,
                            cudaStream_t st);
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st);
