@@ -97,7 +97,7 @@ def test_n16_boot_shape(oracle):
 
 
 def test_dnum_must_divide(oracle):
-    """params.rs:111-116: dnum 3 does not divide 32 q primes (BASELINE's n16_boot dnum)."""
+    """params.rs:111-116: dnum 3 does not divide 32 q primes (a dnum of 3 on the n16_boot chain)."""
     with pytest.raises(oracle.OracleError):
         oracle.Params.from_bits(16, [54] + [42] * 31, [60] * 4, 42, 3)
 
