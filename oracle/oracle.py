@@ -131,6 +131,13 @@ def _declare(L):
     L.orc_decode_complex.argtypes = [vp, U64P, C.c_uint64, C.c_double, DP]
     L.orc_encrypt_sk.argtypes = [vp, C.c_char_p, U64P, C.c_uint64, C.c_double, C.POINTER(vp)]
     L.orc_decrypt.argtypes = [vp, vp, U64P]
+    L.orc_rng_new.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.orc_rng_free.argtypes = [vp]
+    L.orc_rng_next_u64.argtypes = [vp, C.c_uint64, U64P]
+    L.orc_keygen_public.argtypes = [vp, C.POINTER(vp)]
+    L.orc_pk_free.argtypes = [vp]
+    L.orc_encrypt_sk_rng.argtypes = [vp, vp, U64P, C.c_uint64, C.c_double, C.POINTER(vp)]
+    L.orc_encrypt_pk.argtypes = [vp, vp, vp, U64P, C.c_uint64, C.c_double, C.POINTER(vp)]
     L.orc_boot_new.argtypes = [vp, vp, vp, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
                                C.c_uint64, C.c_int64, C.POINTER(vp)]
     L.orc_boot_free.argtypes = [vp]
@@ -449,6 +456,9 @@ class KeyGenerator:
         _check(lib().orc_keygen_galois(self.h, elt, C.byref(h)))
         return Key(self.params, h)
 
+    def public_key(self):
+        return PublicKey(self)
+
 
 # ---- evaluator -----------------------------------------------------------------------
 
@@ -654,6 +664,73 @@ def encrypt_sk(ev, kg, seed, pt, scale):
     h = C.c_void_p()
     _check(lib().orc_encrypt_sk(kg.h, seed, _p64(p), p.shape[0] - 1, scale, C.byref(h)))
     return Ct(ev, h)
+
+
+class Rng:
+    """One `Rng::from_seed([seed; 32])` stream (crates/ckks-train-core/src/sampler.rs:35-37) that
+    successive calls consume in turn, as the reference's tests pass one `&mut Rng` first to
+    the input sampler and then to the encryptor."""
+
+    def __init__(self, seed):
+        if isinstance(seed, int):
+            seed = bytes([seed]) * 32
+        self.h = C.c_void_p()
+        _check(lib().orc_rng_new(seed, C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            lib().orc_rng_free(self.h)
+        except Exception:
+            pass
+
+    def next_u64(self, count):
+        out = np.zeros(count, np.uint64)
+        lib().orc_rng_next_u64(self.h, count, _p64(out))
+        return out
+
+    def uniform(self, count, a):
+        """`a * (2 u - 1)` with `u = (next_u64() >> 11) * 2^-53`, in order: the `uniform` helper
+        of the reference's bootstrap tests (bootstrap/bootstrapper.rs:446-450)."""
+        u = (self.next_u64(count) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+        return a * (2.0 * u - 1.0)
+
+
+class PublicKey:
+    """KeyGenerator::public_key (crates/ckks-train-ckks/src/keys.rs:365-369)."""
+
+    def __init__(self, kg):
+        self.kg = kg
+        self.h = C.c_void_p()
+        _check(lib().orc_keygen_public(kg.h, C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            lib().orc_pk_free(self.h)
+        except Exception:
+            pass
+
+
+def encrypt_pk(ev, pk, rng, pt, scale):
+    """Public-key encryption of the NTT-form plaintext `pt` (crates/ckks-train-ckks/src/encrypt.rs:68-90)
+    with randomness drawn from the stream `rng` (u, then e0, then e1)."""
+    p = np.ascontiguousarray(pt, np.uint64)
+    h = C.c_void_p()
+    _check(lib().orc_encrypt_pk(pk.kg.h, pk.h, rng.h, _p64(p), p.shape[0] - 1, scale, C.byref(h)))
+    return Ct(ev, h)
+
+
+def encrypt_sk_stream(ev, kg, rng, pt, scale):
+    """Symmetric encryption of `pt` (encrypt.rs:91-101) with randomness drawn from the stream `rng`."""
+    p = np.ascontiguousarray(pt, np.uint64)
+    h = C.c_void_p()
+    _check(lib().orc_encrypt_sk_rng(kg.h, rng.h, _p64(p), p.shape[0] - 1, scale, C.byref(h)))
+    return Ct(ev, h)
+
+
+def precision_bits(expected, actual):
+    """-log2 of the largest absolute error (crates/ckks-train-ckks/src/precision.rs:39-58)."""
+    err = float(np.max(np.abs(np.asarray(expected) - np.asarray(actual))))
+    return float("inf") if err == 0.0 else -np.log2(err)
 
 
 def decrypt(kg, ct):

@@ -369,3 +369,63 @@ def test_key_switch_noise_bound(oracle):
     digits = sum((float(np.prod([float(x) for x in P.q[s_:e_]])) / pp) ** 2 / 12.0 for s_, e_ in P.digit_ranges(level))
     pred = math.sqrt(P.n * 3.2 * 3.2 * digits + P.n * 0.5 / 12.0 + 1.0 / 12.0)
     assert sd <= 6 * pred, (sd, pred)
+
+
+# ---- encrypt.rs:68-90 and bootstrap/bootstrapper.rs:485-574 ------------------------------
+
+def test_public_key_encryption_decrypts(oracle):
+    """Public-key encryption (u ternary, e0 and e1 Gaussian over Q_l * P, divided by P with
+    rounding) decrypts to the plaintext with the noise bound of encrypt.rs:1-12: |r_0 + r_1 s|
+    plus a negligible term, so below 8 * k * N^(1/2)-ish; checked at k = 2 special primes."""
+    O = oracle
+    P = O.Params.from_bits(10, [54, 42, 42, 34], [60, 60], 42, 2)
+    kg = O.KeyGenerator(P, 3)
+    pk = kg.public_key()
+    ev = O.Evaluator(P)
+    enc = O.Encoder(P)
+    r = O.Rng(4)
+    m = r.uniform(P.n // 2, 1.0)
+    for level in (P.max_level, 1):
+        ct = O.encrypt_pk(ev, pk, r, enc.encode(m, 2.0 ** 42, level), 2.0 ** 42)
+        got = enc.decode(O.decrypt(kg, ct), 2.0 ** 42).real
+        assert ct.level == level
+        assert np.abs(got - m).max() < 2.0 ** -30
+
+
+def test_rng_stream_uniform(oracle):
+    """`uniform` of the reference's bootstrap tests: a * (2 ((next_u64 >> 11) 2^-53) - 1) over
+    one stream that later calls continue (bootstrapper.rs:446-450)."""
+    O = oracle
+    words = O.chacha_u64(bytes([2]) * 32, 8)
+    r = O.Rng(2)
+    u = r.uniform(5, 1.0)
+    want = [2.0 * (float(int(w) >> 11) * 2.0 ** -53) - 1.0 for w in words[:5]]
+    assert list(u) == want
+    assert list(r.next_u64(3)) == list(words[5:8])
+
+
+def test_reference_seeded_mini_bootstrap(oracle):
+    """The reference's `mini_bootstrap_precision_level_and_counts` fixture in its random-stream
+    order (keys from rng(1): public key, relinearization key, Bootstrapper::new; rng(2): m, then
+    the public-key encryption): output level 2, 2 SSE switches, 40 relinearizations, one
+    bootstrap counted, exactly Delta; 26.80 bits where the reference prints 26.77
+    (docs/bootstrap.md §11.4; the reference's raw outputs are not published, so the last
+    0.03 bit is not traced to a cause)."""
+    O = oracle
+    q_bits = [54, 42, 42] + [34] * 4 + [58] * 7 + [56] * 4
+    P = O.Params.from_bits(10, q_bits, [60, 60], 42, 9)
+    kg = O.KeyGenerator(P, 1)
+    enc = O.Encoder(P)
+    pk = kg.public_key()
+    rk = kg.relin_key()
+    bs = O.Bootstrapper(P, kg, enc, 9)
+    ev = O.Evaluator(P, rk)
+    r = O.Rng(2)
+    m = r.uniform(P.n // 2, 1.0)
+    ct = O.encrypt_pk(ev, pk, r, enc.encode(m, 2.0 ** 42, P.max_level), 2.0 ** 42)
+    out = bs.bootstrap(ev, ev.mod_switch_to_level(ct, 0))
+    assert out.level == bs.output_level() == 2 and out.scale == 2.0 ** 42
+    c = ev.counter()
+    assert (c["relins"], c["sse_switches"], c["bootstraps"]) == (40, 2, 1)
+    bits = O.precision_bits(m, enc.decode(O.decrypt(kg, out), out.scale).real)
+    assert bits >= 16.0 and abs(bits - 26.77) < 0.1, bits
