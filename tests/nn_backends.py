@@ -162,3 +162,51 @@ def plain_step(ws, bs, x, y, lr, n_valid=None):
         new_b[i] = bs[i] - c * dz.sum(axis=0)
         delta = dz @ ws[i]
     return new_w, new_b, zs, acts
+
+
+def deterministic_keys(P, steps, seed, threads=8):
+    """Relinearization key and the Galois keys of `steps` from `threads` key generators of the
+    same seed: generator t makes the keys of elements t, t + threads, ... one after another in
+    its own task, then generator 0 the relinearization key. The keys depend on the seed and
+    `threads` only (not on the host's core count or on scheduling)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    elts = sorted({O.galois_elt(P.n, s) for s in steps} - {1})
+    kgs = [O.KeyGenerator(P, seed) for _ in range(threads)]
+
+    def task(t):
+        return [(e, kgs[t].galois_key(e)) for e in elts[t::threads]]
+
+    with ThreadPoolExecutor(threads) as ex:
+        parts = list(ex.map(task, range(threads)))
+    gk = dict(kv for part in parts for kv in part)
+    return kgs[0], kgs[0].relin_key(), {e: gk[e] for e in elts}
+
+
+def step_values(v, mlp):
+    """Every ciphertext of one training step in a fixed order, as (name, ciphertext): the
+    forward values, deltas, derivative factors, dz, backward deltas and bias gradients, the
+    transposed weights and weight gradients, then the updated network."""
+    out = []
+    for name in ("z", "a", "delta", "s", "dz", "backward", "db"):
+        for i in sorted(v[name]):
+            out.append((f"{name}{i + 1}", v[name][i]))
+    for name in ("wt", "dw"):
+        for i in sorted(v[name]):
+            es = v[name][i].entries if name == "wt" else v[name][i]
+            out.extend((f"{name}{i + 1}[{k}]", e) for k, e in enumerate(es))
+    for i, (dense, _) in enumerate(mlp.layers):
+        out.extend((f"W{i + 1}'[{k}]", e) for k, e in enumerate(dense.w.entries))
+        out.append((f"b{i + 1}'", dense.b))
+    return out
+
+
+def ct_digest(data, level, scale):
+    """SHA-256 of a ciphertext's words (little-endian u64, components x limbs x N), its level
+    and the bits of its f64 scale."""
+    import hashlib
+    import struct
+
+    h = hashlib.sha256(np.ascontiguousarray(data, "<u8").tobytes())
+    h.update(struct.pack("<Qd", int(level), float(scale)))
+    return h.hexdigest()

@@ -5,32 +5,21 @@
   and the updated network), with equal counters and level traces, on the N = 2^11 miniature
   of n16_train;
 * config 4 at full size: N = 2^16 n16_train (58 + 31 x 42-bit q, 4 x 58-bit p, dnum 8, scale
-  2^42), Layout(2^15, 256, 64), 196 -> 64 -> 10 with Square, B = 64: the decrypted update
-  against the plaintext SGD step and the counter against the cost formula.
+  2^42), Layout(2^15, 256, 64), 196 -> 64 -> 10 with Square, B = 64: ct-for-ct against the
+  oracle's run of the same step (digests of every ciphertext), the counter against the cost
+  formula, and the decrypted update against the plaintext SGD step.
 """
-
-from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import pytest
 
 from gpu_util import assert_same
-from nn_backends import Client, OracleHeOps, plain_step
+from nn_backends import Client, OracleHeOps, ct_digest, deterministic_keys, plain_step, step_values
 from test_nn import MINI, encrypt_network, make_problem
 
 pytestmark = pytest.mark.gpu
 
 N16_TRAIN = dict(log_n=16, q_bits=[58] + [42] * 31, p_bits=[58] * 4, scale_bits=42, dnum=8)
-
-
-def _keys(O, P, steps, seed, threads=8):
-    """Relinearization key and the Galois keys of `steps`, generated in threads (one key
-    generator per thread; the secret depends on the seed only)."""
-    elts = sorted({O.galois_elt(P.n, s) for s in steps} - {1})
-    kgs = [O.KeyGenerator(P, seed) for _ in range(threads)]
-    with ThreadPoolExecutor(threads) as ex:
-        gks = list(ex.map(lambda i: kgs[i % threads].galois_key(elts[i]), range(len(elts))))
-    return kgs[0], kgs[0].relin_key(), dict(zip(elts, gks))
 
 
 def _gpu_env(ckg, P, ps, rk, gk, ctx=None):
@@ -51,7 +40,7 @@ def test_training_step_parity(ckg, oracle):
     nn, O = ckg.nn, oracle
     P = O.Params.from_bits(MINI["log_n"], MINI["q_bits"], MINI["p_bits"], MINI["scale_bits"], MINI["dnum"])
     layout, dims = nn.Layout(P.n // 2, 16, 8), [12, 8, 3]
-    kg, rk, gk = _keys(O, P, nn.mlp_rotation_steps(dims, layout), 21)
+    kg, rk, gk = deterministic_keys(P, nn.mlp_rotation_steps(dims, layout), 21)
     cpu = OracleHeOps(P, rk, gk)
     _, gpu = _gpu_env(ckg, P, MINI, rk, gk)
     client = Client(P, kg)
@@ -107,13 +96,24 @@ class _Replay:
         return c
 
 
-def test_config4_training_step(ckg, oracle):
-    """196 -> 64 -> 10, Square, B = 64 on n16_train: decrypted update vs plaintext SGD."""
+def test_config4_ct_for_ct(ckg, oracle):
+    """Config 4 at full size: 196 -> 64 -> 10, Square, B = 64 on n16_train, Layout(2^15, 256, 64).
+    Every ciphertext of the step (forward values, deltas, derivative factors, dz, transposed
+    weights, backward deltas, weight and bias gradients, the updated network) has the digest
+    of the oracle's ciphertext on the same seeded keys and inputs (tests/golden/config4_digests.json,
+    made by tests/golden/make_config4_digests.py), with its level and scale; the counter and the
+    level trace are the oracle's; and the decrypted update is the plaintext SGD step."""
+    import json
+    import os
+
+    gold_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config4_digests.json")
+    with open(gold_path) as f:
+        gold = json.load(f)
     nn, O = ckg.nn, oracle
     ps = N16_TRAIN
     P = O.Params.from_bits(ps["log_n"], ps["q_bits"], ps["p_bits"], ps["scale_bits"], ps["dnum"])
     layout, dims = nn.Layout(P.n // 2, 256, 64), [196, 64, 10]
-    kg, rk, gk = _keys(O, P, nn.mlp_rotation_steps(dims, layout), 41, threads=16)
+    kg, rk, gk = deterministic_keys(P, nn.mlp_rotation_steps(dims, layout), 41)
     ctx, gpu = _gpu_env(ckg, P, ps, rk, gk)
     del gk
     client = Client(P, kg)
@@ -124,15 +124,22 @@ def test_config4_training_step(ckg, oracle):
                                   lambda c: gpu.upload_ct(c.data(), c.scale))
     lr = 0.05
     tr = nn.Trainer(gpu, layout, [nn.Sgd(lr) for _ in dims[1:]])
-    tr.train_batch(mlp, xc, yc)
+    v = tr.train_batch(mlp, xc, yc)
     assert dict(tr.trace)["W1'"] == top - 9
-    assert gpu.counter() == dict(nn.step_counts(dims, layout), sse_switches=0, bootstraps=0)
+    assert [list(t) for t in tr.trace] == gold["trace"]
+    assert gpu.counter() == gold["counter"] == dict(nn.step_counts(dims, layout), sse_switches=0, bootstraps=0)
+    got = step_values(v, mlp)
+    assert [name for name, _ in got] == [g[0] for g in gold["values"]]
+    for (name, ct), (_, level, scale, digest) in zip(got, gold["values"]):
+        data, sc = gpu.download_ct(ct)
+        assert ct.level() == level and sc == scale, f"{name}: level/scale"
+        assert ct_digest(data, ct.level(), sc) == digest, f"{name}: words differ from the oracle's"
     new_w, new_b, _, _ = plain_step(ws, bs, x, y, lr)
     for i, (dense, _) in enumerate(mlp.layers):
         w = dense.w
         vals = [client.decrypt(gpu.download_ct(e)[0], e.level(), e.scale()) for e in w.entries]
-        got = nn.unpack_weight_diagonals(vals, w.d_out, w.d_in, layout, 0)
-        err = np.abs(got - new_w[i]).max()
+        got_w = nn.unpack_weight_diagonals(vals, w.d_out, w.d_in, layout, 0)
+        err = np.abs(got_w - new_w[i]).max()
         assert err < 1e-5, f"W{i + 1}: {err}"
         bv = client.decrypt(gpu.download_ct(dense.b)[0], dense.b.level(), dense.b.scale())
         assert np.abs(nn.unpack_activations(bv, layout, w.d_out)[0] - new_b[i]).max() < 1e-5, f"b{i + 1}"
