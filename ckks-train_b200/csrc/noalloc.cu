@@ -6,7 +6,11 @@
 // The working space of the key switch (the coefficient copy of the input, the converted
 // digits, both accumulators and the ModDown temporaries) lives in one file-scope device
 // array of fixed size, shared by every call in the process. Its device address is looked
-// up once per device, on the first call made with that device current.
+// up with the device current on every call made outside stream capture, so a context that
+// was reset and re-created (the module loaded again, possibly at another address) gets the
+// new address. A call made while its stream is capturing uses the address found by the
+// last call outside capture on that device, so the first call on a device must come before
+// any capture.
 #include <mutex>
 
 #include "../../include/ckg.h"
@@ -26,13 +30,18 @@ uint64_t* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of g_ks_scratch on the current device (host code may not use the symbol
 // itself as an address: it names a host-side stand-in).
-uint64_t* scratch_on(int device) {
+uint64_t* scratch_on(int device, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[device]) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_ks_scratch);
     if (e != cudaSuccess) ckg::throw_cuda(e, "cudaGetSymbolAddress(g_ks_scratch)");
     g_scratch_addr[device] = (uint64_t*)p;
+  } else if (!g_scratch_addr[device]) {
+    throw ckg::Error(CKG_INVALID_PARAMS,
+                     "the first allocation-free key switch on a device must come before any stream capture");
   }
   return g_scratch_addr[device];
 }
@@ -53,7 +62,7 @@ extern "C" int ckg_key_switch_noalloc(ckg_ctx* ctx, const ckg_key* key, const ui
     if (!key || !key->k) throw ckg::Error(CKG_INVALID_PARAMS, "null key");
     if (c.device < 0 || c.device >= kMaxDevices) throw ckg::Error(CKG_INVALID_PARAMS, "device ordinal out of range");
     c.activate();
-    uint64_t* scratch = scratch_on(c.device);
+    uint64_t* scratch = scratch_on(c.device, c.stream);
     ckg::KsJob j;
     j.in = in;
     j.key = key->k.get();

@@ -655,11 +655,15 @@ void Server::completer() {
     }
     for (auto& seg : f->segs) {  // each segment completes its own requests
       cudaError_t e = cudaSuccess;
-      if (seg.done)
+      if (seg.done) {
         while ((e = cudaEventQuery(seg.done)) == cudaErrorNotReady)
           std::this_thread::sleep_for(std::chrono::microseconds(20));
-      else
+      } else {
+        // No completion event could be created: wait for the whole compute stream, so the
+        // flight's working space and keys are released only after its kernels have run.
+        cudaStreamSynchronize(ctx_->stream);
         e = cudaErrorUnknown;
+      }
       {
         std::lock_guard<std::mutex> lk(mu_);
         const auto t = Clock::now();

@@ -43,13 +43,22 @@ def test_noalloc_matches_key_switch_n16(ckg, oracle):
     _compare_two_calls(ckg, oracle, "cfg2", [23, 23], seed=4)
 
 
-def test_noalloc_rejects_oversized(ckg):
+def test_noalloc_rejects_oversized(ckg, oracle):
     """N = 2^16 with 32 + 4 primes and 8 digits needs 216 MiB at its top level: rejected
-    with a clear error before anything runs; a low level of the same context fits."""
-    q, p = ckg.primes_for_bits(16, [54] + [42] * 16 + [34] * 4 + [58] * 7 + [56] * 4, [60] * 4)
-    ctx = ckg.Context(16, q, p, 8)
+    with a clear error before anything runs. A low level of the same context (level 3,
+    about 22 MiB) fits, and gives the regular entry point's result."""
+    P = oracle.Params.from_bits(16, [54] + [42] * 16 + [34] * 4 + [58] * 7 + [56] * 4, [60] * 4, 42, 8)
+    ctx = ckg.Context(16, P.q, P.p, 8)
     n = 1 << 16
     dd = to_dev(np.zeros((32, n), np.uint64))
     out = empty_dev((32, n))
     with pytest.raises(ckg.InvalidParams, match="working space"):
         ctx.key_switch_noalloc(None, ptr(dd), 31, ptr(out), ptr(out))
+    key = ctx.upload_key(oracle.KeyGenerator(P, 6).relin_key().export())
+    d = to_dev(P.random_q(77, 3))
+    rb, ra, nb, na = (empty_dev((4, n)) for _ in range(4))
+    ctx.key_switch(key, ptr(d), 3, ptr(rb), ptr(ra))
+    ctx.key_switch_noalloc(key, ptr(d), 3, ptr(nb), ptr(na))
+    ctx.sync()
+    assert_same(from_dev(nb), from_dev(rb), "n16_boot level 3: b")
+    assert_same(from_dev(na), from_dev(ra), "n16_boot level 3: a")
