@@ -939,6 +939,9 @@ def main():
     ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
     ap.add_argument("--no-mlp", action="store_true")
+    ap.add_argument("--bconv", default="auto", choices=["auto", "tc", "int"],
+                    help="base conversion engine: tensor cores from 6 sources (auto, the default), tensor cores "
+                         "at every source count (tc), integer kernels (int)")
     ap.add_argument("--ntt-wave", type=int, default=None, help="fixed NTT limb wave (with --chunk-items; default: autotune)")
     ap.add_argument("--chunk-items", type=int, default=None, help="fixed batch chunk size (with --ntt-wave)")
     ap.add_argument("--mlp-only", action="store_true", help="measure the encrypted MLP training step only")
@@ -1018,6 +1021,7 @@ def main():
             print(json.dumps({"bootstrap": out}))
         return
     S = Setup(ckg, torch, local)
+    S.ctx.bconv_tc = {"int": 0, "auto": 1, "tc": 2}[args.bconv]
     if args.serve_only:
         sv = BootServing(ckg, torch, local)
         out = sv.measure(args.serve_requests)
@@ -1110,7 +1114,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64",
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
-                "config": dict(config, key_switches_per_step=int(mix.ks),
+                "config": dict(config, key_switches_per_step=int(mix.ks), bconv=args.bconv,
                                autotune={"ntt_wave": tuning["ntt_wave"], "chunk_items": tuning["chunk_items"],
                                          "trials_ms": [[w, c, round(m, 3)] for w, c, m in tuning["trials"]]}),
                 "e2e": e2e,

@@ -46,7 +46,8 @@ struct Batch::Stage {
   List tensor, pmul, gather, intt_in, fwd_conv, ip, intt_p, md_conv, fwd_md, fin_ks, intt_last, rs_conv, fwd_rs,
       fin_rs;
   std::vector<std::pair<int, List>> modup;  // by number of source primes
-  int ip_max_limbs = 0;
+  std::vector<int> modup_dst;               // the largest target count of each modup list
+  int ip_max_limbs = 0, md_dst = 0, rs_dst = 0;
 };
 
 Batch::Batch(Evaluator* ev) : ev_(ev), ctx_(ev->ctx()), chunk_items_(kChunkItems) {}
@@ -354,7 +355,14 @@ void Batch::build() {
     S.gather = db.put(gather);
     S.intt_in = db.put(intt_in);
     for (int ns = 1; ns <= kMaxSrc; ++ns)
-      if (!modup[ns].empty()) S.modup.push_back({ns, db.put(modup[ns])});
+      if (!modup[ns].empty()) {
+        S.modup.push_back({ns, db.put(modup[ns])});
+        int mx = 0;
+        for (const ConvJob& j : modup[ns]) mx = std::max(mx, j.n_dst);
+        S.modup_dst.push_back(mx);
+      }
+    for (const ConvJob& j : md_conv) S.md_dst = std::max(S.md_dst, j.n_dst);
+    for (const ConvJob& j : rs_conv) S.rs_dst = std::max(S.rs_dst, j.n_dst);
     S.fwd_conv = db.put(fwd_conv);
     S.ip = db.put(ip);
     S.intt_p = db.put(intt_p);
@@ -384,16 +392,18 @@ void Batch::issue() {
     launch_binary_ptr(c.dt, (const BinRef*)at(S->pmul), S->pmul.count, 2, c.stream);
     launch_gather_ptr(c.dt, (const GatherRef*)at(S->gather), S->gather.count, c.stream);
     if (S->intt_in.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_in), S->intt_in.count, true, c.stream);
-    for (auto& m : S->modup) launch_bconv_ptr(c.dt, (const ConvJob*)at(m.second), m.second.count, m.first, c.stream);
+    for (size_t g = 0; g < S->modup.size(); ++g)
+      launch_bconv_ptr(c.dt, (const ConvJob*)at(S->modup[g].second), S->modup[g].second.count, S->modup[g].first,
+                       c.stream, S->modup_dst[g]);
     if (S->fwd_conv.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->fwd_conv), S->fwd_conv.count, false, c.stream);
     launch_inner_product_ptr(c.dt, (int)c.alpha, (int)c.L, (int)c.k, (const IpJob*)at(S->ip), S->ip.count,
                              S->ip_max_limbs, c.stream);
     if (S->intt_p.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_p), S->intt_p.count, true, c.stream);
-    launch_bconv_ptr(c.dt, (const ConvJob*)at(S->md_conv), S->md_conv.count, (int)c.k, c.stream);
+    launch_bconv_ptr(c.dt, (const ConvJob*)at(S->md_conv), S->md_conv.count, (int)c.k, c.stream, S->md_dst);
     launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_md), (const FinRef*)at(S->fin_ks), S->fin_ks.count,
                           c.stream);
     if (S->intt_last.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_last), S->intt_last.count, true, c.stream);
-    launch_bconv_ptr(c.dt, (const ConvJob*)at(S->rs_conv), S->rs_conv.count, 1, c.stream);
+    launch_bconv_ptr(c.dt, (const ConvJob*)at(S->rs_conv), S->rs_conv.count, 1, c.stream, S->rs_dst);
     launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_rs), (const FinRef*)at(S->fin_rs), S->fin_rs.count,
                           c.stream);
   }

@@ -87,6 +87,15 @@ int ckg_ctx_sync(ckg_ctx* ctx) {
   c.activate();
   CKG_CUDA(cudaStreamSynchronize(c.stream));
   c.sync_transfers();
+  const int f = device_fault_take();
+  if (f > 0) throw Error(CKG_DEVICE, "a kernel recorded a device fault (code " + std::to_string(f) + ")");
+  CKG_API_END
+}
+
+int ckg_device_fault(ckg_ctx* ctx, int32_t* code) {
+  CKG_API_BEGIN
+  ctx_of(ctx).activate();
+  *code = device_fault_take();
   CKG_API_END
 }
 
@@ -593,6 +602,21 @@ int ckg_ctx_set_ntt_wave(ckg_ctx* ctx, int32_t limbs) {
 }
 
 int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx) { return ctx && ctx->c ? ctx->c->dt.ntt_wave : -1; }
+
+int ckg_ctx_set_bconv_tc(ckg_ctx* ctx, int32_t on) {
+  CKG_API_BEGIN
+  Context& c = ctx_of(ctx);
+  if (on < 0 || on > 2) throw Error(CKG_INVALID_PARAMS, "conversion engine mode must be 0, 1 or 2");
+  if (on) {
+    bool big = c.log_n >= 7;
+    for (uint64_t v : c.primes) big = big && v >= (1ULL << 30);
+    if (!big) throw Error(CKG_INVALID_PARAMS, "tensor-core conversion needs N >= 2^7 and primes of at least 30 bits");
+  }
+  c.dt.bconv_tc = on;
+  CKG_API_END
+}
+
+int32_t ckg_ctx_bconv_tc(ckg_ctx* ctx) { return ctx && ctx->c ? ctx->c->dt.bconv_tc : -1; }
 
 int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items) {
   CKG_API_BEGIN

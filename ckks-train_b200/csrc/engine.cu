@@ -170,6 +170,9 @@ uint32_t ip_f64_offset(uint64_t q, uint32_t beta) {
   return (uint32_t)off;
 }
 
+void tc_block(const std::vector<HostMod>& mods, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst,
+              std::vector<uint64_t>& w);
+
 // Conversion table (kernels.cuh ConvLayout) for sources `src` -> targets `dst` (global prime
 // indices): sum_j y_j [S/s_j]_t - e [S]_t - [h]_t with h = (S-1)/2. Targets that allow it get the
 // FP64-assisted record and come first.
@@ -241,7 +244,66 @@ std::vector<uint64_t> conv_table(const std::vector<HostMod>& mods, const std::ve
       for (size_t j = 0; j < ns; ++j) w.push_back(0);
     }
   }
+  tc_block(mods, src, dst, w);
   return w;
+}
+
+// The tensor-core block of a conversion table (kernels.cuh ConvLayout, bconv_tc.cu): the
+// per-target constants and the byte-split weights. sum_j y_j w_tj = sum_j sum_a y_j[a] 2^(8a) w_tj
+// is congruent mod t to sum_b 2^(8b) C_b with C_b = sum_(j,a) y_j[a] W[o, b][j, a], where
+// W[o, b][j, a] is byte b of [2^(8a) w_tj]_t: a u8 x u8 -> s32 product of the source bytes (the
+// y_j words as stored) with these weight bytes.
+void tc_block(const std::vector<HostMod>& mods, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst,
+              std::vector<uint64_t>& w) {
+  const size_t ns = src.size(), nd = dst.size();
+  while (w.size() % 2) w.push_back(0);
+  bool big = true;
+  for (uint32_t t : dst) big = big && mods[t].q >= (1ULL << 30);
+  if (ns == 0 || ns > (size_t)ConvLayout::kTcMaxSrc || nd == 0 || nd > (size_t)ConvLayout::kTcMaxDst || !big) {
+    w.push_back(0);  // no block: the header reads K = N = 0
+    w.push_back(0);
+    return;
+  }
+  const int K = ns <= 4 ? 32 : 64;
+  const int N = (int)((8 * nd + 15) / 16 * 16);
+  w.push_back((uint64_t)K | ((uint64_t)N << 32));
+  w.push_back(0);
+  std::vector<uint8_t> B((size_t)N * K, 0);
+  for (size_t o = 0; o < nd; ++o) {
+    const HostMod& m = mods[dst[o]];
+    uint64_t S = 1 % m.q;
+    for (uint32_t s : src) S = m.mul(S, mods[s].q % m.q);
+    const uint64_t h = m.mul(m.sub(S, 1 % m.q), (m.q + 1) / 2);
+    auto bits = [](double v) {
+      uint64_t b;
+      memcpy(&b, &v, 8);
+      return b;
+    };
+    w.push_back(m.q);
+    w.push_back(bits(1.0 / (double)m.q));
+    w.push_back(m.q - S);
+    w.push_back(m.q - h);
+    w.push_back(bits((double)(m.q - S)));
+    w.push_back(bits((double)(m.q - h)));
+    for (size_t j = 0; j < ns; ++j) {
+      uint64_t qhat = 1 % m.q;
+      for (size_t i = 0; i < ns; ++i)
+        if (i != j) qhat = m.mul(qhat, mods[src[i]].q % m.q);
+      uint64_t v = qhat;  // [2^(8a) w_tj]_t for a = 0, 1, ...
+      for (int a = 0; a < 8; ++a) {
+        const int k = (int)(8 * j + a);
+        for (int b = 0; b < 8; ++b) {
+          const int r = (int)(8 * o + b);
+          B[(size_t)(r / 8) * (8 * K) + (k / 16) * 128 + (r % 8) * 16 + (k % 16)] = (uint8_t)(v >> (8 * b));
+        }
+        v = m.mul(v, 256 % m.q);
+      }
+    }
+  }
+  const size_t words = B.size() / 8;
+  const size_t at = w.size();
+  w.resize(at + words);
+  memcpy(w.data() + at, B.data(), B.size());
 }
 
 }  // namespace
@@ -338,10 +400,18 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
   CKG_CUDA(cudaMemcpy(d_twd_fwd, twdf.data(), np * n * sizeof(double), cudaMemcpyHostToDevice));
   CKG_CUDA(cudaMemcpy(d_twd_inv, twdi.data(), np * n * sizeof(double), cudaMemcpyHostToDevice));
   dt = DevTables{d_prime, d_tw_fwd, d_tw_inv, d_twd_fwd, d_twd_inv, (int)log_n};
+  // The tensor-core conversion's FP64 quotient needs targets of at least 30 bits, and its tiles
+  // 128 coefficients; then every table of <= 8 sources and <= 32 targets carries its block.
+  {
+    bool big = true;
+    for (uint64_t v : primes) big = big && v >= (1ULL << 30);
+    dt.bconv_tc = big && log_n >= 7 ? 1 : 0;
+  }
 
   // conversion tables
   std::vector<uint64_t> conv;
   auto push = [&](const std::vector<uint64_t>& t) {
+    if (conv.size() % 2) conv.push_back(0);  // tables start on 16-byte boundaries
     size_t off = conv.size();
     conv.insert(conv.end(), t.begin(), t.end());
     return off;

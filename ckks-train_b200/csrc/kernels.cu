@@ -1308,12 +1308,15 @@ void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src,
       cb.j[i] = jobs[off + i];
       cb.j[i].n_dst = n_dst;
     }
-    bconv_launch(d, cb, cb.count, n_src, st);
+    if (!launch_bconv_tc(d, cb, cb.count, n_src, n_dst, st)) bconv_launch(d, cb, cb.count, n_src, st);
   }
 }
 
-void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st) {
-  if (count) bconv_launch(d, ConvPtrs{count, n_src, 0, 0, dev_jobs}, count, n_src, st);
+void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st,
+                      int max_dst) {
+  if (!count) return;
+  if (max_dst > 0 && launch_bconv_tc_ptr(d, dev_jobs, count, n_src, max_dst, st)) return;
+  bconv_launch(d, ConvPtrs{count, n_src, 0, 0, dev_jobs}, count, n_src, st);
 }
 
 void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJob* jobs, int count, cudaStream_t st) {

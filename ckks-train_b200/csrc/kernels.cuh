@@ -82,6 +82,17 @@ struct ConvLayout {
   static __host__ __device__ int size(int n_src, int n_dst) {
     return kHeadWords + kSrcWords * n_src + dst_words(n_src) * n_dst;
   }
+  // The tensor-core block follows the records at the next 16-byte boundary (tables start on
+  // one), for n_src <= kTcMaxSrc and n_dst <= kTcMaxDst:
+  //   word 0: K | N << 32 (K = 32 or 64 operand bytes per coefficient, N = MMA width, a
+  //   multiple of 16 >= 8 n_dst), word 1: 0; then 6 words per target in output order: t,
+  //   bits(1/t), t - [S]_t, t - [h]_t, bits(f64(t - [S]_t)), bits(f64(t - [h]_t)); then the
+  //   B operand: N rows (target o, byte b at row 8 o + b) of K bytes, row (o, b) holding at
+  //   byte 8 j + a the byte b of [2^(8a) w_oj]_t, stored as 8-row x 16-byte core matrices (row
+  //   group stride 8 K bytes, K-chunk stride 128).
+  static constexpr int kTcMaxSrc = 8;
+  static constexpr int kTcMaxDst = 32;
+  static __host__ __device__ int tc_offset(int n_src, int n_dst) { return (size(n_src, n_dst) + 1) & ~1; }
 };
 // FP64-assisted records serve at most this many sources (kernel register arrays).
 constexpr int kMaxSrcF64 = 8;

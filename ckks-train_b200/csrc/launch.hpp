@@ -20,6 +20,7 @@ struct DevTables {
   const double* twd_inv;
   int log_n;
   int ntt_wave;  // limbs per column + row launch pair of device-list transforms (0: all at once)
+  int bconv_tc;  // tensor-core conversions (<= 8 sources, <= 32 targets): 0 off, 1 from 6 sources, 2 all
 };
 
 void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st);
@@ -42,7 +43,17 @@ void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStr
 
 // The same kernels over work lists resident in device memory (one launch each).
 void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st);
-void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st);
+// max_dst: the largest job's target count (0: unknown, the integer kernel runs).
+void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st,
+                      int max_dst = 0);
+// The tensor-core conversion (bconv_tc.cu); false when it does not apply (d.bconv_tc off, more
+// than 8 sources or 32 targets, N < 2^7), in which case nothing was launched.
+bool launch_bconv_tc(const DevTables& d, const ConvBatch& cb, int count, int n_src, int max_dst, cudaStream_t st);
+bool launch_bconv_tc_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, int max_dst,
+                         cudaStream_t st);
+// Reads and clears the current device's fault word: nonzero when a kernel's bounded wait ran out
+// (1) or it was handed a table without its tensor-core block (2); -1 when it cannot be read.
+int device_fault_take();
 void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const IpJob* dev_jobs, int count,
                               int max_limbs, cudaStream_t st);
 void launch_finish_ptr(const DevTables& d, const FinRef* dev_refs, int count, cudaStream_t st);

@@ -168,6 +168,10 @@ def _declare(L):
     L.ckg_ctx_set_ntt_wave.argtypes = [VP, C.c_int32]
     L.ckg_ctx_ntt_wave.argtypes = [VP]
     L.ckg_ctx_ntt_wave.restype = C.c_int32
+    L.ckg_ctx_set_bconv_tc.argtypes = [VP, C.c_int32]
+    L.ckg_ctx_bconv_tc.argtypes = [VP]
+    L.ckg_ctx_bconv_tc.restype = C.c_int32
+    L.ckg_device_fault.argtypes = [VP, C.POINTER(C.c_int32)]
     L.ckg_batch_set_chunk_items.argtypes = [VP, C.c_int32]
     L.ckg_batch_chunk_items.argtypes = [VP]
     L.ckg_batch_chunk_items.restype = C.c_int32
@@ -315,6 +319,22 @@ class Context:
     @ntt_wave.setter
     def ntt_wave(self, limbs):
         _check(lib().ckg_ctx_set_ntt_wave(self.h, int(limbs)))
+
+    @property
+    def bconv_tc(self):
+        """Base conversion engine (bit-neutral): 0 integer kernels, 1 tensor cores from 6 sources
+        on (the default where the context qualifies), 2 tensor cores for every source count."""
+        return lib().ckg_ctx_bconv_tc(self.h)
+
+    @bconv_tc.setter
+    def bconv_tc(self, mode):
+        _check(lib().ckg_ctx_set_bconv_tc(self.h, int(mode)))
+
+    def device_fault(self):
+        """Reads and clears the device fault word (0: none)."""
+        v = C.c_int32()
+        _check(lib().ckg_device_fault(self.h, C.byref(v)))
+        return v.value
 
     def digit_ranges(self, level):
         """keyswitch::digit_ranges (crates/ckks-train-ckks/src/keyswitch.rs:68-74)."""

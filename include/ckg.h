@@ -130,8 +130,10 @@ CKG_API int ckg_key_switch(ckg_ctx* ctx, const ckg_key* key, const uint64_t* in,
  *    (e.g. N = 2^16 with 32 data + 4 special primes at its top level) is rejected with
  *    CKG_INVALID_PARAMS and a message stating both sizes; N = 2^16 with 24 + 8 primes and
  *    3 digits fits at every level.
- *  - The first call on a device looks up that array's device address; make that first
- *    call before any stream capture.
+ *  - Every call made outside stream capture looks up that array's device address on the
+ *    context's device (so a device reset and a new context are followed); a call made
+ *    while the stream captures reuses the last address found, so make the first call on a
+ *    device before any stream capture.
  *  - Every call shares the array and leaves it holding its own intermediates; nothing in
  *    it needs to start at zero (each call writes every word it reads). Calls that overlap
  *    on the GPU, for instance from two contexts with different streams on one device,
@@ -256,6 +258,19 @@ CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
  * replay), at most `max_trials` of them; `n_trials` the count. */
 CKG_API int ckg_ctx_set_ntt_wave(ckg_ctx* ctx, int32_t limbs);
 CKG_API int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx);
+/* Base conversion engine of a context (bit-neutral; no reference counterpart: the reference's
+ * basis_convert runs on CUDA cores). Conversions of <= 8 sources and <= 32 targets can run as
+ * exact u8 x u8 -> s32 products on the tensor cores (tcgen05) with an FP64-quotient reduction.
+ * Mode 1 (the default when N >= 2^7 and every prime has at least 30 bits) uses them from 6
+ * sources on, where they measured faster than the integer kernels; 2 for every source count;
+ * 0 never. Setting 1 or 2 on a context that does not qualify fails with CKG_INVALID_PARAMS. */
+CKG_API int ckg_ctx_set_bconv_tc(ckg_ctx* ctx, int32_t on);
+CKG_API int32_t ckg_ctx_bconv_tc(ckg_ctx* ctx);
+/* Reads and clears the device fault word of the context's device: 0 when no kernel recorded a
+ * fault, 1 when a kernel's bounded wait ran out (it freed its tensor memory and returned without
+ * its results), 2 when a conversion table lacked its tensor-core block; ckg_ctx_sync also checks
+ * it and fails with CKG_DEVICE. */
+CKG_API int ckg_device_fault(ckg_ctx* ctx, int32_t* code);
 CKG_API int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items);
 CKG_API int32_t ckg_batch_chunk_items(const ckg_batch* b);
 CKG_API int ckg_batch_autotune(ckg_batch* b, int32_t reps, int32_t* trials, int32_t max_trials, int32_t* n_trials);
