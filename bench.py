@@ -939,6 +939,8 @@ def main():
     ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
     ap.add_argument("--no-mlp", action="store_true")
+    ap.add_argument("--ntt", default="plain", choices=["tma", "plain"],
+                    help="NTT column passes: per-tile (plain, the default) or persistent TMA-staged (tma)")
     ap.add_argument("--bconv", default="auto", choices=["auto", "tc", "int"],
                     help="base conversion engine: tensor cores from 6 sources (auto, the default), tensor cores "
                          "at every source count (tc), integer kernels (int)")
@@ -1022,6 +1024,7 @@ def main():
         return
     S = Setup(ckg, torch, local)
     S.ctx.bconv_tc = {"int": 0, "auto": 1, "tc": 2}[args.bconv]
+    S.ctx.ntt_tma = args.ntt == "tma"
     if args.serve_only:
         sv = BootServing(ckg, torch, local)
         out = sv.measure(args.serve_requests)
@@ -1114,7 +1117,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64",
                 "data": "synthetic (seeded uniform ciphertexts and plaintexts, uniform key material)",
-                "config": dict(config, key_switches_per_step=int(mix.ks), bconv=args.bconv,
+                "config": dict(config, key_switches_per_step=int(mix.ks), bconv=args.bconv, ntt=args.ntt,
                                autotune={"ntt_wave": tuning["ntt_wave"], "chunk_items": tuning["chunk_items"],
                                          "trials_ms": [[w, c, round(m, 3)] for w, c, m in tuning["trials"]]}),
                 "e2e": e2e,

@@ -387,25 +387,29 @@ void Batch::issue() {
   Context& c = *ctx_;
   const unsigned char* base = (const unsigned char*)desc_->p;
   auto at = [&](const List& l) { return base + l.off; };
+  // every limb a column pass reads is in the scratch, carved in whole limbs
+  const LimbRegion reg{scratch_->p, scratch_->words / c.n};
+  const LimbRegion* rg = scratch_->p ? &reg : nullptr;
   for (Stage* S : chunks_) {
     launch_tensor_ptr(c.dt, (const TensorRef*)at(S->tensor), S->tensor.count, c.stream);
     launch_binary_ptr(c.dt, (const BinRef*)at(S->pmul), S->pmul.count, 2, c.stream);
     launch_gather_ptr(c.dt, (const GatherRef*)at(S->gather), S->gather.count, c.stream);
-    if (S->intt_in.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_in), S->intt_in.count, true, c.stream);
+    if (S->intt_in.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_in), S->intt_in.count, true, c.stream, rg);
     for (size_t g = 0; g < S->modup.size(); ++g)
       launch_bconv_ptr(c.dt, (const ConvJob*)at(S->modup[g].second), S->modup[g].second.count, S->modup[g].first,
                        c.stream, S->modup_dst[g]);
-    if (S->fwd_conv.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->fwd_conv), S->fwd_conv.count, false, c.stream);
+    if (S->fwd_conv.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->fwd_conv), S->fwd_conv.count, false, c.stream, rg);
     launch_inner_product_ptr(c.dt, (int)c.alpha, (int)c.L, (int)c.k, (const IpJob*)at(S->ip), S->ip.count,
                              S->ip_max_limbs, c.stream);
-    if (S->intt_p.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_p), S->intt_p.count, true, c.stream);
+    if (S->intt_p.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_p), S->intt_p.count, true, c.stream, rg);
     launch_bconv_ptr(c.dt, (const ConvJob*)at(S->md_conv), S->md_conv.count, (int)c.k, c.stream, S->md_dst);
     launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_md), (const FinRef*)at(S->fin_ks), S->fin_ks.count,
-                          c.stream);
-    if (S->intt_last.count) launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_last), S->intt_last.count, true, c.stream);
+                          c.stream, rg);
+    if (S->intt_last.count)
+      launch_ntt_ptr(c.dt, (const LimbRef*)at(S->intt_last), S->intt_last.count, true, c.stream, rg);
     launch_bconv_ptr(c.dt, (const ConvJob*)at(S->rs_conv), S->rs_conv.count, 1, c.stream, S->rs_dst);
     launch_ntt_finish_ptr(c.dt, (const LimbRef*)at(S->fwd_rs), (const FinRef*)at(S->fin_rs), S->fin_rs.count,
-                          c.stream);
+                          c.stream, rg);
   }
 }
 

@@ -618,6 +618,14 @@ int ckg_ctx_set_bconv_tc(ckg_ctx* ctx, int32_t on) {
 
 int32_t ckg_ctx_bconv_tc(ckg_ctx* ctx) { return ctx && ctx->c ? ctx->c->dt.bconv_tc : -1; }
 
+int ckg_ctx_set_ntt_tma(ckg_ctx* ctx, int32_t on) {
+  CKG_API_BEGIN
+  ctx_of(ctx).dt.ntt_tma = on ? 1 : 0;
+  CKG_API_END
+}
+
+int32_t ckg_ctx_ntt_tma(ckg_ctx* ctx) { return ctx && ctx->c ? ctx->c->dt.ntt_tma : -1; }
+
 int ckg_batch_set_chunk_items(ckg_batch* b, int32_t items) {
   CKG_API_BEGIN
   if (items < 1) throw Error(CKG_INVALID_PARAMS, "chunk size must be positive");

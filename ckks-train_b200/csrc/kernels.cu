@@ -6,6 +6,8 @@
 // 2^50, which run exactly on the FP64 pipe (see kF64Bound), and the overflow estimate of
 // exact base conversion, done with __dmul_rn / __dadd_rn so that no multiply-add is
 // contracted (crates/ckks-train-core/src/baseconv.rs:198-206).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -147,16 +149,20 @@ CKG_DEV uint64_t centred_lift(uint64_t x, uint64_t ql, uint64_t q, uint64_t one_
 }
 
 // Forward column pass: stages 0..LOGS-1 on 2^LOGS-point columns (stride 256).
+// Column block `cb` (columns cb * 16 ..); with `tile` the input columns are read from that
+// shared-memory copy ([row][16] words, the same buffer as `sm`) instead of ref.src: every thread
+// writes its exchange words where it read its inputs, so no barrier is needed between the two.
 template <int LOGS, bool LAZY>
 CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roots, uint64_t* sm, uint64_t lift_q,
-                           uint64_t one_s) {
+                           uint64_t one_s, int cb, const uint64_t* tile) {
   constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
   const uint64_t two_q = 2 * q;
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
-  const int col = blockIdx.x * kCols + c;
+  const int col = cb * kCols + c;
   uint64_t x[1 << E1];
 #pragma unroll
-  for (int j = 0; j < (1 << E1); ++j) x[j] = ref.src[col + (size_t)kRow * (ts + TPS * j)];
+  for (int j = 0; j < (1 << E1); ++j)
+    x[j] = tile ? tile[(ts + TPS * j) * kCols + c] : ref.src[col + (size_t)kRow * (ts + TPS * j)];
   if (lift_q) {
 #pragma unroll
     for (int j = 0; j < (1 << E1); ++j) x[j] = centred_lift(x[j], lift_q, q, one_s);
@@ -195,20 +201,20 @@ CKG_DEV void fwd_cols_body(const LimbRef& ref, uint64_t q, const ulonglong2* roo
 // The same pass with FP64 butterflies; writes the raw doubles for the row pass.
 template <int LOGS>
 CKG_DEV void fwd_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm,
-                               uint64_t lift_q) {
+                               uint64_t lift_q, int cb, const uint64_t* tile) {
   constexpr int E1 = (LOGS + 1) / 2, E2 = LOGS / 2, TPS = 1 << E2, V = 1 << (E1 - E2);
   const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
-  const int col = blockIdx.x * kCols + c;
+  const int col = cb * kCols + c;
   double x[1 << E1];
+  auto in = [&](int j) { return tile ? tile[(ts + TPS * j) * kCols + c] : ref.src[col + (size_t)kRow * (ts + TPS * j)]; };
   if (lift_q) {
     const uint64_t qi = __ldg(&P->q), one_s = __ldg(&P->one_s);
 #pragma unroll
-    for (int j = 0; j < (1 << E1); ++j)
-      x[j] = f64_of(centred_lift(ref.src[col + (size_t)kRow * (ts + TPS * j)], lift_q, qi, one_s));
+    for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(centred_lift(in(j), lift_q, qi, one_s));
   } else {
 #pragma unroll
-    for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(ref.src[col + (size_t)kRow * (ts + TPS * j)]);
+    for (int j = 0; j < (1 << E1); ++j) x[j] = f64_of(in(j));
   }
 #pragma unroll
   for (int r = 0; r < E1; ++r) {
@@ -257,13 +263,13 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
   if (in_place && !ref.aux) ref.src = ref.dst;
   const uint64_t q = __ldg(&pc[ref.prime].q);
   if (q < kF64Bound) {
-    fwd_cols_body_f64<LOGS>(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), sm, lift_q);
+    fwd_cols_body_f64<LOGS>(ref, pc + ref.prime, twd + ((size_t)ref.prime << log_n), sm, lift_q, blockIdx.x, nullptr);
     return;
   }
   const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   const uint64_t one_s = __ldg(&pc[ref.prime].one_s);
-  if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm, lift_q, one_s);
-  else fwd_cols_body<LOGS, false>(ref, q, roots, sm, lift_q, one_s);
+  if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, sm, lift_q, one_s, blockIdx.x, nullptr);
+  else fwd_cols_body<LOGS, false>(ref, q, roots, sm, lift_q, one_s, blockIdx.x, nullptr);
 }
 
 // Forward row pass: stages s0..s0+7 (s0 = logN - 8) on 256-point rows, final reduction.
@@ -563,14 +569,16 @@ __global__ void __launch_bounds__(256, 4)
 // Inverse column pass with FP64 butterflies over the raw doubles of the row pass; N^-1 in
 // the last stage, canonical output.
 template <int LOGS>
-CKG_DEV void inv_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm) {
+CKG_DEV void inv_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const double* roots, uint64_t* sm, int cb,
+                               const uint64_t* tile) {
   constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
   const double q = __ldg(&P->qd), qinv = __ldg(&P->qinv);
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
-  const int col = blockIdx.x * kCols + c;
+  const int col = cb * kCols + c;
   double x[1 << F1];
 #pragma unroll
-  for (int j = 0; j < (1 << F1); ++j) x[j] = bits_dbl(ref.src[col + (size_t)kRow * ((ts << F1) + j)]);
+  for (int j = 0; j < (1 << F1); ++j)
+    x[j] = bits_dbl(tile ? tile[((ts << F1) + j) * kCols + c] : ref.src[col + (size_t)kRow * ((ts << F1) + j)]);
 #pragma unroll
   for (int v = 0; v < F1; ++v) {
     const int d = 1 << v;
@@ -616,26 +624,18 @@ CKG_DEV void inv_cols_body_f64(const LimbRef& ref, const PrimeConst* P, const do
   }
 }
 
-template <int LOGS, class B>
-__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
-    k_ntt_inv_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
-                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
+// The inverse column pass with integer butterflies (primes from 2^50 on).
+template <int LOGS>
+CKG_DEV void inv_cols_body(const LimbRef& ref, const PrimeConst* P, const ulonglong2* roots, uint64_t* sm, int cb,
+                           const uint64_t* tile) {
   constexpr int F1 = (LOGS + 1) / 2, F2 = LOGS / 2, TPS = 1 << F2, V = 1 << (F1 - F2);
-  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
-  LimbRef ref = b.r[blockIdx.y];
-  if (in_place) ref.src = ref.dst;
-  const PrimeConst* P = pc + ref.prime;
-  if (__ldg(&P->q) < kF64Bound) {
-    inv_cols_body_f64<LOGS>(ref, P, twd + ((size_t)ref.prime << log_n), sm);
-    return;
-  }
   const uint64_t q = __ldg(&P->q), two_q = 2 * q;
-  const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
   const int c = threadIdx.x % kCols, ts = threadIdx.x / kCols;
-  const int col = blockIdx.x * kCols + c;
+  const int col = cb * kCols + c;
   uint64_t x[1 << F1];
 #pragma unroll
-  for (int j = 0; j < (1 << F1); ++j) x[j] = ref.src[col + (size_t)kRow * ((ts << F1) + j)];
+  for (int j = 0; j < (1 << F1); ++j)
+    x[j] = tile ? tile[((ts << F1) + j) * kCols + c] : ref.src[col + (size_t)kRow * ((ts << F1) + j)];
   // local stage v: pair distance 2^v, twiddle index 2^(LOGS-1-v) + (k >> (v+1))
 #pragma unroll
   for (int v = 0; v < F1; ++v) {
@@ -681,6 +681,137 @@ __global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
 #pragma unroll
     for (int j = 0; j < (1 << F2); ++j) ref.dst[col + (size_t)kRow * (t2 + (j << F1))] = y[j];
   }
+}
+
+template <int LOGS, class B>
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 4 : 1)
+    k_ntt_inv_cols(const __grid_constant__ B b, const PrimeConst* __restrict__ pc,
+                   const ulonglong2* __restrict__ tw, const double* __restrict__ twd, int log_n, int in_place) {
+  extern __shared__ uint64_t sm[];  // [2^LOGS][kCols]
+  LimbRef ref = b.r[blockIdx.y];
+  if (in_place) ref.src = ref.dst;
+  const PrimeConst* P = pc + ref.prime;
+  if (__ldg(&P->q) < kF64Bound) inv_cols_body_f64<LOGS>(ref, P, twd + ((size_t)ref.prime << log_n), sm, blockIdx.x, nullptr);
+  else inv_cols_body<LOGS>(ref, P, tw + ((size_t)ref.prime << log_n), sm, blockIdx.x, nullptr);
+}
+
+// ------------------------------------------------------------------------------------
+// Persistent column passes with TMA staging. Each CTA walks the list's (limb, column block)
+// tiles with a stride of the grid. A tile (2^LOGS rows of 16 words, 128 bytes apart from row to
+// row by 2 KB) is one box of a 3-D tensor map over the list's region (256 columns x 2^LOGS rows x
+// limbs, a limb being N words): a single cp.async.bulk.tensor copy brings it into shared memory,
+// completing on the stage's mbarrier, two stages deep, so the next tile is in flight while one is
+// transformed and a stage is refilled as soon as its tile is done. The stage buffer is also the
+// pass's exchange buffer. Waits are bounded (about a second of clock): on timeout the kernel
+// records a fault (g_ntt_fault = 1), drains its copies (bounded) and returns; a limb outside the
+// map's region is not copied and records fault 3 (the host checks every list first).
+// ------------------------------------------------------------------------------------
+
+__device__ int g_ntt_fault;
+
+CKG_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+CKG_DEV void mbar_init1(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+CKG_DEV bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > (2LL << 30)) {
+      atomicExch(&g_ntt_fault, 1);
+      return false;
+    }
+  }
+}
+CKG_DEV void mbar_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Box (x, y, z) of a 3-D tensor map into shared memory (no multicast).
+CKG_DEV void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int LOGS, bool INV, class B>
+__global__ void __launch_bounds__(kCols * (1 << (LOGS / 2)), LOGS <= 8 ? 3 : 1)
+    k_ntt_cols_tma(const __grid_constant__ B b, const __grid_constant__ CUtensorMap map, const uint64_t* base,
+                   uint64_t region_limbs, const PrimeConst* __restrict__ pc, const ulonglong2* __restrict__ tw,
+                   const double* __restrict__ twd, int log_n, int in_place, int items) {
+  constexpr int TILE = (1 << LOGS) * kCols;  // words per stage
+  constexpr int NBLK = kRow / kCols;         // column blocks per limb
+  extern __shared__ __align__(128) uint64_t smt[];
+  uint64_t* bars = smt + 2 * TILE;
+  __shared__ int stage_ok[2];
+  auto source = [&](const LimbRef& r) -> const uint64_t* {
+    return (INV ? in_place : (in_place && !r.aux)) ? r.dst : r.src;
+  };
+  auto issue = [&](int item, int s) {  // by one thread
+    const uint64_t off = (uint64_t)(source(b.r[item / NBLK]) - base);
+    const uint64_t z = off >> log_n;
+    const bool ok = (off & ((1ull << log_n) - 1)) == 0 && z < region_limbs;
+    stage_ok[s] = ok;
+    if (!ok) atomicExch(&g_ntt_fault, 3);
+    mbar_expect(&bars[s], ok ? TILE * 8 : 0);
+    if (ok) tma_load_3d(smt + s * TILE, &map, (item % NBLK) * kCols, 0, (int)z, &bars[s]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init1(&bars[0]);
+    mbar_init1(&bars[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int G = gridDim.x;
+  int issued = 0;  // tiles issued by this CTA (thread 0's count)
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < items) issue(blockIdx.x, 0), ++issued;
+    if ((int)blockIdx.x + G < items) issue(blockIdx.x + G, 1), ++issued;
+  }
+  int k = 0;
+  for (int item = blockIdx.x; item < items; item += G, ++k) {
+    const int s = k & 1;
+    const bool ok = mbar_wait_bounded(&bars[s], (k >> 1) & 1);
+    if (__syncthreads_or(!ok)) break;
+    uint64_t* tile = smt + s * TILE;
+    if (stage_ok[s]) {
+      LimbRef ref = b.r[item / NBLK];
+      ref.src = source(ref);
+      const int cb = item % NBLK;
+      const PrimeConst* P = pc + ref.prime;
+      const uint64_t q = __ldg(&P->q);
+      if (!INV) {
+        const uint64_t lift_q = ref.aux ? __ldg(&pc[ref.aux - 1].q) : 0;
+        if (q < kF64Bound) {
+          fwd_cols_body_f64<LOGS>(ref, P, twd + ((size_t)ref.prime << log_n), tile, lift_q, cb, tile);
+        } else {
+          const ulonglong2* roots = tw + ((size_t)ref.prime << log_n);
+          const uint64_t one_s = __ldg(&P->one_s);
+          if (q < kLazyBound) fwd_cols_body<LOGS, true>(ref, q, roots, tile, lift_q, one_s, cb, tile);
+          else fwd_cols_body<LOGS, false>(ref, q, roots, tile, lift_q, one_s, cb, tile);
+        }
+      } else {
+        if (q < kF64Bound) inv_cols_body_f64<LOGS>(ref, P, twd + ((size_t)ref.prime << log_n), tile, cb, tile);
+        else inv_cols_body<LOGS>(ref, P, tw + ((size_t)ref.prime << log_n), tile, cb, tile);
+      }
+    }
+    // every thread is done with the stage; its exchange writes (generic proxy) are ordered
+    // before the copy (async proxy) that refills it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0 && item + 2 * G < items) issue(item + 2 * G, s), ++issued;
+  }
+  // After a timeout, copies issued for tiles not yet waited on may still be in flight: wait
+  // for them (bounded) before the shared memory is released.
+  if (threadIdx.x == 0)
+    for (int kk = k; kk < issued; ++kk) mbar_wait_bounded(&bars[kk & 1], (kk >> 1) & 1);
 }
 
 // Small transforms (logN <= 11): one CTA per limb, the limb in shared memory, radix-2.
@@ -1201,8 +1332,86 @@ void set_smem(T* fn, int bytes) {
   cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+// The tensor map of a region of `limbs` limbs (N words each) from `base`: 256 columns x N/256
+// rows x limbs, boxes of 16 columns x all rows x one limb.
+bool limb_tensor_map(CUtensorMap* map, const uint64_t* base, uint64_t limbs, int log_n) {
+  auto enc = tensor_map_encoder();
+  if (!enc || log_n < 12 || log_n > 16 || ((uintptr_t)base & 15)) return false;
+  const cuuint32_t rows = 1u << (log_n - kRowLog);
+  cuuint64_t dims[3] = {(cuuint64_t)kRow, rows, limbs};
+  cuuint64_t strides[2] = {(cuuint64_t)kRow * 8, ((cuuint64_t)1 << log_n) * 8};
+  cuuint32_t box[3] = {(cuuint32_t)kCols, rows, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, (void*)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// The region the column pass reads of a by-value list: from its lowest source, when every source
+// lies a whole number of limbs above it.
+template <class B>
+bool list_region(const B& b, int count, int in_place, bool inverse, int log_n, LimbRegion* out) {
+  if constexpr (std::is_same<B, LimbBatch>::value) {
+    auto src = [&](const LimbRef& r) { return (inverse ? in_place : (in_place && !r.aux)) ? r.dst : r.src; };
+    const uint64_t* lo = src(b.r[0]);
+    for (int i = 1; i < count; ++i) lo = std::min(lo, (const uint64_t*)src(b.r[i]));
+    uint64_t hi = 0;
+    for (int i = 0; i < count; ++i) {
+      const uint64_t off = (uint64_t)(src(b.r[i]) - lo);
+      if (off & ((1ull << log_n) - 1)) return false;
+      hi = std::max(hi, (off >> log_n) + 1);
+    }
+    *out = LimbRegion{lo, hi};
+    return true;
+  }
+  return false;
+}
+
+template <int LOGS, bool INV, class B>
+bool launch_cols_tma(const B& b, int count, const DevTables& d, int in_place, cudaStream_t st, LimbRegion reg) {
+  CUtensorMap map;
+  if (!limb_tensor_map(&map, reg.base, reg.limbs, d.log_n)) return false;
+  const int smem = 2 * (1 << LOGS) * kCols * 8 + 16;
+  const int threads = kCols * (1 << (LOGS / 2));
+  auto fn = k_ntt_cols_tma<LOGS, INV, B>;
+  set_smem(fn, smem);
+  static const int per_sm = [&] {
+    int v = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, threads, smem);
+    return v > 0 ? v : 1;
+  }();
+  const int items = count * (kRow / kCols);
+  const int grid = std::min(items, std::max(1, d.sms) * per_sm);
+  fn<<<grid, threads, smem, st>>>(b, map, reg.base, reg.limbs, d.prime, INV ? d.tw_inv : d.tw_fwd,
+                                  INV ? d.twd_inv : d.twd_fwd, d.log_n, in_place, items);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return true;
+}
+
 template <int LOGS, class B>
-void launch_cols(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st) {
+void launch_cols(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st,
+                 const LimbRegion* region) {
+  if (d.ntt_tma && LOGS <= 8) {
+    LimbRegion reg{};
+    if (region ? (reg = *region, true) : list_region(b, count, in_place, inverse, d.log_n, &reg)) {
+      if (inverse ? launch_cols_tma<LOGS, true>(b, count, d, in_place, st, reg)
+                  : launch_cols_tma<LOGS, false>(b, count, d, in_place, st, reg))
+        return;
+    }
+  }
   const int smem = (1 << LOGS) * kCols * 8;
   const int threads = kCols * (1 << (LOGS / 2));
   dim3 grid(kRow / kCols, count);
@@ -1217,21 +1426,23 @@ void launch_cols(bool inverse, const B& b, int count, const DevTables& d, int in
 }
 
 template <class B>
-void launch_cols_any(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st) {
+void launch_cols_any(bool inverse, const B& b, int count, const DevTables& d, int in_place, cudaStream_t st,
+                     const LimbRegion* region = nullptr) {
   switch (d.log_n - kRowLog) {
-    case 4: launch_cols<4>(inverse, b, count, d, in_place, st); break;
-    case 5: launch_cols<5>(inverse, b, count, d, in_place, st); break;
-    case 6: launch_cols<6>(inverse, b, count, d, in_place, st); break;
-    case 7: launch_cols<7>(inverse, b, count, d, in_place, st); break;
-    case 8: launch_cols<8>(inverse, b, count, d, in_place, st); break;
-    case 9: launch_cols<9>(inverse, b, count, d, in_place, st); break;
+    case 4: launch_cols<4>(inverse, b, count, d, in_place, st, region); break;
+    case 5: launch_cols<5>(inverse, b, count, d, in_place, st, region); break;
+    case 6: launch_cols<6>(inverse, b, count, d, in_place, st, region); break;
+    case 7: launch_cols<7>(inverse, b, count, d, in_place, st, region); break;
+    case 8: launch_cols<8>(inverse, b, count, d, in_place, st, region); break;
+    case 9: launch_cols<9>(inverse, b, count, d, in_place, st, region); break;
     default: break;
   }
 }
 
 // Both passes of a batched transform: src -> dst, then dst in place.
 template <class B>
-void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStream_t st) {
+void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStream_t st,
+                const LimbRegion* region = nullptr) {
   if (count == 0) return;
   if (d.log_n <= 11) {
     const int n = 1 << d.log_n;
@@ -1242,11 +1453,11 @@ void ntt_passes(const DevTables& d, const B& b, int count, bool inverse, cudaStr
   }
   const dim3 rgrid((1 << d.log_n) / (kRow * kRowsPerCta), count);
   if (!inverse) {
-    launch_cols_any(false, b, count, d, 0, st);
+    launch_cols_any(false, b, count, d, 0, st, region);
     k_ntt_fwd_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_fwd, d.twd_fwd, d.log_n, 1);
   } else {
     k_ntt_inv_rows<B><<<rgrid, 256, 0, st>>>(b, d.prime, d.tw_inv, d.twd_inv, d.log_n, 0);
-    launch_cols_any(true, b, count, d, 1, st);
+    launch_cols_any(true, b, count, d, 1, st, region);
   }
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
@@ -1290,11 +1501,12 @@ void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse
 
 // Device lists go in waves of d.ntt_wave limbs: a wave's column pass and row pass run back to
 // back, so the intermediate limbs can stay in L2 between them.
-void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st) {
+void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st,
+                    const LimbRegion* region) {
   const int wave = d.ntt_wave > 0 ? d.ntt_wave : count;
   for (int off = 0; off < count; off += wave) {
     const int c = std::min(wave, count - off);
-    ntt_passes(d, LimbPtrs{c, 0, dev_refs + off}, c, inverse, st);
+    ntt_passes(d, LimbPtrs{c, 0, dev_refs + off}, c, inverse, st, region);
   }
 }
 
@@ -1373,7 +1585,7 @@ void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaSt
 }
 
 void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const FinRef* dev_fin, int count,
-                           cudaStream_t st) {
+                           cudaStream_t st, const LimbRegion* region) {
   if (!count) return;
   if (d.log_n <= 11) {
     launch_ntt_ptr(d, dev_cols, count, false, st);
@@ -1383,7 +1595,7 @@ void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const Fi
   const int wave = d.ntt_wave > 0 ? d.ntt_wave : count;
   for (int off = 0; off < count; off += wave) {
     const int c = std::min(wave, count - off);
-    launch_cols_any(false, LimbPtrs{c, 0, dev_cols + off}, c, d, 1, st);
+    launch_cols_any(false, LimbPtrs{c, 0, dev_cols + off}, c, d, 1, st, region);
     k_ntt_fwd_rows_finish<FinPtrs><<<dim3((1 << d.log_n) / (kRow * kRowsPerCta), c), 256, 0, st>>>(
         FinPtrs{c, 0, dev_fin + off}, d.prime, d.tw_fwd, d.twd_fwd, d.log_n);
     g_launches.fetch_add(1, std::memory_order_relaxed);

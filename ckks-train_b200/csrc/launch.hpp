@@ -21,6 +21,15 @@ struct DevTables {
   int log_n;
   int ntt_wave;  // limbs per column + row launch pair of device-list transforms (0: all at once)
   int bconv_tc;  // tensor-core conversions (<= 8 sources, <= 32 targets): 0 off, 1 from 6 sources, 2 all
+  int ntt_tma;   // nonzero: NTT column passes run persistent with TMA-staged tiles (tensor maps)
+  int sms;       // streaming multiprocessors of the device
+};
+
+// A device region holding whole limbs (N words each) from `base`: the TMA-staged column passes
+// read the limbs of a list through one tensor map over it.
+struct LimbRegion {
+  const uint64_t* base;
+  uint64_t limbs;
 };
 
 void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st);
@@ -34,7 +43,7 @@ void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream
 void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st,
                        const LimbRef* cols = nullptr);
 void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const FinRef* dev_fin, int count,
-                           cudaStream_t st);
+                           cudaStream_t st, const LimbRegion* region = nullptr);
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st);
 void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
                   const uint32_t* perm, cudaStream_t st);
@@ -42,7 +51,9 @@ void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, co
 void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st);
 
 // The same kernels over work lists resident in device memory (one launch each).
-void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st);
+// `region`: every limb the column passes read lies in it (enables the TMA-staged passes).
+void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool inverse, cudaStream_t st,
+                    const LimbRegion* region = nullptr);
 // max_dst: the largest job's target count (0: unknown, the integer kernel runs).
 void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, int n_src, cudaStream_t st,
                       int max_dst = 0);

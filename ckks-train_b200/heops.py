@@ -172,6 +172,9 @@ def _declare(L):
     L.ckg_ctx_bconv_tc.argtypes = [VP]
     L.ckg_ctx_bconv_tc.restype = C.c_int32
     L.ckg_device_fault.argtypes = [VP, C.POINTER(C.c_int32)]
+    L.ckg_ctx_set_ntt_tma.argtypes = [VP, C.c_int32]
+    L.ckg_ctx_ntt_tma.argtypes = [VP]
+    L.ckg_ctx_ntt_tma.restype = C.c_int32
     L.ckg_batch_set_chunk_items.argtypes = [VP, C.c_int32]
     L.ckg_batch_chunk_items.argtypes = [VP]
     L.ckg_batch_chunk_items.restype = C.c_int32
@@ -329,6 +332,16 @@ class Context:
     @bconv_tc.setter
     def bconv_tc(self, mode):
         _check(lib().ckg_ctx_set_bconv_tc(self.h, int(mode)))
+
+    @property
+    def ntt_tma(self):
+        """True when NTT column passes run persistent with TMA-staged tiles (bit-neutral; off by
+        default, measured slower than the per-tile passes at N = 2^16)."""
+        return lib().ckg_ctx_ntt_tma(self.h) == 1
+
+    @ntt_tma.setter
+    def ntt_tma(self, on):
+        _check(lib().ckg_ctx_set_ntt_tma(self.h, 1 if on else 0))
 
     def device_fault(self):
         """Reads and clears the device fault word (0: none)."""

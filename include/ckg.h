@@ -266,6 +266,13 @@ CKG_API int32_t ckg_ctx_ntt_wave(ckg_ctx* ctx);
  * 0 never. Setting 1 or 2 on a context that does not qualify fails with CKG_INVALID_PARAMS. */
 CKG_API int ckg_ctx_set_bconv_tc(ckg_ctx* ctx, int32_t on);
 CKG_API int32_t ckg_ctx_bconv_tc(ckg_ctx* ctx);
+/* NTT column-pass staging of a context (bit-neutral; no reference counterpart). 1: persistent
+ * column passes whose tiles reach shared memory as one box of a 3-D tensor map per tile
+ * (cp.async.bulk.tensor), two stages deep; lists whose limbs do not all lie whole limbs apart
+ * in one region take the per-tile kernels. 0 (the default, measured faster at N = 2^16): per-tile
+ * kernels that load their tile with ordinary loads. */
+CKG_API int ckg_ctx_set_ntt_tma(ckg_ctx* ctx, int32_t on);
+CKG_API int32_t ckg_ctx_ntt_tma(ckg_ctx* ctx);
 /* Reads and clears the device fault word of the context's device: 0 when no kernel recorded a
  * fault, 1 when a kernel's bounded wait ran out (it freed its tensor memory and returned without
  * its results), 2 when a conversion table lacked its tensor-core block; ckg_ctx_sync also checks

@@ -165,3 +165,69 @@ def test_mod_down_near_ties(pair):
         ctx.mod_down(ptr(dq), level, ptr(dp), ptr(out))
         ctx.sync()
         assert_same(from_dev(out), P.mod_down(q, p), f"near-tie mod_down level {level}")
+
+
+def test_conversion_engines(pair):
+    """ModUp and ModDown with the base conversions on the tensor cores (exact u8 x u8 -> s32
+    products, FP64-quotient reduction) and on the integer kernels: both give the oracle's words,
+    on random and near-tie inputs and on all-(q-1) limbs (largest partial sums)."""
+    P, ctx = pair
+    L = P.max_level
+    default = ctx.bconv_tc
+    engines = [0, 2] if default else [0]  # integer kernels; tensor cores at every source count
+    try:
+        for tc in engines:
+            ctx.bconv_tc = tc
+            for level in sorted({L, L // 2, 0}):
+                for kind in ("random", "ties", "max"):
+                    if kind == "random":
+                        x = P.random_q(6000 + level, level)
+                        p = P.random_p(6100 + level)
+                    elif kind == "ties":
+                        x = P.ntt(near_tie_limbs(P.q[: level + 1], P.n))
+                        p = P.ntt(near_tie_limbs(P.p, P.n), basis=1)
+                    else:
+                        x = np.stack([np.full(P.n, q - 1, np.uint64) for q in P.q[: level + 1]])
+                        p = np.stack([np.full(P.n, q - 1, np.uint64) for q in P.p])
+                    dx, dp = to_dev(x), to_dev(p)
+                    what = f"engine {'tc' if tc else 'int'} level {level} {kind}"
+                    for j in range(len(P.digit_ranges(level))):
+                        oq, op_ = empty_dev((level + 1, P.n)), empty_dev((P.np_, P.n))
+                        ctx.mod_up(ptr(dx), level, j, ptr(oq), ptr(op_))
+                        ctx.sync()
+                        wq, wp = P.mod_up(x, j)
+                        assert_same(from_dev(oq), wq, f"mod_up Q {what} digit {j}")
+                        assert_same(from_dev(op_), wp, f"mod_up P {what} digit {j}")
+                    out = empty_dev(x.shape)
+                    ctx.mod_down(ptr(dx), level, ptr(dp), ptr(out))
+                    ctx.sync()
+                    assert_same(from_dev(out), P.mod_down(x, p), f"mod_down {what}")
+        assert ctx.device_fault() == 0
+    finally:
+        ctx.bconv_tc = default
+
+
+def test_ntt_tma_staging(pair):
+    """The opt-in TMA-staged column passes (one tensor-map box per tile, two stages deep) give the
+    per-tile kernels' words: forward and inverse over every prime, in place and out of place."""
+    P, ctx = pair
+    if P.n < (1 << 12):
+        pytest.skip("two-pass transforms only")
+    primes = list(range(len(ctx.primes)))
+    allp = ctx.primes
+    x = np.stack([oracle_rand(P, 211 + i, allp[i]) for i in primes])
+    want_f = np.stack([P.ntt(x[i:i + 1], first_prime=i if i < P.nq else i - P.nq, basis=0 if i < P.nq else 1)[0]
+                       for i in primes])
+    try:
+        ctx.ntt_tma = True
+        d = to_dev(x)
+        out = empty_dev(x.shape)
+        ctx.ntt(ptr(d), ptr(out), primes, inverse=False)
+        ctx.sync()
+        assert_same(from_dev(out), want_f, "forward NTT, TMA-staged columns")
+        ctx.ntt(ptr(out), ptr(out), primes, inverse=True)
+        ctx.sync()
+        assert_same(from_dev(out), x, "inverse NTT in place, TMA-staged columns")
+        assert ctx.device_fault() == 0
+    finally:
+        ctx.ntt_tma = False
