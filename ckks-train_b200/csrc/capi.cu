@@ -540,6 +540,48 @@ int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* cons
   CKG_API_END
 }
 
+}  // extern "C"
+
+namespace {
+template <class T, class H, class F>
+std::vector<MatvecJob<T>> matvec_jobs(uint32_t njobs, const uint32_t* d, const uint32_t* stride, const H* const* entries,
+                                      const ckg_ct* const* xs, F entry) {
+  if (njobs && (!d || !stride || !entries || !xs)) throw Error(CKG_INVALID_PARAMS, "null job arrays");
+  std::vector<MatvecJob<T>> jobs(njobs);
+  size_t off = 0;
+  for (uint32_t i = 0; i < njobs; ++i) {
+    jobs[i].d = d[i];
+    jobs[i].stride = stride[i];
+    for (uint32_t k = 0; k < d[i]; ++k) jobs[i].entries.push_back(entries[off + k] ? entry(entries[off + k]) : nullptr);
+    off += d[i];
+    jobs[i].x = ct_of(xs[i]);
+  }
+  return jobs;
+}
+}  // namespace
+
+extern "C" {
+
+int ckg_matvec_enc_batch(ckg_eval* ev, uint32_t njobs, const uint32_t* d, const uint32_t* stride,
+                         const ckg_ct* const* entries, const ckg_ct* const* xs, ckg_ct** outs) {
+  CKG_API_BEGIN
+  auto jobs = matvec_jobs<Ct>(njobs, d, stride, entries, xs, [](const ckg_ct* e) { return e->c; });
+  auto v = ev_of(ev).matvec_enc_batch(jobs);
+  check_launch();
+  for (size_t i = 0; i < v.size(); ++i) outs[i] = new ckg_ct{v[i]};
+  CKG_API_END
+}
+
+int ckg_matvec_plain_batch(ckg_eval* ev, uint32_t njobs, const uint32_t* d, const uint32_t* stride,
+                           const ckg_pt* const* entries, const ckg_ct* const* xs, ckg_ct** outs) {
+  CKG_API_BEGIN
+  auto jobs = matvec_jobs<Pt>(njobs, d, stride, entries, xs, [](const ckg_pt* e) { return e->p; });
+  auto v = ev_of(ev).matvec_plain_batch(jobs);
+  check_launch();
+  for (size_t i = 0; i < v.size(); ++i) outs[i] = new ckg_ct{v[i]};
+  CKG_API_END
+}
+
 // ---- batched execution ------------------------------------------------------------------
 
 static Batch& batch_of(ckg_batch* b) {

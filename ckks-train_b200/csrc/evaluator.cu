@@ -540,6 +540,10 @@ Ct Evaluator::bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, c
         std::vector<std::pair<Ct, Pt>> prods;
         for (uint32_t k2 = 0; k2 < baby; ++k2) prods.push_back({xs[k2], entries[k1 * baby + k2]});
         inner = mac_plain(prods);
+      } else if (cfg_.lazy_relin) {  // encrypted diagonals, products unrelinearized: one fused pass
+        std::vector<std::pair<Ct, Ct>> prods;
+        for (uint32_t k2 = 0; k2 < baby; ++k2) prods.push_back({entries[k1 * baby + k2], xs[k2]});
+        inner = mac_tensor(prods);
       } else {
         for (uint32_t k2 = 0; k2 < baby; ++k2) {
           Ct t = mul(entries[k1 * baby + k2], xs[k2]);
@@ -554,18 +558,16 @@ Ct Evaluator::bsgs(uint32_t d, uint32_t stride, const std::vector<T>& entries, c
   return acc;
 }
 
-Ct Evaluator::matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x) {
+void Evaluator::check_matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x) const {
   check_diagonals(*ctx_, d, stride, entries);
   check_galois_input(x);                       // linalg.rs:608-622
   for (auto& p : entries) check_basis_pt(p);
   for (auto& p : entries)
     if (p->level != x->level) throw Error(ST_LEVEL_MISMATCH, "level mismatch");
   check_rotation_keys(rotation_steps(d, stride));
-  return bsgs(d, stride, entries, x, [&](const Pt& w, const Ct& xr) { return mul_plain(xr, w); },
-              [](const Ct& c) { return c; });
 }
 
-Ct Evaluator::matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x) {
+void Evaluator::check_matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x) const {
   check_diagonals(*ctx_, d, stride, entries);
   check_galois_input(x);                       // linalg.rs:642-678
   for (auto& c : entries) check_galois_input(c);
@@ -574,11 +576,226 @@ Ct Evaluator::matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& ent
   check_rotation_keys(rotation_steps(d, stride));
   if (x->level == 0) throw Error(ST_NO_LEVELS_LEFT, "no levels left");
   relin_key_checked();
+}
+
+Ct Evaluator::matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x) {
+  check_matvec_plain(d, stride, entries, x);
+  return bsgs(d, stride, entries, x, [&](const Pt& w, const Ct& xr) { return mul_plain(xr, w); },
+              [](const Ct& c) { return c; });
+}
+
+Ct Evaluator::matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x) {
+  check_matvec_enc(d, stride, entries, x);
   if (cfg_.lazy_relin)
     return bsgs(d, stride, entries, x, [&](const Ct& w, const Ct& xr) { return mul_no_relin(w, xr); },
                 [&](const Ct& c) { return relinearize(c); });
   return bsgs(d, stride, entries, x, [&](const Ct& w, const Ct& xr) { return mul(w, xr); },
               [](const Ct& c) { return c; });
+}
+
+Ct Evaluator::mac_tensor(const std::vector<std::pair<Ct, Ct>>& terms) {
+  const Ct& a0 = terms[0].first;
+  const uint32_t level = a0->level;
+  ctx_->activate();
+  Ct acc;
+  for (size_t first = 0; first < terms.size(); first += kMaxMacTensorTerms) {
+    const size_t cnt = std::min<size_t>(kMaxMacTensorTerms, terms.size() - first);
+    Ct r = new_ct(3, level, a0->scale * terms[0].second->scale);
+    MacTensorBatch b{};
+    b.count = (int)cnt;
+    b.limbs = (int)level + 1;
+    b.out0 = r->comp_mut(0);
+    b.out1 = r->comp_mut(1);
+    b.out2 = r->comp_mut(2);
+    for (size_t t = 0; t < cnt; ++t) {
+      b.a0[t] = terms[first + t].first->comp(0);
+      b.a1[t] = terms[first + t].first->comp(1);
+      b.b0[t] = terms[first + t].second->comp(0);
+      b.b1[t] = terms[first + t].second->comp(1);
+    }
+    launch_mac_tensor(ctx_->dt, b, ctx_->stream);
+    acc = acc ? add(acc, r) : r;
+  }
+  count([&](OpCounter& c) { c.ct_ct_tensor += terms.size(); });
+  return acc;
+}
+
+// The jobs' BSGS products stage by stage (the optimized configuration; operands checked): every
+// stage issues one key-switch launch sequence per level for all jobs.
+template <class T>
+std::vector<Ct> Evaluator::bsgs_batch(const std::vector<MatvecJob<T>>& jobs) {
+  constexpr bool kEnc = std::is_same<T, Ct>::value;
+  Context& c = *ctx_;
+  c.activate();
+  const size_t nj = jobs.size(), N = c.n;
+  uint64_t rotations = 0, relins = 0;
+  std::map<uint32_t, std::vector<size_t>> by_level;
+  for (size_t j = 0; j < nj; ++j) by_level[jobs[j].x->level].push_back(j);
+  // 1. the hoisted baby rotations x -> rot(x, k2 stride), one ModUp per input (evaluator.rs:572-616)
+  std::vector<std::vector<Ct>> xs(nj);
+  for (auto& kv : by_level) {
+    const uint32_t l = kv.first;
+    const size_t per = conv_limbs(c, l) * N;
+    constexpr size_t kGroup = 32;  // inputs per ModUp group (bounds the digit buffers)
+    for (size_t g0 = 0; g0 < kv.second.size(); g0 += kGroup) {
+      std::vector<size_t> need;
+      std::vector<const uint64_t*> ins;
+      for (size_t u = g0; u < std::min(kv.second.size(), g0 + kGroup); ++u) {
+        const size_t j = kv.second[u];
+        const uint32_t baby = bsgs_split(jobs[j].d).first;
+        xs[j].assign(baby, jobs[j].x);
+        bool any = false;
+        for (uint32_t k2 = 1; k2 < baby; ++k2) any = any || rotation_elt((int32_t)(k2 * jobs[j].stride)).has_value();
+        if (any) {
+          need.push_back(j);
+          ins.push_back(jobs[j].x->comp(1));
+        }
+      }
+      if (need.empty()) continue;
+      auto conv = c.alloc(need.size() * per);
+      std::vector<uint64_t*> convs;
+      for (size_t i = 0; i < need.size(); ++i) convs.push_back(conv->p + i * per);
+      mod_up_many(c, ins, l, convs);
+      std::vector<KsJob> ks;
+      for (size_t i = 0; i < need.size(); ++i) {
+        const MatvecJob<T>& jb = jobs[need[i]];
+        const uint32_t baby = bsgs_split(jb.d).first;
+        for (uint32_t k2 = 1; k2 < baby; ++k2) {
+          auto e = rotation_elt((int32_t)(k2 * jb.stride));
+          if (!e) continue;
+          const uint32_t* perm = c.perm(*e);
+          Ct r = new_ct(2, l, jb.x->scale);
+          KsJob k;
+          k.in = jb.x->comp(1);
+          k.key = &galois_key(*e);
+          k.out_b = r->comp_mut(0);
+          k.out_a = r->comp_mut(1);
+          k.add_b = jb.x->comp(0);
+          k.add_b_perm = perm;
+          k.perm = perm;
+          k.conv = convs[i];
+          ks.push_back(k);
+          xs[need[i]][k2] = r;
+          rotations++;
+        }
+      }
+      key_switch_many(c, ks, l);
+    }
+  }
+  // 2. the inner sums of every giant block (linalg.rs:659-670)
+  struct Block {
+    size_t job;
+    int64_t shift;
+    Ct v;
+  };
+  std::vector<Block> blocks;
+  for (size_t j = 0; j < nj; ++j) {
+    const auto bg = bsgs_split(jobs[j].d);
+    for (uint32_t k1 = 0; k1 < bg.second; ++k1) {
+      Ct inner;
+      if constexpr (kEnc) {
+        std::vector<std::pair<Ct, Ct>> prods;
+        for (uint32_t k2 = 0; k2 < bg.first; ++k2) prods.push_back({jobs[j].entries[k1 * bg.first + k2], xs[j][k2]});
+        inner = mac_tensor(prods);
+      } else {
+        std::vector<std::pair<Ct, Pt>> prods;
+        for (uint32_t k2 = 0; k2 < bg.first; ++k2) prods.push_back({xs[j][k2], jobs[j].entries[k1 * bg.first + k2]});
+        inner = mac_plain(prods);
+      }
+      blocks.push_back({j, (int64_t)bg.first * k1 * jobs[j].stride, inner});
+    }
+  }
+  xs.clear();
+  std::map<uint32_t, std::vector<size_t>> blocks_at;
+  for (size_t b = 0; b < blocks.size(); ++b) blocks_at[blocks[b].v->level].push_back(b);
+  // 3. relinearize every block (encrypted diagonals, lazy relinearization: evaluator.rs:441-460)
+  if constexpr (kEnc) {
+    const DevKey& rk = relin_key_checked();
+    for (auto& kv : blocks_at) {
+      std::vector<KsJob> ks;
+      std::vector<Ct> inputs;  // held until the key switches that read them are queued
+      for (size_t b : kv.second) {
+        const Ct& v = blocks[b].v;
+        Ct r = new_ct(2, v->level, v->scale);
+        KsJob k;
+        k.in = v->comp(2);
+        k.key = &rk;
+        k.out_b = r->comp_mut(0);
+        k.out_a = r->comp_mut(1);
+        k.add_b = v->comp(0);
+        k.add_a = v->comp(1);
+        ks.push_back(k);
+        inputs.push_back(v);
+        blocks[b].v = r;
+        relins++;
+      }
+      key_switch_many(c, ks, kv.first);
+    }
+  }
+  // 4. the giant rotations of the blocks (evaluator.rs:640-646, 800-805)
+  for (auto& kv : blocks_at) {
+    const uint32_t l = kv.first;
+    std::vector<size_t> rot;
+    for (size_t b : kv.second)
+      if (blocks[b].shift != 0 && rotation_elt((int32_t)blocks[b].shift)) rot.push_back(b);
+    if (rot.empty()) continue;
+    const size_t limbs = l + 1;
+    auto tmp = c.alloc(rot.size() * limbs * N);
+    std::vector<KsJob> ks;
+    std::vector<Ct> inputs;  // held until the key switches that read them are queued
+    for (size_t i = 0; i < rot.size(); ++i) {
+      Block& bl = blocks[rot[i]];
+      const uint64_t elt = *rotation_elt((int32_t)bl.shift);
+      const uint32_t* perm = c.perm(elt);
+      uint64_t* t = tmp->p + i * limbs * N;
+      std::vector<LimbRef> refs;
+      for (uint32_t q = 0; q < limbs; ++q) refs.push_back(LimbRef{bl.v->comp(1) + q * N, t + q * N, q, 0});
+      launch_unary(c.dt, refs.data(), (int)refs.size(), 3, nullptr, perm, c.stream);  // sigma_g(c1)
+      Ct r = new_ct(2, l, bl.v->scale);
+      KsJob k;
+      k.in = t;
+      k.key = &galois_key(elt);
+      k.out_b = r->comp_mut(0);
+      k.out_a = r->comp_mut(1);
+      k.add_b = bl.v->comp(0);
+      k.add_b_perm = perm;  // + sigma_g(c0)
+      ks.push_back(k);
+      inputs.push_back(bl.v);
+      bl.v = r;
+      rotations++;
+    }
+    key_switch_many(c, ks, l);
+  }
+  // 5. the sums over the giant blocks
+  std::vector<Ct> out(nj);
+  for (auto& bl : blocks) out[bl.job] = out[bl.job] ? add(out[bl.job], bl.v) : bl.v;
+  count([&](OpCounter& k) {
+    k.rotations += rotations;
+    k.relins += relins;
+  });
+  return out;
+}
+
+std::vector<Ct> Evaluator::matvec_enc_batch(const std::vector<MatvecJob<Ct>>& jobs) {
+  for (auto& j : jobs) check_matvec_enc(j.d, j.stride, j.entries, j.x);
+  if (jobs.empty()) return {};
+  if (!(cfg_.hoist && cfg_.bsgs && cfg_.lazy_relin)) {
+    std::vector<Ct> out;
+    for (auto& j : jobs) out.push_back(matvec_enc(j.d, j.stride, j.entries, j.x));
+    return out;
+  }
+  return bsgs_batch(jobs);
+}
+
+std::vector<Ct> Evaluator::matvec_plain_batch(const std::vector<MatvecJob<Pt>>& jobs) {
+  for (auto& j : jobs) check_matvec_plain(j.d, j.stride, j.entries, j.x);
+  if (jobs.empty()) return {};
+  if (!(cfg_.hoist && cfg_.bsgs)) {
+    std::vector<Ct> out;
+    for (auto& j : jobs) out.push_back(matvec_plain(j.d, j.stride, j.entries, j.x));
+    return out;
+  }
+  return bsgs_batch(jobs);
 }
 
 }  // namespace ckg

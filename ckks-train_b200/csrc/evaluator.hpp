@@ -74,6 +74,14 @@ typedef std::shared_ptr<DevKey> KeyPtr;
 std::pair<uint32_t, uint32_t> bsgs_split(uint32_t d);
 std::vector<int32_t> rotation_steps(uint32_t d, uint32_t stride);
 
+// One product of a batched BSGS call: W x with d pre-rotated diagonals at `stride` lanes.
+template <class T>
+struct MatvecJob {
+  uint32_t d = 0, stride = 1;
+  std::vector<T> entries;
+  Ct x;
+};
+
 class Evaluator {
  public:
   Evaluator(Context* ctx, KeyPtr relin, std::vector<KeyPtr> galois, EvalConfig cfg);
@@ -119,6 +127,19 @@ class Evaluator {
   // sum_t mul_plain(x_t, w_t) in one pass (operands checked by the caller: 2 components,
   // one level, equal scales); counts one ct_pt_mults per term as the separate ops would.
   Ct mac_plain(const std::vector<std::pair<Ct, Pt>>& terms);
+  // sum_t mul_no_relin(a_t, b_t) in one pass (3 components; operands checked by the caller:
+  // 2 components, one level > 0, equal scales); counts one ct_ct_tensor per term.
+  Ct mac_tensor(const std::vector<std::pair<Ct, Ct>>& terms);
+  // matvec_enc_batch (crates/ckks-train-cuda/src/evaluator.rs:437-520): every job checked as
+  // matvec_enc, in order, before any work; results and counts equal those of the jobs run one
+  // by one. With the optimized configuration the jobs run stage by stage together: all hoisted
+  // baby rotations, all inner sums, all relinearizations, all giant rotations (one key-switch
+  // launch sequence per stage and level); other configurations run the jobs one by one.
+  std::vector<Ct> matvec_enc_batch(const std::vector<MatvecJob<Ct>>& jobs);
+  // The same for plaintext diagonals (matvec_plain per job).
+  std::vector<Ct> matvec_plain_batch(const std::vector<MatvecJob<Pt>>& jobs);
+  void check_matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x) const;
+  void check_matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x) const;
 
   // BootstrapArithmetic (bootstrap/poly.rs:453-486), ModRaise (bootstrap/modraise.rs) and
   // the exact monomial product of CoeffToSlot (bootstrap/linear.rs:921-936).
@@ -150,6 +171,8 @@ class Evaluator {
   std::optional<uint64_t> rotation_elt(int32_t steps) const;
   void check_rotation_keys(const std::vector<int32_t>& steps) const;
   Ct apply_galois(const Ct& a, uint64_t elt);
+  template <class T>
+  std::vector<Ct> bsgs_batch(const std::vector<MatvecJob<T>>& jobs);
   Ct raise_level0(const Ct& a);
   template <class F>
   void count(F f) {

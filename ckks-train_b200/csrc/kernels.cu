@@ -1308,6 +1308,30 @@ __global__ void __launch_bounds__(256)
   b.out1[off] = reduce128(h1, l1, P);
 }
 
+// The same over ciphertext pairs: the three tensor components summed over the terms in 128 bits
+// (each product < 2^120, at most 2 * kMaxMacTensorTerms of them per sum), one reduction each,
+// equal to the reduced products added one by one.
+__global__ void __launch_bounds__(256)
+    k_mac_tensor(const __grid_constant__ MacTensorBatch b, const PrimeConst* __restrict__ pc, int n) {
+  const int i = blockIdx.y;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const size_t off = (size_t)i * n + c;
+  uint64_t h0 = 0, l0 = 0, h1 = 0, l1 = 0, h2 = 0, l2 = 0;
+  for (int t = 0; t < b.count; ++t) {
+    const uint64_t x0 = __ldg(b.a0[t] + off), x1 = __ldg(b.a1[t] + off);
+    const uint64_t y0 = __ldg(b.b0[t] + off), y1 = __ldg(b.b1[t] + off);
+    mac128(h0, l0, x0, y0);
+    mac128(h1, l1, x0, y1);
+    mac128(h1, l1, x1, y0);
+    mac128(h2, l2, x1, y1);
+  }
+  const PrimeConst P = pc[i];
+  b.out0[off] = reduce128(h0, l0, P);
+  b.out1[off] = reduce128(h1, l1, P);
+  b.out2[off] = reduce128(h2, l2, P);
+}
+
 // Centered lift of a level-0 coefficient-form limb (src of every ref) into prime r.prime:
 // residues above (q_0 - 1) / 2 are read as negative (poly.rs:298-345).
 __global__ void __launch_bounds__(256)
@@ -1691,6 +1715,12 @@ void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const Sca
 void launch_mac_plain(const DevTables& d, const MacBatch& b, cudaStream_t st) {
   const int n = 1 << d.log_n;
   k_mac_plain<<<dim3((n + 255) / 256, b.limbs), 256, 0, st>>>(b, d.prime, n);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+void launch_mac_tensor(const DevTables& d, const MacTensorBatch& b, cudaStream_t st) {
+  const int n = 1 << d.log_n;
+  k_mac_tensor<<<dim3((n + 255) / 256, b.limbs), 256, 0, st>>>(b, d.prime, n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 

@@ -171,6 +171,21 @@ struct MacBatch {
   const uint64_t* w[kMaxMacTerms];
 };
 
+// Fused ciphertext-ciphertext multiply-accumulate (the inner sums of BSGS with encrypted
+// diagonals): out0 = sum_t a0_t b0_t, out1 = sum_t (a0_t b1_t + a1_t b0_t), out2 = sum_t a1_t b1_t,
+// limb i at offset i * N of every base pointer, prime index i.
+constexpr int kMaxMacTensorTerms = 32;
+struct MacTensorBatch {
+  int count, limbs;
+  uint64_t* out0;
+  uint64_t* out1;
+  uint64_t* out2;
+  const uint64_t* a0[kMaxMacTensorTerms];
+  const uint64_t* a1[kMaxMacTensorTerms];
+  const uint64_t* b0[kMaxMacTensorTerms];
+  const uint64_t* b1[kMaxMacTensorTerms];
+};
+
 // Multiplication of limbs by a per-prime constant (Shoup pair per global prime index).
 constexpr int kMaxPrimes = 64;
 struct ScalarTable {

@@ -75,6 +75,7 @@ void launch_gather_ptr(const DevTables& d, const GatherRef* dev_refs, int count,
 void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st,
                    int mode = 0);
 void launch_mac_plain(const DevTables& d, const MacBatch& b, cudaStream_t st);
+void launch_mac_tensor(const DevTables& d, const MacTensorBatch& b, cudaStream_t st);
 // Centered lift of the coefficient-form level-0 limb `src` into the prime of each ref.
 void launch_lift_level0(const DevTables& d, const LimbRef* refs, int count, cudaStream_t st);
 

@@ -589,15 +589,32 @@ void Server::worker() {
         for (auto& r : in_batch) placed.insert(r.get());
         f->close_segment(ctx_->stream, in_batch);
       }
+      // Mat-vecs: each checked on its own (a failing request fails alone), then one batched call
+      // per owner (all hoisted baby rotations, inner sums and giant rotations of the owner's
+      // requests as one launch sequence per stage) and one completion segment for them.
+      std::map<uint32_t, std::vector<ReqPtr>> matvecs;
       for (auto& r : batch) {
         if (r->kind != REQ_MATVEC || failed_req(r)) continue;
         try {
-          r->out = f->evs[r->owner]->matvec_plain(r->d, r->stride, r->diag, r->a);
-          owners_in_batch.insert(r->owner);
-          placed.insert(r.get());
-          f->close_segment(ctx_->stream, {r});
+          f->evs[r->owner]->check_matvec_plain(r->d, r->stride, r->diag, r->a);
+          matvecs[r->owner].push_back(r);
         } catch (const Error& e) {
           errs.push_back({r, {e.code, e.what()}});
+        }
+      }
+      for (auto& kv : matvecs) {
+        std::vector<MatvecJob<Pt>> jobs;
+        for (auto& r : kv.second) jobs.push_back(MatvecJob<Pt>{r->d, r->stride, r->diag, r->a});
+        try {
+          std::vector<Ct> outs = f->evs[kv.first]->matvec_plain_batch(jobs);
+          for (size_t i = 0; i < outs.size(); ++i) {
+            kv.second[i]->out = outs[i];
+            placed.insert(kv.second[i].get());
+          }
+          owners_in_batch.insert(kv.first);
+          f->close_segment(ctx_->stream, kv.second);
+        } catch (const Error& e) {
+          for (auto& r : kv.second) errs.push_back({r, {e.code, e.what()}});
         }
       }
       for (auto& r : batch) {

@@ -156,6 +156,9 @@ def _declare(L):
     L.ckg_exact_product_scale.argtypes = [VP, C.c_uint32, C.c_double, C.POINTER(C.c_double)]
     L.ckg_matvec_plain.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
     L.ckg_matvec_enc.argtypes = [VP, C.c_uint32, C.c_uint32, C.POINTER(VP), VP, C.POINTER(VP)]
+    for name in ("ckg_matvec_enc_batch", "ckg_matvec_plain_batch"):
+        getattr(L, name).argtypes = [VP, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(VP),
+                                     C.POINTER(VP), C.POINTER(VP)]
     L.ckg_batch_create.argtypes = [VP, C.POINTER(VP)]
     L.ckg_batch_destroy.argtypes = [VP]
     L.ckg_batch_mul_relin_rescale.argtypes = [VP, VP, VP, C.POINTER(VP)]
@@ -754,6 +757,25 @@ class CudaEvaluator:
     def matvec_enc(self, d, stride, entries, x):
         arr = (VP * len(entries))(*[e.h for e in entries])
         return self._ct(lib().ckg_matvec_enc, d, stride, arr, x.h)
+
+    def _matvec_batch(self, fn, jobs):
+        n = len(jobs)
+        ds = (C.c_uint32 * max(n, 1))(*[j[0] for j in jobs])
+        ss = (C.c_uint32 * max(n, 1))(*[j[1] for j in jobs])
+        flat = [e for j in jobs for e in j[2]]
+        es = (VP * max(len(flat), 1))(*[e.h for e in flat])
+        xs = (VP * max(n, 1))(*[j[3].h for j in jobs])
+        outs = (VP * max(n, 1))()
+        _check(fn(self.h, n, ds, ss, es, xs, outs))
+        return [Ciphertext(self, VP(outs[i])) for i in range(n)]
+
+    def matvec_enc_batch(self, jobs):
+        """CudaEvaluator::matvec_enc_batch (evaluator.rs:437-520): jobs of (d, stride, entries, x)."""
+        return self._matvec_batch(lib().ckg_matvec_enc_batch, jobs)
+
+    def matvec_plain_batch(self, jobs):
+        """matvec_plain for every job of (d, stride, entries, x), batched stage by stage."""
+        return self._matvec_batch(lib().ckg_matvec_plain_batch, jobs)
 
     # ---- bootstrapping (include/ckg.h, "bootstrapping") ----
 

@@ -224,6 +224,20 @@ CKG_API int ckg_matvec_plain(ckg_eval* ev, uint32_t d, uint32_t stride, const ck
                      ckg_ct** out);
 CKG_API int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_ct* const* entries, const ckg_ct* x,
                    ckg_ct** out);
+/* CudaEvaluator::matvec_enc_batch (crates/ckks-train-cuda/src/evaluator.rs:437-520): njobs
+ * products W_i x_i, job i with d[i] entries at entries[o_i .. o_i + d[i]) (o_i = d[0] + ... +
+ * d[i-1]), stride[i] and input xs[i]; outs[i] receives W_i x_i. Every job is checked as
+ * ckg_matvec_enc, in order, before any work (the first failure is returned, nothing counted);
+ * results and counts equal those of the jobs run one by one. With the optimized EvalConfig the
+ * jobs run stage by stage together (all hoisted baby rotations, all inner sums, all
+ * relinearizations, all giant rotations: one key-switch launch sequence per stage and level)
+ * where the reference spreads whole jobs over streams. */
+CKG_API int ckg_matvec_enc_batch(ckg_eval* ev, uint32_t njobs, const uint32_t* d, const uint32_t* stride,
+                                 const ckg_ct* const* entries, const ckg_ct* const* xs, ckg_ct** outs);
+/* The same for plaintext diagonals (ckg_matvec_plain per job; no counterpart in the reference,
+ * which batches only encrypted diagonals). */
+CKG_API int ckg_matvec_plain_batch(ckg_eval* ev, uint32_t njobs, const uint32_t* d, const uint32_t* stride,
+                                   const ckg_pt* const* entries, const ckg_ct* const* xs, ckg_ct** outs);
 
 /* ---- batched execution at uneven levels ----------------------------------------------
  * A batch holds many ops on ciphertexts of any levels and runs them as one sequence of
@@ -233,8 +247,8 @@ CKG_API int ckg_matvec_enc(ckg_eval* ev, uint32_t d, uint32_t stride, const ckg_
  * rotate = evaluator.rs:534-540; mul_plain then rescale = evaluator.rs:262-271, 498-510),
  * checked when the op is added; the outputs are returned at once and hold their values
  * after run / launch_graph completes on the context's stream. Every run adds the ops'
- * counts to the evaluator's OpCounter. This extends the reference's multi-stream
- * matvec_enc_batch (crates/ckks-train-cuda/src/evaluator.rs:437-520) to any op mix. */
+ * counts to the evaluator's OpCounter. Mat-vec products batch through ckg_matvec_enc_batch /
+ * ckg_matvec_plain_batch. */
 typedef struct ckg_batch ckg_batch;
 CKG_API int ckg_batch_create(ckg_eval* ev, ckg_batch** out);
 CKG_API void ckg_batch_destroy(ckg_batch* b);

@@ -93,3 +93,24 @@ def test_cfg2_per_op_hoisted_and_matvec(cfg2):
     pts = np.stack([P.random_q(90 + i, 23) for i in range(d)])
     env.check(env.cpu.matvec_plain(d, 1, pts, env.scale, x_c),
               env.gpu.matvec_plain(d, 1, [env.gpu.upload_pt(p, env.scale) for p in pts], x_g), "matvec_plain d 4")
+
+
+def test_cfg2_matvec_enc_batch(cfg2):
+    """matvec_enc_batch at N = 2^16, 24 + 8 primes, dnum 3: two jobs at two levels, each equal to
+    the oracle's matvec_enc, with the counters of the jobs one by one."""
+    env = cfg2
+    P = env.P
+    env.cpu.reset_counter()
+    env.gpu.reset_counter()
+    want, jobs = [], []
+    for n, level in enumerate((23, 9)):
+        x_c, x_g = env.pair(random_ct(P, 910 + n, level))
+        ents = [env.pair(random_ct(P, 920 + 10 * n + i, level)) for i in range(4)]
+        want.append(env.cpu.matvec_enc(4, 1, [c for c, _ in ents], x_c))
+        jobs.append((4, 1, [g for _, g in ents], x_g))
+    got = env.gpu.matvec_enc_batch(jobs)
+    for n, (w, g) in enumerate(zip(want, got)):
+        data, scale = env.gpu.download_ct(g)
+        assert g.level() == w.level and scale == w.scale
+        assert_same(data, w.data(), f"cfg2 matvec_enc_batch job {n}")
+    assert env.gpu.counter() == env.cpu.counter()

@@ -252,3 +252,47 @@ def test_key_switch_cfg2(ckg, oracle):
         wb, wa = rk.key_switch(d)
         assert_same(from_dev(ob), wb, f"cfg2 key_switch b level {level}")
         assert_same(from_dev(oa), wa, f"cfg2 key_switch a level {level}")
+
+
+def test_matvec_batches(env):
+    """matvec_enc_batch (crates/ckks-train-cuda/src/evaluator.rs:437-520) and its plaintext twin:
+    jobs of several sizes, strides and levels give the oracle's matvec_enc / matvec_plain result
+    for each job, bit for bit, and the counters of the jobs run one by one, under every
+    EvalConfig; a failing job fails the whole call before any work, with nothing counted."""
+    P = env.P
+    L = P.max_level
+    if L < 1:
+        pytest.skip("needs a level above 0")
+    big = 4 if P.n // 2 < 64 else 16
+    specs = [(big, 1, L), (8, 1, max(L // 2, 1)), (4, 2, L), (4, 1, 1)]
+    for cfg in itertools.product([True, False], repeat=3):
+        env.set_config(*cfg)
+        for kind in ("enc", "plain"):
+            env.cpu.reset_counter()
+            env.gpu.reset_counter()
+            want, jobs = [], []
+            for n, (d, stride, level) in enumerate(specs):
+                x_c, x_g = env.pair(random_ct(P, 500 + n, level))
+                if kind == "enc":
+                    ents = [env.pair(random_ct(P, 600 + 20 * n + i, level)) for i in range(d)]
+                    want.append(env.cpu.matvec_enc(d, stride, [c for c, _ in ents], x_c))
+                    jobs.append((d, stride, [g for _, g in ents], x_g))
+                else:
+                    pts = np.stack([P.random_q(700 + 20 * n + i, level) for i in range(d)])
+                    want.append(env.cpu.matvec_plain(d, stride, pts, env.scale, x_c))
+                    jobs.append((d, stride, [env.gpu.upload_pt(p, env.scale) for p in pts], x_g))
+            got = (env.gpu.matvec_enc_batch if kind == "enc" else env.gpu.matvec_plain_batch)(jobs)
+            for n, (w, g) in enumerate(zip(want, got)):
+                data, scale = env.gpu.download_ct(g)
+                assert g.level() == w.level and scale == w.scale, f"job {n}"
+                assert_same(data, w.data(), f"matvec_{kind}_batch job {n} {cfg}")
+            assert env.gpu.counter() == env.cpu.counter(), f"matvec_{kind}_batch counters {cfg}"
+    env.set_config(True, True, True)
+    # the first failing job fails the call: nothing runs, nothing is counted
+    env.gpu.reset_counter()
+    x_hi = env.gpu.upload_ct(random_ct(P, 801, L), env.scale)
+    x_lo = env.gpu.upload_ct(random_ct(P, 802, L - 1), env.scale)
+    ents = [env.gpu.upload_ct(random_ct(P, 810 + i, L), env.scale) for i in range(4)]
+    with pytest.raises(env.ckg.LevelMismatch):
+        env.gpu.matvec_enc_batch([(4, 1, ents, x_hi), (4, 1, ents, x_lo)])
+    assert sum(env.gpu.counter().values()) == 0
