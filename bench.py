@@ -246,30 +246,43 @@ class Mix:
         for (kind, level, steps) in self.ops:
             lv = level if kind == "rot" else level - 1
             self.out_host.append(torch.empty((2, lv + 1, self.S.n), dtype=torch.int64, pin_memory=True))
+        self.out_ptrs = [t.data_ptr() for t in self.out_host]
+        self.inflight, self.host_s = [], 0.0
+        self.stream = torch.cuda.ExternalStream(self.S.ctx.stream)
 
     def step_e2e(self):
-        """Upload every input from pinned host memory, build and run the batch, download
-        every result to pinned host memory, through the C ABI's overlapped host transfers:
-        this step's uploads run beside the previous step's compute and downloads."""
-        ev = self.S.ev
-        ins, h2d = [], 0
+        """Upload every input from pinned host memory, build and run the batch, download every
+        result to pinned host memory, through the C ABI's overlapped list transfers (one call
+        per list): this step's uploads run beside the previous step's compute and downloads. At
+        most two steps are in flight (the host waits for the compute of the step before last)."""
+        torch, ev = self.S.torch, self.S.ev
+        if len(self.inflight) >= 2:
+            self.inflight.pop(0).synchronize()
+        t0 = time.perf_counter()
+        ct_items, pt_items, h2d = [], [], 0
         for (kind, level, steps), (ha, hb) in zip(self.ops, self.host):
-            a = ev.upload_ct_overlap(ha.data_ptr(), 2, level, SCALE)
+            ct_items.append((ha.data_ptr(), 2, level, SCALE))
             h2d += ha.numel() * 8
-            extra = None
             if kind == "mul":
-                extra = ev.upload_ct_overlap(hb.data_ptr(), 2, level, SCALE)
+                ct_items.append((hb.data_ptr(), 2, level, SCALE))
                 h2d += hb.numel() * 8
             elif kind == "pmul":
-                extra = ev.upload_pt_overlap(hb.data_ptr(), level, SCALE)
+                pt_items.append((hb.data_ptr(), level, SCALE))
                 h2d += hb.numel() * 8
-            ins.append((kind, a, extra, steps))
+        cts = iter(ev.upload_ct_overlap_list(ct_items))
+        pts = iter(ev.upload_pt_overlap_list(pt_items) if pt_items else [])
+        ins = []
+        for kind, level, steps in self.ops:
+            a = next(cts)
+            ins.append((kind, a, next(cts) if kind == "mul" else (next(pts) if kind == "pmul" else None), steps))
         b, outs = self.make_batch(ins)
         b.run()
-        d2h = 0
-        for r, dst in zip(outs, self.out_host):
-            ev.download_ct_overlap(r, dst.data_ptr())
-            d2h += r.size() * (r.level() + 1) * self.S.n * 8
+        e = torch.cuda.Event()
+        e.record(self.stream)
+        self.inflight.append(e)
+        ev.download_ct_overlap_list(outs, self.out_ptrs)
+        d2h = sum(t.numel() * 8 for t in self.out_host)
+        self.host_s += time.perf_counter() - t0
         return h2d, d2h
 
 
@@ -846,6 +859,82 @@ def ntt_pair(torch, ctx, n, limbs=768):
     return buf, primes
 
 
+def raw_keyswitch(torch, ks_call, stream_ptr, q_all, n, level=PLAIN_LEVEL, calls=128, distinct=16, seed=7):
+    """Config 2's per-op key switch: `calls` single key switches of level-`level` polynomials
+    (24 limbs at level 23), one call each (ks_call(in_ptr, out_b_ptr, out_a_ptr)), cycling over
+    `distinct` seeded uniform inputs (more than L2 together), timed with CUDA events on the
+    caller's stream after three warm-up calls."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    qcol = q_all[: level + 1].view(-1, 1)
+    ins = [torch.randint(0, 1 << 62, (level + 1, n), generator=g, device="cuda", dtype=torch.int64) % qcol
+           for _ in range(distinct)]
+    ob = torch.empty((level + 1, n), dtype=torch.int64, device="cuda")
+    oa = torch.empty_like(ob)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    for i in range(3):
+        ks_call(ins[i % distinct].data_ptr(), ob.data_ptr(), oa.data_ptr())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for i in range(calls):
+        ks_call(ins[i % distinct].data_ptr(), ob.data_ptr(), oa.data_ptr())
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    return {"value": round(calls / (ms * 1e-3), 2), "unit": "keyswitch/s", "ms_per_keyswitch": round(ms / calls, 4),
+            "workload": f"{calls} key switches of single polynomials at {level + 1} limbs (N=2^16, 24+8 primes, "
+                        "dnum 3), one call each"}
+
+
+def ntt_32_limbs(torch, ntt_call, stream_ptr, n, reps=20):
+    """Config 2's standalone transform: forward + inverse NTT over 32 limbs (24 data + 8 special
+    primes), in place, timed with CUDA events on the caller's stream."""
+    buf = torch.randint(0, 1 << 40, (32, n), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    primes = list(range(32))
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    for _ in range(2):
+        ntt_call(buf.data_ptr(), primes, False)
+        ntt_call(buf.data_ptr(), primes, True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        ntt_call(buf.data_ptr(), primes, False)
+        ntt_call(buf.data_ptr(), primes, True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return {"us_per_pair": round(a.elapsed_time(b) * 1e3 / reps, 2), "limbs": 32}
+
+
+def reference_gpu(torch):
+    """The reference's own CUDA kernels (crates/ckks-train-cuda/kernels, unmodified, --fmad=false)
+    through the launch sequences of its host code, on this device: the per-op key switch and the
+    32-limb NTT pair of config 2 (oracle/ref_gpu)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built (the reference tree was absent at build time)"}
+    P = O.Params.from_bits(LOG_N, Q_BITS, P_BITS, 50, DNUM)
+    R = ref_gpu.RefGpu(LOG_N, P.q, P.p, DNUM)
+    n = P.n
+    q_all = torch.tensor(P.q + P.p, dtype=torch.int64, device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    key = torch.randint(0, 1 << 62, (DNUM, 2, P.nq + P.np_, n), generator=g, device="cuda",
+                        dtype=torch.int64) % q_all.view(1, 1, -1, 1)
+    torch.cuda.synchronize()
+    ks = raw_keyswitch(torch, lambda i, b, a: R.key_switch(i, PLAIN_LEVEL, key.data_ptr(), b, a), R.stream, q_all, n)
+    ntt = ntt_32_limbs(torch, lambda buf, primes, inv: R.ntt(buf, primes, inv), R.stream, n)
+    return {"kernels": "crates/ckks-train-cuda/kernels/{ntt,basis,keyswitch}.cu compiled unmodified (--fmad=false) "
+                       "and driven through the launch sequences of src/ks.rs, src/basis.rs, src/device.rs "
+                       "(oracle/ref_gpu/ref_ks.cu)",
+            "keyswitch_raw": ks, "ntt_pair": ntt}
+
+
 def ntt_roofline(torch, S, peaks, limbs=768):
     """Forward + inverse NTT over `limbs` limbs (24 data + 8 special primes cycled, as in a
     batched stage), timed alone with CUDA events on the library's stream. Algorithmic bytes
@@ -880,48 +969,108 @@ def ntt_roofline(torch, S, peaks, limbs=768):
 
 class CpuPath:
     """The oracle's CPU evaluator (the reference's CPU path restated, OpenMP over the units
-    of its `parallel` feature) with keys from its own key generator (relinearization key
-    and the Galois keys of the first rotation steps of the mix)."""
+    of its `parallel` feature) with keys from its own key generator: the relinearization key
+    and, generated on first use, the Galois key of every rotation step a sample draws."""
 
     def __init__(self, threads, seed=20261203):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
-        self.O = O
+        self.O, self.threads = O, threads
         O.set_threads(threads)
         self.P = O.Params.from_bits(LOG_N, Q_BITS, P_BITS, 50, DNUM)
-        kg = O.KeyGenerator(self.P, 5)
-        rk = kg.relin_key()
+        self.kg = O.KeyGenerator(self.P, 5)
+        self.rk = self.kg.relin_key()
         self.ops = mix_ops(seed, 256)
-        elts = sorted({O.galois_elt(self.P.n, s) for kind, _, s in self.ops if kind == "rot"})[:4]
-        self.gk = {e: kg.galois_key(e) for e in elts}
-        self.ev = O.Evaluator(self.P, rk, self.gk)
-        self.pos = 0
+        self.gk, self.ev, self.pos = {}, None, 0
+
+    def take(self, key_switches):
+        """The next ops of the mix, in order (wrapping), that hold `key_switches` key switches;
+        every rotation among them gets its Galois key before it is timed."""
+        out, ks = [], 0
+        while ks < key_switches:
+            op = self.ops[self.pos]
+            self.pos = (self.pos + 1) % len(self.ops)
+            out.append(op)
+            ks += op[0] != "pmul"
+        need = {self.O.galois_elt(self.P.n, s) for kind, _, s in out if kind == "rot"} - set(self.gk)
+        for e in sorted(need):
+            self.gk[e] = self.kg.galois_key(e)
+        if need or self.ev is None:
+            self.ev = self.O.Evaluator(self.P, self.rk, self.gk)
+        return out
 
 
-def cpu_sample(threads, budget_s=20.0, seed=20261203, path=None):
-    """Key switches per second of the CPU path on ops drawn in order from the same mix
-    (rotations whose Galois key was not generated are skipped), until the budget is used."""
-    cp = path or CpuPath(threads, seed)
-    O, P, ev, gk = cp.O, cp.P, cp.ev, cp.gk
-    ops = cp.ops[cp.pos:] + cp.ops[:cp.pos]
-    ks, t0 = 0, time.perf_counter()
-    for kind, level, steps in ops:
-        if kind == "rot" and O.galois_elt(P.n, steps) not in gk:
-            continue
-        a = ev.ct(np.stack([P.random_q(ks * 2 + 1, level), P.random_q(ks * 2 + 2, level)]), SCALE)
+def cpu_host():
+    """The host the CPU numbers were taken on: model name and logical CPUs."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "logical_cpus": os.cpu_count()}
+
+
+def cpu_sample(path, key_switches=120):
+    """Key switches per second of the CPU path on the next ops of the seeded mix, drawn in
+    order with none skipped; only the ops themselves are timed (input generation and Galois
+    key generation are not)."""
+    O, P = path.O, path.P
+    ops = path.take(key_switches)
+    ev = path.ev
+    load0 = os.getloadavg()[0]
+    ks, dt, kinds = 0, 0.0, {"mul": 0, "rot": 0, "pmul": 0}
+    for i, (kind, level, steps) in enumerate(ops):
+        a = ev.ct(np.stack([P.random_q(2 * i + 1, level), P.random_q(2 * i + 2, level)]), SCALE)
+        pt = P.random_q(7, level) if kind == "pmul" else None
+        t0 = time.perf_counter()
         if kind == "mul":
             ev.rescale(ev.mul(a, a))
-            ks += 1
         elif kind == "rot":
             ev.rotate(a, steps)
-            ks += 1
         else:
-            ev.rescale(ev.mul_plain(a, P.random_q(7, level), SCALE))
-        cp.pos = (cp.pos + 1) % len(cp.ops)
-        if time.perf_counter() - t0 > budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return ks / dt, f"{ks} key switches of the seeded op mix (limbs 4..24) in {dt:.1f} s"
+            ev.rescale(ev.mul_plain(a, pt, SCALE))
+        dt += time.perf_counter() - t0
+        ks += kind != "pmul"
+        kinds[kind] += 1
+    load1 = os.getloadavg()[0]
+    sample = (f"{ks} key switches of the seeded op mix in order, none skipped ({kinds['mul']} HMult+relin+rescale, "
+              f"{kinds['rot']} rotations over {len(path.gk)} Galois keys, {kinds['pmul']} PtMult+rescale; "
+              f"limbs 4..24) in {dt:.1f} s on {path.threads} threads; 1-min load {load0:.2f} -> {load1:.2f}")
+    return ks / dt, sample
+
+
+def cpu_crosscheck(threads):
+    """The port against the reference's published CPU figure for the same op: relinearize at
+    level 31 of n16_train (N = 2^16, 58 + 31 x 42-bit q, 4 x 58-bit p, dnum 8), median of 3,
+    on 1 thread and on 12 (or all, if fewer) threads. The published medians are 639.6 ms and
+    240.1 ms on an i9-13900KF (docs/m4-report.md, table 1.1, row relinearize)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    wide = min(12, threads)
+    O.set_threads(threads)
+    P = O.Params.from_bits(16, MLP_Q_BITS, MLP_P_BITS, 42, MLP_DNUM)
+    kg = O.KeyGenerator(P, 5)
+    ev = O.Evaluator(P, kg.relin_key(), {})
+    a = ev.ct(np.stack([P.random_q(1, 31), P.random_q(2, 31)]), 2.0 ** 42)
+    b = ev.ct(np.stack([P.random_q(3, 31), P.random_q(4, 31)]), 2.0 ** 42)
+    c = ev.mul_no_relin(a, b)
+    out = {"op": "relinearize, n16_train level 31", "published_ms": {"1": 639.6, "12": 240.1},
+           "published_cpu": "i9-13900KF"}
+    for th in (1, wide):
+        O.set_threads(th)
+        ev.relinearize(c)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ev.relinearize(c)
+            ts.append(time.perf_counter() - t0)
+        out[f"ms_{th}_threads"] = round(sorted(ts)[1] * 1e3, 1)
+    O.set_threads(threads)
+    return out
 
 
 def main():
@@ -967,23 +1116,35 @@ def main():
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        vals, sample = [], ""
+        vals, samples = [], []
         path = CpuPath(threads)
-        budget = max(4.0, 40.0 / max(args.steps, 1))
+        per_step = -(-120 // max(args.steps, 1))
         for _ in range(args.warmup):
-            cpu_sample(threads, budget_s=1.0, path=path)
+            cpu_sample(path, key_switches=2)
         for _ in range(max(args.steps, 1)):
-            v, sample = cpu_sample(threads, budget_s=budget, path=path)
+            v, sample = cpu_sample(path, key_switches=per_step)
             vals.append(v)
+            samples.append(sample)
         v = float(np.mean(vals))
+        sample = f"{len(samples)} steps of: " + samples[-1]
+        host = dict(cpu_host(), crosscheck=cpu_crosscheck(threads))
+        ref_gpu_line = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                torch.cuda.set_device(local)
+                ref_gpu_line = reference_gpu(torch)
+        except Exception as e:  # noqa: BLE001 -- the CPU arm's line stands without it
+            ref_gpu_line = {"unavailable": f"{type(e).__name__}: {e}"}
         print(json.dumps({"impl": "reference", "metric": metric, "value": round(v, 3), "unit": unit,
                           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
                           "data": "synthetic", "config": config,
-                          "cpu_baseline": {"value": round(v, 3), "unit": unit, "cores": threads, "kind": "port",
-                                           "sample": sample},
+                          "cpu_baseline": dict({"value": round(v, 3), "unit": unit, "cores": threads,
+                                                "kind": "port", "sample": sample}, **host),
                           "e2e": {"value": round(v, 3), "unit": unit, "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}))
+                                  "d2h_bytes_per_step": 0},
+                          "reference_gpu": ref_gpu_line}))
         return
 
     import torch
@@ -1058,11 +1219,15 @@ def main():
     e2e = None
     if not args.no_e2e:
         mix.prepare_e2e()
-        steps_e = max(1, args.steps)
-        ms_e, (h2d, d2h) = timed(torch, S.ctx, mix.step_e2e, steps_e, 1, dist, tail=S.ctx.join_transfers)
+        steps_e = max(8, args.steps)
+        mix.step_e2e()
+        mix.inflight.clear()
+        mix.host_s = 0.0
+        ms_e, (h2d, d2h) = timed(torch, S.ctx, mix.step_e2e, steps_e, 0, dist, tail=S.ctx.join_transfers)
         e2e = {"value": round(mix.ks * steps_e * world / (ms_e * 1e-3), 2), "unit": unit,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": round(ms_e / steps_e, 3)}
+               "ms_per_step": round(ms_e / steps_e, 3), "steps": steps_e,
+               "host_ms_per_step": round(mix.host_s * 1e3 / steps_e, 2)}
         if rank == 0:  # no collective inside: the other ranks skip it
             e2e["host_link"] = pcie_ceiling(torch, h2d, d2h, ms_e / steps_e)
     plain = None
@@ -1082,6 +1247,9 @@ def main():
                              "one evaluator call per op; better of two timed runs of 2 steps after 3 warm-up steps",
                  "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
+    ks_raw = raw_keyswitch(torch, lambda i, b, a: S.ctx.key_switch(S.relin, i, PLAIN_LEVEL, b, a), S.ctx.stream,
+                           S.q_all, S.n)
+    ntt32 = ntt_32_limbs(torch, lambda buf, primes, inv: S.ctx.ntt(buf, buf, primes, inv), S.ctx.stream, S.n)
     roof = ntt_roofline(torch, S, peaks)
     roof_stream = stream_roofline(rank_stream(rank, args.ops), S.n, S.ctx.k, S.ctx.alpha, ms / args.steps, peaks)
     # The bootstrap, training-step and serving figures are single-GPU measurements: a run on N > 1
@@ -1110,8 +1278,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sample = cpu_sample(threads)
-        cpu = {"value": round(v, 3), "unit": unit, "cores": threads, "kind": "port", "sample": sample}
+        v, sample = cpu_sample(CpuPath(threads))
+        cpu = dict({"value": round(v, 3), "unit": unit, "cores": threads, "kind": "port", "sample": sample},
+                   **cpu_host(), crosscheck=cpu_crosscheck(threads))
     if rank == 0:
         line = {"metric": metric, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -1121,7 +1290,8 @@ def main():
                                autotune={"ntt_wave": tuning["ntt_wave"], "chunk_items": tuning["chunk_items"],
                                          "trials_ms": [[w, c, round(m, 3)] for w, c, m in tuning["trials"]]}),
                 "e2e": e2e,
-                "gpu_launches": int(launches_per_step * args.steps), "plain": plain, "roofline": roof,
+                "gpu_launches": int(launches_per_step * args.steps), "plain": plain,
+                "keyswitch_raw": ks_raw, "ntt_pair_32_limbs": ntt32, "roofline": roof,
                 "roofline_stream": roof_stream,
                 "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
                 "clocks": clk.summary()}

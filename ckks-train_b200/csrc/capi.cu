@@ -442,6 +442,47 @@ int ckg_ct_download_overlap(const ckg_ct* ct, uint64_t* host) {
   CKG_API_END
 }
 
+int ckg_ct_upload_overlap_list(ckg_eval* ev, uint32_t count, const uint64_t* const* hosts, const uint32_t* ncomp,
+                               const uint32_t* levels, const double* scales, ckg_ct** out) {
+  CKG_API_BEGIN
+  if (count && (!hosts || !ncomp || !levels || !scales || !out)) throw Error(CKG_INVALID_PARAMS, "null list");
+  std::vector<Evaluator::CtUpload> items(count);
+  for (uint32_t i = 0; i < count; ++i) items[i] = {hosts[i], ncomp[i], levels[i], scales[i]};
+  std::vector<Ct> cts = ev_of(ev).upload_overlapped_list(items);
+  for (uint32_t i = 0; i < count; ++i) out[i] = new ckg_ct{cts[i]};
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_pt_upload_overlap_list(ckg_eval* ev, uint32_t count, const uint64_t* const* hosts, const uint32_t* levels,
+                               const double* scales, ckg_pt** out) {
+  CKG_API_BEGIN
+  if (count && (!hosts || !levels || !scales || !out)) throw Error(CKG_INVALID_PARAMS, "null list");
+  std::vector<Evaluator::CtUpload> items(count);
+  for (uint32_t i = 0; i < count; ++i) items[i] = {hosts[i], 0, levels[i], scales[i]};
+  std::vector<Pt> pts = ev_of(ev).upload_pt_overlapped_list(items);
+  for (uint32_t i = 0; i < count; ++i) out[i] = new ckg_pt{pts[i]};
+  check_launch();
+  CKG_API_END
+}
+
+int ckg_ct_download_overlap_list(uint32_t count, const ckg_ct* const* cts, uint64_t* const* hosts) {
+  CKG_API_BEGIN
+  if (!count) return CKG_OK;
+  if (!cts || !hosts) throw Error(CKG_INVALID_PARAMS, "null list");
+  Context* ctx = ct_of(cts[0])->ctx;
+  std::vector<Context::DevPart> parts(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    const Ct& c = ct_of(cts[i]);
+    if (!hosts[i]) throw Error(CKG_INVALID_PARAMS, "null host buffer");
+    if (c->ctx != ctx) throw Error(CKG_INVALID_PARAMS, "ciphertexts of different contexts in one list");
+    const size_t words = (size_t)(c->level + 1) * ctx->n;
+    parts[i] = {&c->buf, c->comp(0), words, c->comp_stride, c->ncomp, hosts[i]};
+  }
+  ctx->download_overlapped_list(parts);
+  CKG_API_END
+}
+
 void ckg_pt_info(const ckg_pt* pt, uint32_t* level, double* scale) {
   if (level) *level = pt->p->level;
   if (scale) *scale = pt->p->scale;

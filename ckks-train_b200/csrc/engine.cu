@@ -1,5 +1,6 @@
 // Device context set-up (prime constants, twiddle and conversion tables) and the
 // polynomial-level algorithms of the evaluator path. See engine.hpp for the layouts.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -47,6 +48,17 @@ void Context::transfer_streams() {
     r->own = true;
     *sp = r;
   }
+  if (!xpool) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CKG_CUDA(cudaMemPoolCreate(&xpool, &props));
+    uint64_t thr = UINT64_MAX;
+    int no = 0;
+    CKG_CUDA(cudaMemPoolSetAttribute(xpool, cudaMemPoolAttrReleaseThreshold, &thr));
+    CKG_CUDA(cudaMemPoolSetAttribute(xpool, cudaMemPoolReuseAllowInternalDependencies, &no));
+  }
 }
 
 namespace {
@@ -69,8 +81,31 @@ DevBufPtr Context::upload_overlapped(const uint64_t* host, size_t words) {
   b->device = device;
   b->words = words;
   if (!words) return b;
-  CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, xfer_in->s));
+  CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, words * 8, xpool, xfer_in->s));
   CKG_CUDA(cudaMemcpyAsync(b->p, host, words * 8, cudaMemcpyHostToDevice, xfer_in->s));
+  stream_after(stream, xfer_in->s);
+  return b;
+}
+
+DevBufPtr Context::upload_overlapped_list(const std::vector<HostPart>& parts, std::vector<size_t>& offsets) {
+  activate();
+  transfer_streams();
+  auto b = std::make_shared<DevBuf>();
+  b->sres = sres;
+  b->device = device;
+  offsets.assign(parts.size(), 0);
+  size_t total = 0;
+  for (size_t i = 0; i < parts.size(); ++i) {
+    offsets[i] = total;
+    total += (parts[i].words + 31) & ~(size_t)31;
+  }
+  b->words = total;
+  if (!total) return b;
+  CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, total * 8, xpool, xfer_in->s));
+  for (size_t i = 0; i < parts.size(); ++i)
+    if (parts[i].words)
+      CKG_CUDA(cudaMemcpyAsync(b->p + offsets[i], parts[i].host, parts[i].words * 8, cudaMemcpyHostToDevice,
+                               xfer_in->s));
   stream_after(stream, xfer_in->s);
   return b;
 }
@@ -100,6 +135,41 @@ void Context::download_overlapped(const DevBufPtr& buf, const uint64_t* dev, siz
   CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   CKG_CUDA(cudaEventRecord(e, xfer_out->s));
   w.push_back(e);
+}
+
+void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
+  activate();
+  transfer_streams();
+  if (parts.empty()) return;
+  stream_after(xfer_out->s, stream);
+  for (const DevPart& d : parts) {
+    if (d.pitch_words == d.row_words)
+      CKG_CUDA(cudaMemcpyAsync(d.host, d.dev, d.rows * d.row_words * 8, cudaMemcpyDeviceToHost, xfer_out->s));
+    else
+      CKG_CUDA(cudaMemcpy2DAsync(d.host, d.row_words * 8, d.dev, d.pitch_words * 8, d.row_words * 8, d.rows,
+                                 cudaMemcpyDeviceToHost, xfer_out->s));
+  }
+  // every buffer's free waits for the copies (one event per distinct buffer)
+  std::vector<DevBuf*> seen;
+  for (const DevPart& d : parts) {
+    DevBuf* b = d.buf->get();
+    if (std::find(seen.begin(), seen.end(), b) != seen.end()) continue;
+    seen.push_back(b);
+    auto& w = b->waits;
+    for (size_t i = 0; i < w.size();) {
+      if (cudaEventQuery(w[i]) == cudaSuccess) {
+        cudaEventDestroy(w[i]);
+        w[i] = w.back();
+        w.pop_back();
+      } else {
+        ++i;
+      }
+    }
+    cudaEvent_t e;
+    CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CKG_CUDA(cudaEventRecord(e, xfer_out->s));
+    w.push_back(e);
+  }
 }
 
 void Context::join_transfers() {
@@ -466,6 +536,7 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
 Context::~Context() {
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
+  if (xpool) cudaMemPoolDestroy(xpool);  // released once its last block is freed
   for (auto& kv : perms) cudaFree(kv.second);
   if (d_xhalf) cudaFree(d_xhalf);
   cudaFree(d_prime);

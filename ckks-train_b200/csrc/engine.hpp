@@ -128,11 +128,28 @@ struct Context {
   // Overlapped host transfers: an upload stream and a download stream beside `stream`
   // (created on first use). Buffers they fill are allocated on the upload stream and freed on
   // `stream`, which waits for the copy before its first use.
+  // Upload buffers come from their own pool, which reuses a freed block only once its free
+  // has completed (no stream wait inserted): the next uploads never wait for queued compute.
   StreamPtr xfer_in, xfer_out;
+  cudaMemPool_t xpool = nullptr;
   void transfer_streams();
   DevBufPtr upload_overlapped(const uint64_t* host, size_t words);
+  // Several host buffers into one allocation (one copy each, one stream dependency):
+  // part i starts at offsets[i] words (256-byte aligned).
+  struct HostPart {
+    const uint64_t* host;
+    size_t words;
+  };
+  DevBufPtr upload_overlapped_list(const std::vector<HostPart>& parts, std::vector<size_t>& offsets);
   void download_overlapped(const DevBufPtr& buf, const uint64_t* dev, size_t row_words, size_t pitch_words,
                            size_t rows, uint64_t* host);
+  struct DevPart {
+    const DevBufPtr* buf;
+    const uint64_t* dev;
+    size_t row_words, pitch_words, rows;
+    uint64_t* host;
+  };
+  void download_overlapped_list(const std::vector<DevPart>& parts);
   void join_transfers();  // `stream` waits for every transfer queued so far
   void sync_transfers();  // the host waits for them
 };

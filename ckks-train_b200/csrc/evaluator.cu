@@ -118,6 +118,54 @@ Pt Evaluator::upload_pt_overlapped(const uint64_t* host, uint32_t level, double 
   return p;
 }
 
+std::vector<Ct> Evaluator::upload_overlapped_list(const std::vector<CtUpload>& items) {
+  std::vector<Context::HostPart> parts;
+  for (const CtUpload& u : items) {
+    if (u.ncomp < 2) throw Error(ST_INVALID_PARAMS, "a ciphertext needs at least 2 components");
+    if (u.level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+    if (!u.host) throw Error(ST_INVALID_PARAMS, "null host buffer");
+    check_ct_scale(u.scale);
+    parts.push_back({u.host, (size_t)u.ncomp * (u.level + 1) * ctx_->n});
+  }
+  std::vector<size_t> off;
+  DevBufPtr buf = ctx_->upload_overlapped_list(parts, off);
+  std::vector<Ct> out;
+  for (size_t i = 0; i < items.size(); ++i) {
+    auto c = std::make_shared<CtObj>();
+    c->ctx = ctx_;
+    c->buf = buf;
+    c->offset = off[i];
+    c->ncomp = items[i].ncomp;
+    c->level = items[i].level;
+    c->scale = items[i].scale;
+    c->comp_stride = (size_t)(items[i].level + 1) * ctx_->n;
+    out.push_back(c);
+  }
+  return out;
+}
+
+std::vector<Pt> Evaluator::upload_pt_overlapped_list(const std::vector<CtUpload>& items) {
+  std::vector<Context::HostPart> parts;
+  for (const CtUpload& u : items) {
+    if (u.level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
+    if (!u.host) throw Error(ST_INVALID_PARAMS, "null host buffer");
+    parts.push_back({u.host, (size_t)(u.level + 1) * ctx_->n});
+  }
+  std::vector<size_t> off;
+  DevBufPtr buf = ctx_->upload_overlapped_list(parts, off);
+  std::vector<Pt> out;
+  for (size_t i = 0; i < items.size(); ++i) {
+    auto p = std::make_shared<PtObj>();
+    p->ctx = ctx_;
+    p->buf = buf;
+    p->offset = off[i];
+    p->level = items[i].level;
+    p->scale = items[i].scale;
+    out.push_back(p);
+  }
+  return out;
+}
+
 Pt Evaluator::upload_pt(const uint64_t* src, bool device_src, uint32_t level, double scale) {
   if (level > ctx_->L) throw Error(ST_INVALID_PARAMS, "level above max_level");
   ctx_->activate();

@@ -30,9 +30,10 @@ typedef std::shared_ptr<const CtObj> Ct;
 struct PtObj {
   Context* ctx = nullptr;
   DevBufPtr buf;
+  size_t offset = 0;  // words from buf->p to limb 0
   uint32_t level = 0;
   double scale = 0;
-  const uint64_t* data() const { return buf->p; }
+  const uint64_t* data() const { return buf->p + offset; }
 };
 typedef std::shared_ptr<const PtObj> Pt;
 
@@ -101,6 +102,14 @@ class Evaluator {
   // The same from host memory on the context's upload stream (Context::upload_overlapped).
   Ct upload_overlapped(const uint64_t* host, uint32_t ncomp, uint32_t level, double scale);
   Pt upload_pt_overlapped(const uint64_t* host, uint32_t level, double scale);
+  // A list of them in one allocation and one stream dependency; every entry is checked first.
+  struct CtUpload {
+    const uint64_t* host;
+    uint32_t ncomp, level;
+    double scale;
+  };
+  std::vector<Ct> upload_overlapped_list(const std::vector<CtUpload>& items);
+  std::vector<Pt> upload_pt_overlapped_list(const std::vector<CtUpload>& items);  // ncomp unused
 
   Ct add(const Ct& a, const Ct& b) { return add_sub(a, b, false); }
   Ct sub(const Ct& a, const Ct& b) { return add_sub(a, b, true); }

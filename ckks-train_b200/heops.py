@@ -199,6 +199,11 @@ def _declare(L):
     L.ckg_ct_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_pt_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_ct_download_overlap.argtypes = [VP, VP]
+    L.ckg_ct_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.POINTER(VP)]
+    L.ckg_pt_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_double), C.POINTER(VP)]
+    L.ckg_ct_download_overlap_list.argtypes = [C.c_uint32, C.POINTER(VP), C.POINTER(VP)]
     L.ckg_ctx_join_transfers.argtypes = [VP]
     DP = C.POINTER(C.c_double)
     L.ckg_boot_mul_const.argtypes = [VP, VP, C.c_double, C.c_double, C.POINTER(VP)]
@@ -633,6 +638,32 @@ class CudaEvaluator:
         """Queues the copy of `ct` to the pinned host address `ptr` on the download stream;
         complete after ctx.sync()."""
         _check(lib().ckg_ct_download_overlap(ct.h, VP(ptr)))
+
+    def upload_ct_overlap_list(self, items):
+        """upload_ct_overlap of every (ptr, ncomp, level, scale) in `items` in one call (one device
+        allocation, one stream dependency)."""
+        n = len(items)
+        hosts = (VP * n)(*[VP(p) for p, _, _, _ in items])
+        out = (VP * n)()
+        _check(lib().ckg_ct_upload_overlap_list(self.h, n, hosts, (C.c_uint32 * n)(*[c for _, c, _, _ in items]),
+                                                (C.c_uint32 * n)(*[lv for _, _, lv, _ in items]),
+                                                (C.c_double * n)(*[sc for _, _, _, sc in items]), out))
+        return [Ciphertext(self, VP(h)) for h in out]
+
+    def upload_pt_overlap_list(self, items):
+        """upload_pt_overlap of every (ptr, level, scale) in `items` in one call."""
+        n = len(items)
+        hosts = (VP * n)(*[VP(p) for p, _, _ in items])
+        out = (VP * n)()
+        _check(lib().ckg_pt_upload_overlap_list(self.h, n, hosts, (C.c_uint32 * n)(*[lv for _, lv, _ in items]),
+                                                (C.c_double * n)(*[sc for _, _, sc in items]), out))
+        return [Plaintext(self, VP(h), lv, sc) for h, (_, lv, sc) in zip(out, items)]
+
+    def download_ct_overlap_list(self, cts, ptrs):
+        """download_ct_overlap of every ciphertext in `cts` to the matching pinned host address."""
+        n = len(cts)
+        _check(lib().ckg_ct_download_overlap_list(n, (VP * n)(*[c.h for c in cts]),
+                                                  (VP * n)(*[VP(p) for p in ptrs])))
 
     def download_ct_async(self, ct, ptr):
         """Queues the copy of `ct` to the host address `ptr`; complete after ctx.sync()."""

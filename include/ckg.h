@@ -194,6 +194,15 @@ CKG_API int ckg_ct_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t n
 CKG_API int ckg_pt_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
 CKG_API int ckg_ct_download_overlap(const ckg_ct* ct, uint64_t* host);
 CKG_API int ckg_ctx_join_transfers(ckg_ctx* ctx);
+/* Lists of the same in one call each: the uploads share one device allocation and one
+ * stream dependency (every entry is checked before anything is queued; on an error no handle
+ * is made); the downloads share one stream dependency and must come from one context. */
+CKG_API int ckg_ct_upload_overlap_list(ckg_eval* ev, uint32_t count, const uint64_t* const* hosts,
+                                       const uint32_t* ncomp, const uint32_t* levels, const double* scales,
+                                       ckg_ct** out);
+CKG_API int ckg_pt_upload_overlap_list(ckg_eval* ev, uint32_t count, const uint64_t* const* hosts,
+                                       const uint32_t* levels, const double* scales, ckg_pt** out);
+CKG_API int ckg_ct_download_overlap_list(uint32_t count, const ckg_ct* const* cts, uint64_t* const* hosts);
 CKG_API ckg_pt* ckg_pt_clone(const ckg_pt* pt);
 CKG_API void ckg_pt_free(ckg_pt* pt);
 

@@ -72,3 +72,34 @@ def test_freed_handles_are_not_overwritten_early(env):
         gpu.upload_ct_overlap(0, 2, L, env.scale)
     with pytest.raises(ckg.InvalidParams):
         gpu.upload_ct_overlap(host.data_ptr(), 1, L, env.scale)
+
+
+def test_overlapped_lists_match_oracle(env):
+    """The list forms (one call per list, one shared allocation): uneven levels, the same
+    results as the oracle, every entry checked before anything is queued."""
+    ckg, P, gpu, cpu = env.ckg, env.P, env.gpu, env.cpu
+    L = P.max_level
+    levels = [L, L - 1, L, 1]
+    ins = [random_ct(P, 30 + i, lv) for i, lv in enumerate(levels)]
+    pts = [P.random_q(60 + i, lv) for i, lv in enumerate(levels)]
+    host_in = [_pinned(a) for a in ins]
+    host_pt = [_pinned(p) for p in pts]
+    outs_host = [_empty_pinned((2, lv, P.n)) for lv in levels]
+    for step in range(2):
+        g = gpu.upload_ct_overlap_list([(h.data_ptr(), 2, lv, env.scale) for h, lv in zip(host_in, levels)])
+        gp = gpu.upload_pt_overlap_list([(h.data_ptr(), lv, env.scale) for h, lv in zip(host_pt, levels)])
+        b = ckg.Batch(gpu)
+        res = [b.mul_plain_rescale(c, p) for c, p in zip(g, gp)]
+        b.run()
+        gpu.download_ct_overlap_list(res, [h.data_ptr() for h in outs_host])
+        del res, g, gp, b
+    env.ctx.join_transfers()
+    env.ctx.sync()
+    for i, (a, p) in enumerate(zip(ins, pts)):
+        w = cpu.rescale(cpu.mul_plain(cpu.ct(a, env.scale), p, env.scale))
+        assert_same(outs_host[i].numpy().view(np.uint64), w.data(), f"list entry {i}")
+    with pytest.raises(ckg.InvalidParams):  # a bad entry late in the list: nothing is made
+        gpu.upload_ct_overlap_list([(host_in[0].data_ptr(), 2, L, env.scale), (0, 2, L, env.scale)])
+    with pytest.raises(ckg.InvalidParams):
+        gpu.upload_pt_overlap_list([(host_pt[0].data_ptr(), L + 1, env.scale)])
+    assert gpu.upload_ct_overlap_list([]) == []
