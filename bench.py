@@ -338,7 +338,7 @@ class Serving:
     params_text = "N=2^16, 24x50-bit q + 8x60-bit p, dnum 3"
     mix_text = "5/8 single ops (HMult+relin+rescale | rotation), 3/8 64x64 BSGS plaintext mat-vec"
 
-    def __init__(self, S, owners=SERVE_OWNERS, budget=SERVE_BUDGET, seed=7):
+    def __init__(self, S, owners=SERVE_OWNERS, budget=SERVE_BUDGET, seed=7, router=None, rank=0):
         ckg, torch = S.ckg, S.torch
         self.S, self.owners = S, owners
         self.rng = np.random.default_rng(seed)
@@ -348,38 +348,59 @@ class Serving:
         self.steps = [k for k in range(1, bg)] + [bg * k for k in range(1, SERVE_D // bg)]
         shape = (DNUM, 2, len(ctx.q) + ctx.k, ctx.n)
         qcol = S.q_all.view(1, 1, -1, 1)
+        # On N GPUs every rank registers only the owners the router places on it.
+        local = router.owners_of(rank) if router else list(range(owners))
         t0 = time.time()
-        for _ in range(owners):
-            o = self.srv.add_owner()
+        self.slot = {}  # owner -> the server's owner id on this rank
+        for g in local:
+            o = self.slot[g] = self.srv.add_owner()
             for e in [0] + [galois_elt(ctx.n, st) for st in self.steps]:
                 t = S.uniform(shape, qcol)
                 self.srv.add_key_device(o, t.data_ptr(), shape, e)
                 del t
         self.register_s = time.time() - t0
-        self.key_bytes = owners * (1 + len(self.steps)) * int(np.prod(shape)) * 8
-        self.inputs = [[S.ct(l)[0] for l in (23, 17, 11, 5)] for _ in range(owners)]
+        self.key_bytes = len(local) * (1 + len(self.steps)) * int(np.prod(shape)) * 8
+        self.inputs = {g: [S.ct(l)[0] for l in (23, 17, 11, 5)] for g in local}
         self.diag = {l: [S.pt(l)[0] for _ in range(SERVE_D)] for l in (23, 11)}
 
+    @staticmethod
+    def key_bytes_per_owner():
+        """Registered key bytes of one owner (15 keys at N=2^16, 24+8 primes, dnum 3)."""
+        return 15 * DNUM * 2 * (len(Q_BITS) + len(P_BITS)) * (1 << LOG_N) * 8
+
     def request(self):
-        o = int(self.rng.integers(self.owners))
+        """The next request of the one seeded stream every rank draws alike: a callable that
+        submits it here, or None when its owner is placed on another rank."""
+        g = int(self.rng.integers(self.owners))
         r = self.rng.random()
-        ins = self.inputs[o]
         if r < 5 / 16:
-            a = ins[int(self.rng.integers(4))]
+            which, st = int(self.rng.integers(4)), None
+        elif r < 10 / 16:
+            which = int(self.rng.integers(4))
+            st = self.steps[int(self.rng.integers(len(self.steps)))]
+        else:
+            which, st = int(self.rng.integers(2)), None
+        if g not in self.slot:
+            return None
+        o, ins = self.slot[g], self.inputs[g]
+        if r < 5 / 16:
+            a = ins[which]
             return lambda: self.srv.submit_mul(o, a, a)
         if r < 10 / 16:
-            a = ins[int(self.rng.integers(4))]
-            st = self.steps[int(self.rng.integers(len(self.steps)))]
+            a = ins[which]
             return lambda: self.srv.submit_rotate(o, a, st)
-        i = int(self.rng.integers(2))
-        x, lvl = ins[0 if i == 0 else 2], (23, 11)[i]
+        x, lvl = ins[0 if which == 0 else 2], (23, 11)[which]
         return lambda: self.srv.submit_matvec(o, SERVE_D, 1, self.diag[lvl], x)
 
     def run(self, count, rate=None):
-        """Submits `count` requests (all at once, or Poisson at `rate` per second) while a
+        """Draws `count` requests of the stream and submits those placed here (all at once, or
+        at the due times of Poisson arrivals at `rate` per second over the whole stream) while a
         collector takes the results; returns per-request (submitted, completed) in us."""
         reqs = [self.request() for _ in range(count)]
         gaps = self.rng.exponential(1.0 / rate, count) if rate else np.zeros(count)
+        dues = np.cumsum(gaps)
+        local = [(d, q) for d, q in zip(dues, reqs) if q is not None]
+        count = len(local)
         ids, times, lag = [], [], [0.0]
         done = threading.Event()
 
@@ -398,38 +419,49 @@ class Serving:
         th = threading.Thread(target=collect, daemon=True)
         th.start()
         start = time.perf_counter()
-        due = 0.0
-        for k in range(count):
-            due += gaps[k]
+        for due, submit in local:
             now = time.perf_counter() - start
             if due > now:
                 time.sleep(due - now)
             lag[0] = max(lag[0], time.perf_counter() - start - due)
-            ids.append(reqs[k]())
+            ids.append(submit())
         done.wait()
         th.join()
-        return np.array([(t[0], t[2]) for t in times]), lag[0]
+        return np.array([(t[0], t[2]) for t in times]).reshape(-1, 2), lag[0]
 
-    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD):
+    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD, dist=None):
+        """Capacity (saturated), then `requests` Poisson arrivals at `load` x capacity. With `dist`
+        (one rank per GPU, owners placed by the router) capacity is the sum over ranks, the
+        latencies of all ranks are pooled and the span is the longest rank's."""
         self.run(96)  # warm-up: Galois permutations, pools, first key uploads
         sat, _ = self.run(min(400, requests))
-        capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6)
+        capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6) if len(sat) else 0.0
+        if dist:
+            capacity = sum(gather_objects(dist, capacity))
         st0 = self.srv.stats()
         rate = load * capacity
         t, lag = self.run(requests, rate)
         st = self.srv.stats()
         lat = (t[:, 1] - t[:, 0]) * 1e-3
-        span = (t[:, 1].max() - t[:, 0].min()) * 1e-6
+        span = (t[:, 1].max() - t[:, 0].min()) * 1e-6 if len(t) else 0.0
         d = {k: st[k] - st0[k] for k in ("batches", "multi_owner_batches", "key_hits", "key_misses",
                                           "key_evictions", "key_upload_bytes", "budget_waits")}
-        return {"requests": requests, "owners": self.owners, "params": self.params_text, "mix": self.mix_text,
+        peak_dev, key_bytes = st["peak_device_bytes"], self.key_bytes
+        if dist:
+            parts = gather_objects(dist, (lat.tolist(), span, lag, d, peak_dev, key_bytes))
+            lat = np.array([x for p in parts for x in p[0]])
+            span, lag = max(p[1] for p in parts), max(p[2] for p in parts)
+            d = {k: sum(p[3][k] for p in parts) for k in d}
+            peak_dev, key_bytes = max(p[4] for p in parts), sum(p[5] for p in parts)
+        return {"requests": requests, "served": int(len(lat)), "owners": self.owners, "params": self.params_text,
+                "mix": self.mix_text,
                 "capacity_req_s": round(capacity, 2), "offered_req_s": round(rate, 2),
                 "throughput_req_s": round(requests / span, 2),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
                 "mean_ms": round(float(lat.mean()), 3), "max_submit_lag_ms": round(lag * 1e3, 3),
                 "hbm_budget_gib": round(self.srv.stats()["hbm_budget"] / 2 ** 30, 2),
-                "key_set_gib": round(self.key_bytes / 2 ** 30, 2),
-                "peak_device_gib": round(st["peak_device_bytes"] / 2 ** 30, 2),
+                "key_set_gib": round(key_bytes / 2 ** 30, 2),
+                "peak_device_gib": round(peak_dev / 2 ** 30, 2),
                 "key_hit_rate": round(d["key_hits"] / max(1, d["key_hits"] + d["key_misses"]), 3),
                 "key_upload_gib": round(d["key_upload_bytes"] / 2 ** 30, 2),
                 "batches": d["batches"], "multi_owner_batches": d["multi_owner_batches"],
@@ -708,6 +740,13 @@ def max_over_ranks(dist, ms, device="cuda"):
     t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def gather_objects(dist, obj):
+    """Every rank's `obj`, in rank order (a collective: every rank calls it)."""
+    out = [None] * dist.get_world_size()
+    dist.all_gather_object(out, obj)
+    return out
 
 
 def rank_stream(rank, count=MIX_OPS):
@@ -1252,8 +1291,8 @@ def main():
     ntt32 = ntt_32_limbs(torch, lambda buf, primes, inv: S.ctx.ntt(buf, buf, primes, inv), S.ctx.stream, S.n)
     roof = ntt_roofline(torch, S, peaks)
     roof_stream = stream_roofline(rank_stream(rank, args.ops), S.n, S.ctx.k, S.ctx.alpha, ms / args.steps, peaks)
-    # The bootstrap, training-step and serving figures are single-GPU measurements: a run on N > 1
-    # GPUs (one replica per rank) reports the batched stream only.
+    # The bootstrap, training-step and bootstrap-serving figures are single-GPU measurements: a run
+    # on N > 1 GPUs (one replica per rank) reports the batched stream and the routed serving loop.
     single = world == 1
     boot = None
     if not args.no_boot and single:
@@ -1274,6 +1313,13 @@ def main():
         del sv
         sv = Serving(S, owners=args.serve_owners)
         serving_spill = sv.measure(args.serve_requests)
+        sv.close()
+    elif not args.no_serve:  # N GPUs: owners placed on ranks by the router, one server per rank
+        mix.batch = None
+        router = ckg.OwnerRouter([Serving.key_bytes_per_owner()] * args.serve_owners, world)
+        sv = Serving(S, owners=args.serve_owners, router=router, rank=rank)
+        serving_spill = dict(sv.measure(args.serve_requests, dist=dist), ranks=world,
+                             owners_per_rank=[len(router.owners_of(r)) for r in range(world)])
         sv.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -46,3 +46,4 @@ from .heops import (  # noqa: F401
     seal_parms_id,
 )
 from . import nn  # noqa: F401,E402
+from .router import OwnerRouter  # noqa: F401,E402
