@@ -62,6 +62,9 @@ SERVE_REQUESTS = 1000
 SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
 SERVE_BOOT_OWNERS = 8        # n16_boot serving with bootstrap requests
 SERVE_BOOT_BUDGET = 96 << 30
+SERVE_BOOT_SPILL_OWNERS = 32  # the same with key spill: up to 32 owners within host memory
+SERVE_BOOT_SPILL_BUDGET = 48 << 30
+SERVE_BOOT_SPILL_REQUESTS = 400
 
 
 def load_package():
@@ -484,8 +487,9 @@ class BootServing(Serving):
     params_text = "n16_boot: N=2^16, 32 q primes + 4x60-bit p, dnum 8, BootParams::default_n16"
     mix_text = "1/4 HMult+relin+rescale, 1/4 rotation, 3/10 64x64 BSGS plaintext mat-vec, 1/5 full SSE bootstrap"
 
-    def __init__(self, ckg, torch, device, owners=SERVE_BOOT_OWNERS, budget=SERVE_BOOT_BUDGET, seed=9):
-        self.owners = owners
+    def __init__(self, ckg, torch, device, owners=SERVE_BOOT_OWNERS, budget=SERVE_BOOT_BUDGET, seed=9,
+                 boot_lane=True):
+        self.owners, self.lanes = owners, 2 if boot_lane else 1
         self.rng = np.random.default_rng(seed)
         q, p = ckg.primes_for_bits(16, BOOT_Q_BITS, BOOT_P_BITS)
         self.ctx = ctx = ckg.Context(16, q, p, BOOT_DNUM, device=device)
@@ -504,7 +508,7 @@ class BootServing(Serving):
             return uniform(shape, torch.cat([qall[:qlimbs], qall[len(q):]]).view(1, 1, -1, 1)), shape
 
         self.ev = ckg.CudaEvaluator(ctx, None, [])
-        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=self.ev)
+        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=self.ev, boot_lane=boot_lane)
         bp = ckg.BootParams()
         self.srv.enable_bootstrap(bp, BOOT_DELTA)
         boot_steps = ckg.boot_rotation_steps(bp)
@@ -557,7 +561,29 @@ class BootServing(Serving):
 
     def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD):
         out = super().measure(requests, load)
+        out["lanes"] = self.lanes
         return out
+
+    @staticmethod
+    def owner_bytes():
+        """Pinned host bytes of one owner's keys: 38 switching keys at 32 + 4 limbs, dnum 8,
+        and the level-0 SSE key."""
+        limbs = len(BOOT_Q_BITS) + len(BOOT_P_BITS)
+        return 38 * BOOT_DNUM * 2 * limbs * (1 << 16) * 8 + 2 * (1 + len(BOOT_P_BITS)) * (1 << 16) * 8
+
+    @staticmethod
+    def spill_owners(limit=SERVE_BOOT_SPILL_OWNERS):
+        """Owners for the spill run: `limit`, or fewer so that their keys take at most an eighth
+        of the host's available memory (one GPU's share of an 8-GPU host)."""
+        avail = 0
+        try:
+            with open("/proc/meminfo") as f:
+                for line in f:
+                    if line.startswith("MemAvailable:"):
+                        avail = int(line.split()[1]) * 1024
+        except OSError:
+            pass
+        return max(2, min(limit, int(avail / 8 // BootServing.owner_bytes())))
 
 
 class BootBench:
@@ -1226,15 +1252,20 @@ def main():
     S.ctx.bconv_tc = {"int": 0, "auto": 1, "tc": 2}[args.bconv]
     S.ctx.ntt_tma = args.ntt == "tma"
     if args.serve_only:
-        sv = BootServing(ckg, torch, local)
-        out = sv.measure(args.serve_requests)
-        sv.close()
-        del sv
+        res = {}
+        for key, kw, count in (("serving", {}, args.serve_requests),
+                               ("serving_one_lane", {"boot_lane": False}, args.serve_requests),
+                               ("serving_boot_spill", {"owners": BootServing.spill_owners(),
+                                                       "budget": SERVE_BOOT_SPILL_BUDGET}, SERVE_BOOT_SPILL_REQUESTS)):
+            sv = BootServing(ckg, torch, local, **kw)
+            res[key] = sv.measure(count)
+            sv.close()
+            del sv
         sv = Serving(S, owners=args.serve_owners)
-        out2 = sv.measure(args.serve_requests)
+        res["serving_spill"] = sv.measure(args.serve_requests)
         sv.close()
         if rank == 0:
-            print(json.dumps({"serving": out, "serving_spill": out2}))
+            print(json.dumps(res))
         return
     if args.profile == "plain":
         P = Plain(S)
@@ -1304,11 +1335,19 @@ def main():
         mb = MlpBench(ckg, torch, local)
         mlp_step = mb.measure()
         del mb
-    serving = serving_spill = None
+    serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
         mix.batch = None
         sv = BootServing(ckg, torch, local)
         serving = sv.measure(args.serve_requests)
+        sv.close()
+        del sv
+        sv = BootServing(ckg, torch, local, boot_lane=False)
+        serving_one_lane = sv.measure(args.serve_requests)
+        sv.close()
+        del sv
+        sv = BootServing(ckg, torch, local, owners=BootServing.spill_owners(), budget=SERVE_BOOT_SPILL_BUDGET)
+        serving_boot_spill = sv.measure(SERVE_BOOT_SPILL_REQUESTS)
         sv.close()
         del sv
         sv = Serving(S, owners=args.serve_owners)
@@ -1339,7 +1378,8 @@ def main():
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain,
                 "keyswitch_raw": ks_raw, "ntt_pair_32_limbs": ntt32, "roofline": roof,
                 "roofline_stream": roof_stream,
-                "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_spill": serving_spill, "cpu_baseline": cpu,
+                "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_one_lane": serving_one_lane,
+                "serving_boot_spill": serving_boot_spill, "serving_spill": serving_spill, "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line))
     mix.batch = None

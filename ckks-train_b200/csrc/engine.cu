@@ -39,6 +39,33 @@ DevBuf::~DevBuf() {
 
 void Context::activate() const { CKG_CUDA(cudaSetDevice(device)); }
 
+thread_local LaneBinding tl_lane;
+
+CtxStream::operator cudaStream_t() const {
+  return tl_lane.ctx == c_ && tl_lane.lane ? tl_lane.lane->sres->s : c_->sres->s;
+}
+
+Lane::Lane(int device) {
+  sres = std::make_shared<StreamRes>();
+  sres->device = device;
+  CKG_CUDA(cudaStreamCreateWithFlags(&sres->s, cudaStreamNonBlocking));
+  sres->own = true;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  CKG_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t thr = UINT64_MAX;
+  int no = 0;
+  CKG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  CKG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+}
+
+Lane::~Lane() {
+  if (sres && sres->s) cudaStreamSynchronize(sres->s);
+  if (pool) cudaMemPoolDestroy(pool);  // released once its last block is freed
+}
+
 void Context::transfer_streams() {
   for (StreamPtr* sp : {&xfer_in, &xfer_out}) {
     if (*sp) continue;
@@ -77,7 +104,7 @@ DevBufPtr Context::upload_overlapped(const uint64_t* host, size_t words) {
   activate();
   transfer_streams();
   auto b = std::make_shared<DevBuf>();
-  b->sres = sres;  // freed in compute order, after every use there
+  b->sres = cur_sres();  // freed in compute order, after every use there
   b->device = device;
   b->words = words;
   if (!words) return b;
@@ -91,7 +118,7 @@ DevBufPtr Context::upload_overlapped_list(const std::vector<HostPart>& parts, st
   activate();
   transfer_streams();
   auto b = std::make_shared<DevBuf>();
-  b->sres = sres;
+  b->sres = cur_sres();
   b->device = device;
   offsets.assign(parts.size(), 0);
   size_t total = 0;
@@ -186,10 +213,14 @@ void Context::sync_transfers() {
 
 DevBufPtr Context::alloc(size_t words) {
   auto b = std::make_shared<DevBuf>();
-  b->sres = sres;
+  const Lane* ln = tl_lane.ctx == this ? tl_lane.lane : nullptr;
+  b->sres = ln ? ln->sres : sres;
   b->device = device;
   b->words = words;
-  if (words) CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, stream));
+  if (words) {
+    if (ln) CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, words * 8, ln->pool, ln->sres->s));
+    else CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, sres->s));
+  }
   return b;
 }
 
@@ -413,7 +444,6 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
     CKG_CUDA(cudaStreamCreateWithFlags(&sres->s, cudaStreamNonBlocking));
     sres->own = true;
   }
-  stream = sres->s;
   {  // keep freed pool memory cached: steady-state ops allocate without driver calls
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -558,6 +588,7 @@ const uint64_t* Context::x_half() {
   std::vector<LimbRef> refs;
   for (uint32_t i = 0; i <= L; ++i) refs.push_back(LimbRef{d + (size_t)i * n, d + (size_t)i * n, i, 0});
   launch_ntt(dt, refs.data(), (int)refs.size(), false, stream);
+  CKG_CUDA(cudaStreamSynchronize(stream));  // complete before any stream (lane) reads the cache
   d_xhalf = d;
   return d;
 }

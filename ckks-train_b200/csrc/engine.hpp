@@ -77,6 +77,44 @@ typedef std::shared_ptr<DevBuf> DevBufPtr;
 
 struct Context;
 
+// A compute lane: a second stream beside a context's own, with its own memory pool, which
+// reuses a freed block only once its free has completed (so the lane never waits on work
+// queued on another stream). While a thread holds a LaneScope for a context, every launch,
+// allocation and free it makes through that context goes to the lane.
+struct Lane {
+  StreamPtr sres;
+  cudaMemPool_t pool = nullptr;
+  Lane(int device);
+  ~Lane();
+  Lane(const Lane&) = delete;
+  Lane& operator=(const Lane&) = delete;
+};
+struct LaneBinding {
+  const Context* ctx = nullptr;
+  const Lane* lane = nullptr;
+};
+extern thread_local LaneBinding tl_lane;
+class LaneScope {
+ public:
+  LaneScope(const Context& c, const Lane& l) : prev_(tl_lane) { tl_lane = LaneBinding{&c, &l}; }
+  ~LaneScope() { tl_lane = prev_; }
+  LaneScope(const LaneScope&) = delete;
+  LaneScope& operator=(const LaneScope&) = delete;
+
+ private:
+  LaneBinding prev_;
+};
+
+// A context's stream as its users see it: the context's own, or the calling thread's lane.
+class CtxStream {
+ public:
+  explicit CtxStream(const Context* c) : c_(c) {}
+  operator cudaStream_t() const;
+
+ private:
+  const Context* c_;
+};
+
 // A key-switching key resident in HBM (one allocation).
 struct DevKey {
   Context* ctx = nullptr;
@@ -89,7 +127,10 @@ struct DevKey {
 struct Context {
   int device = 0;
   StreamPtr sres;
-  cudaStream_t stream = nullptr;
+  CtxStream stream{this};
+  StreamPtr cur_sres() const {  // the stream frees of buffers allocated now are ordered on
+    return tl_lane.ctx == this && tl_lane.lane ? tl_lane.lane->sres : sres;
+  }
   uint32_t log_n = 0;
   uint64_t n = 0;
   uint32_t nq = 0, k = 0, dnum = 0, alpha = 0, L = 0;

@@ -1,6 +1,7 @@
 // Serving loop (serve.hpp): admission by HBM budget, LRU key residency with spill to pinned
 // host memory, continuous batching over the Batch executor, per-request timestamps.
 #include <algorithm>
+#include <optional>
 #include <set>
 #include <unordered_set>
 
@@ -19,12 +20,17 @@ double us_since(std::chrono::steady_clock::time_point t0, std::chrono::steady_cl
 
 // A flight is what one worker iteration queued on the device: the batch of key-switching
 // ops, then each mat-vec and each bootstrap, every one closed by its own event (a segment), so
-// a request completes when its own work does.
+// a request completes when its own work does. With two lanes a flight runs on one lane's
+// stream; its outputs are handed to the context's stream once it completes.
 struct Server::Flight {
   struct Segment {
     cudaEvent_t done = nullptr;
     std::vector<ReqPtr> reqs;
   };
+  int lane = 0;
+  cudaStream_t stream = nullptr;  // where its work runs
+  bool rehome = false;            // outputs were allocated on a lane
+  size_t next_seg = 0;            // segments completed so far
   std::vector<Segment> segs;
   std::map<uint32_t, std::unique_ptr<Evaluator>> evs;  // per owner, holding the flight's keys
   std::unique_ptr<Batch> batch;                        // refers to evs: released first
@@ -61,6 +67,10 @@ Server::Server(Context* ctx, const ServerConfig& cfg) : ctx_(ctx), cfg_(cfg) {
   copy_->device = ctx_->device;
   copy_->own = true;
   CKG_CUDA(cudaStreamCreateWithFlags(&copy_->s, cudaStreamNonBlocking));
+  if (cfg_.boot_lane) {
+    batch_lane_ = std::make_unique<Lane>(ctx_->device);
+    boot_lane_ = std::make_unique<Lane>(ctx_->device);
+  }
   t0_ = Clock::now();
   key_bytes_ = std::make_shared<std::atomic<int64_t>>(0);
   worker_ = std::thread([this] { worker(); });
@@ -422,9 +432,21 @@ void Server::worker() {
   } catch (...) {
   }
   std::unique_lock<std::mutex> lk(mu_);
+  // The lane of the earliest waiting request whose lane has room (-1: none). One lane: every
+  // request is on lane 0; two: bootstraps on lane 1, and the others may pass a waiting one.
+  auto lane_of = [&](const Req& r) { return boot_lane_ && r.kind == REQ_BOOTSTRAP ? 1 : 0; };
+  auto pick = [&]() -> int {
+    for (const ReqPtr& r : pending_) {
+      const int l = lane_of(*r);
+      if (inflight_lane_[l] < cfg_.max_inflight) return l;
+      if (!boot_lane_) break;
+    }
+    return -1;
+  };
   while (true) {
-    cv_work_.wait(lk, [&] { return stop_ || (!pending_.empty() && flights_.size() < cfg_.max_inflight); });
+    cv_work_.wait(lk, [&] { return stop_ || pick() >= 0; });
     if (stop_) break;
+    const int lane = pick();
     // ---- admission (under the lock): arrival order, key-switch cap, HBM budget
     std::vector<ReqPtr> batch;
     std::vector<HostKey*> need;
@@ -432,8 +454,12 @@ void Server::worker() {
     size_t new_bytes = 0, work = 0;
     uint64_t ks = 0;
     bool wait_memory = false;
-    while (!pending_.empty()) {
-      ReqPtr r = pending_.front();
+    for (auto pit = pending_.begin(); pit != pending_.end();) {
+      ReqPtr r = *pit;
+      if (lane_of(*r) != lane) {  // the other lane's request keeps its place
+        ++pit;
+        continue;
+      }
       keys_of(*r);
       if (!batch.empty() && ks + r->ks > cfg_.max_batch_ks) break;
       if (r->kind == REQ_BOOTSTRAP && std::any_of(batch.begin(), batch.end(), [](const ReqPtr& x) {
@@ -458,7 +484,7 @@ void Server::worker() {
         if (batch.empty() && flights_.empty()) {
           // nothing on the device holds memory and every other key copy is gone: the
           // request can never fit
-          pending_.pop_front();
+          pit = pending_.erase(pit);
           finish(*r, ST_OOM,
                  "request needs " + std::to_string(extra + r->work_bytes) +
                      " bytes of device memory beyond its resident keys; the serving budget is " +
@@ -469,7 +495,7 @@ void Server::worker() {
         if (batch.empty()) wait_memory = true;
         break;
       }
-      pending_.pop_front();
+      pit = pending_.erase(pit);
       for (HostKey* hk : r->keys)
         if (need_set.insert(hk).second) {
           need.push_back(hk);
@@ -506,10 +532,23 @@ void Server::worker() {
     auto f = std::make_unique<Flight>();
     f->reqs = batch;
     f->work = work;
+    f->lane = lane;
+    Lane* ln = boot_lane_ ? (lane == 1 ? boot_lane_.get() : batch_lane_.get()) : nullptr;
+    std::optional<LaneScope> scope;  // this thread's launches through ctx_ go to the lane
+    if (ln) scope.emplace(*ctx_, *ln);
+    f->stream = ctx_->stream;
+    f->rehome = ln != nullptr;
     std::map<HostKey*, std::pair<int, std::string>> failed;
     std::map<HostKey*, KeyPtr> fresh;
     try {
       ctx_->activate();
+      if (ln) {  // the lane runs after the client's work queued on the context's stream so far
+        cudaEvent_t ready;
+        CKG_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        cudaEventRecord(ready, ctx_->sres->s);
+        cudaStreamWaitEvent(ln->sres->s, ready, 0);
+        cudaEventDestroy(ready);
+      }
       for (HostKey* hk : to_upload) {
         try {
           fresh[hk] = upload(hk);
@@ -651,6 +690,7 @@ void Server::worker() {
     st_.batches++;
     if (owners_in_batch.size() > 1) st_.multi_owner_batches++;
     st_.max_batch_requests = std::max<uint64_t>(st_.max_batch_requests, batch.size());
+    inflight_lane_[lane]++;
     flights_.push_back(f.release());
     building_ = false;
     cv_flight_.notify_all();
@@ -662,66 +702,82 @@ void Server::completer() {
     ctx_->activate();
   } catch (...) {
   }
+  // Flights complete in any order (two lanes): each pass polls every queued flight's next
+  // segments, completes what is done and releases finished flights.
   while (true) {
-    Flight* f = nullptr;
+    std::vector<Flight*> snap;
     {
       std::unique_lock<std::mutex> lk(mu_);
       cv_flight_.wait(lk, [&] { return !flights_.empty() || worker_exited_; });
       if (flights_.empty()) break;
-      f = flights_.front();
+      snap.assign(flights_.begin(), flights_.end());
     }
-    for (auto& seg : f->segs) {  // each segment completes its own requests
-      cudaError_t e = cudaSuccess;
-      if (seg.done) {
-        while ((e = cudaEventQuery(seg.done)) == cudaErrorNotReady)
-          std::this_thread::sleep_for(std::chrono::microseconds(20));
-      } else {
-        // No completion event could be created: wait for the whole compute stream, so the
-        // flight's working space and keys are released only after its kernels have run.
-        cudaStreamSynchronize(ctx_->stream);
-        e = cudaErrorUnknown;
+    bool progress = false;
+    for (Flight* f : snap) {
+      while (f->next_seg < f->segs.size()) {  // each segment completes its own requests
+        auto& seg = f->segs[f->next_seg];
+        cudaError_t e = cudaSuccess;
+        if (seg.done) {
+          e = cudaEventQuery(seg.done);
+          if (e == cudaErrorNotReady) break;
+        } else {
+          // No completion event could be created: wait for the flight's whole stream, so the
+          // flight's working space and keys are released only after its kernels have run.
+          cudaStreamSynchronize(f->stream);
+          e = cudaErrorUnknown;
+        }
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          const auto t = Clock::now();
+          for (auto& r : seg.reqs) {
+            if (r->status != -1) continue;
+            if (e == cudaSuccess) {
+              // a lane's output is freed on the context's stream from now on, after the
+              // client's later work on it
+              if (f->rehome && r->out) r->out->buf->sres = ctx_->sres;
+              finish(*r, ST_OK, "");
+              r->t_done = t;
+            } else {
+              finish(*r, ST_DEVICE, std::string("device error in a served batch: ") + cudaGetErrorString(e));
+            }
+          }
+        }
+        cv_done_.notify_all();
+        f->next_seg++;
+        progress = true;
       }
+      if (f->next_seg < f->segs.size()) continue;
       {
         std::lock_guard<std::mutex> lk(mu_);
-        const auto t = Clock::now();
-        for (auto& r : seg.reqs) {
-          if (r->status != -1) continue;
-          if (e == cudaSuccess) {
-            finish(*r, ST_OK, "");
-            r->t_done = t;
-          } else {
-            finish(*r, ST_DEVICE, std::string("device error in a served batch: ") + cudaGetErrorString(e));
-          }
+        for (auto& kv : f->evs) {
+          OpCounter c = kv.second->counter();
+          OpCounter& o = owners_[kv.first]->counter;
+          o.rotations += c.rotations;
+          o.relins += c.relins;
+          o.ct_ct_tensor += c.ct_ct_tensor;
+          o.ct_pt_mults += c.ct_pt_mults;
+          o.rescales += c.rescales;
+          o.sse_switches += c.sse_switches;
+          o.bootstraps += c.bootstraps;
         }
       }
       cv_done_.notify_all();
-    }
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      for (auto& kv : f->evs) {
-        OpCounter c = kv.second->counter();
-        OpCounter& o = owners_[kv.first]->counter;
-        o.rotations += c.rotations;
-        o.relins += c.relins;
-        o.ct_ct_tensor += c.ct_ct_tensor;
-        o.ct_pt_mults += c.ct_pt_mults;
-        o.rescales += c.rescales;
-        o.sse_switches += c.sse_switches;
-        o.bootstraps += c.bootstraps;
+      // release the flight's keys and working space, then let the worker admit more
+      const size_t work = f->work;
+      const int lane = f->lane;
+      delete f;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        flights_.erase(std::find(flights_.begin(), flights_.end(), f));
+        inflight_work_ -= work;
+        inflight_lane_[lane]--;
+        done_gen_++;
       }
+      progress = true;
+      cv_work_.notify_all();
+      cv_done_.notify_all();
     }
-    cv_done_.notify_all();
-    // release the batch's keys and working space, then let the worker admit more
-    const size_t work = f->work;
-    delete f;
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      flights_.pop_front();
-      inflight_work_ -= work;
-      done_gen_++;
-    }
-    cv_work_.notify_all();
-    cv_done_.notify_all();
+    if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
 }
 

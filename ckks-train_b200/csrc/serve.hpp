@@ -38,8 +38,11 @@ constexpr int ST_CANCELLED = 9;  // request cancelled before it was admitted
 struct ServerConfig {
   size_t hbm_budget = 0;         // bytes: device key copies + working space of queued batches
   uint32_t max_batch_ks = 128;   // key switches admitted into one batch
-  uint32_t max_inflight = 2;     // batches queued on the device at once
+  uint32_t max_inflight = 2;     // batches queued on the device at once (per lane)
   EvalConfig eval;
+  // Two compute lanes: bootstrap flights on one stream, every other flight on another, both
+  // beside the context's stream (which then carries only the client's own work).
+  bool boot_lane = false;
 };
 
 struct ServerStats {
@@ -138,6 +141,8 @@ class Server {
   std::unordered_map<uint64_t, ReqPtr> reqs_;
   std::deque<ReqPtr> pending_;
   std::deque<Flight*> flights_;
+  uint32_t inflight_lane_[2] = {0, 0};           // flights queued per lane
+  std::unique_ptr<Lane> batch_lane_, boot_lane_;  // with cfg_.boot_lane
   std::list<HostKey*> lru_;  // front = most recently used
   size_t inflight_work_ = 0;
   uint64_t next_id_ = 1;

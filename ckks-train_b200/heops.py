@@ -952,14 +952,17 @@ SERVER_STATS = ("submitted", "completed", "failed", "cancelled", "batches", "mul
                 "peak_key_bytes", "peak_device_bytes", "budget_waits", "pending", "hbm_budget")
 
 
+SERVE_BOOT_LANE = 256  # CKG_SERVE_BOOT_LANE
+
+
 class Server:
     """Serving loop over one context (include/ckg.h, "serving loop"): requests from many key
     owners, admitted by HBM budget with LRU key spill to pinned host memory and run with
     continuous batching. `ev` is any evaluator of the context; results are wrapped with it."""
 
-    def __init__(self, ctx, hbm_budget, max_batch_ks=128, max_inflight=2, config=None, ev=None):
+    def __init__(self, ctx, hbm_budget, max_batch_ks=128, max_inflight=2, config=None, ev=None, boot_lane=False):
         self.ctx, self.ev = ctx, ev
-        flags = (config or EvalConfig()).flags
+        flags = (config or EvalConfig()).flags | (SERVE_BOOT_LANE if boot_lane else 0)
         h = VP()
         _check(lib().ckg_server_create(ctx.h, int(hbm_budget), max_batch_ks, max_inflight, flags, C.byref(h)))
         self.h = h

@@ -254,11 +254,13 @@ def test_serve_cancel_and_drain(owners, ckg):
     srv.close()
 
 
-def test_serve_bootstrap_requests(ckg, oracle):
+@pytest.mark.parametrize("boot_lane", [False, True])
+def test_serve_bootstrap_requests(ckg, oracle, boot_lane):
     """Bootstrap requests from two owners (each with its own relinearization, rotation,
-    conjugation and SSE keys) served beside rotations and HMults, on the reference's N = 2^10
-    bootstrap chain: every output equals the oracle's and each owner's OpCounter equals the
-    CPU's."""
+    conjugation and SSE keys) served beside rotations, on the reference's N = 2^10 bootstrap
+    chain, on one compute lane and on two (bootstraps on their own lane, overlapping the
+    rotations): every output equals the oracle's, each owner's OpCounter equals the CPU's, and
+    outputs handed back from a lane are then used by the context's own stream."""
     O = oracle
     q_bits = [54, 42, 42] + [34] * 4 + [58] * 7 + [56] * 4
     delta = 2.0 ** 42
@@ -266,7 +268,7 @@ def test_serve_bootstrap_requests(ckg, oracle):
     enc = O.Encoder(P)
     ctx = ckg.Context(10, P.q, P.p, 9, scale=delta)
     io = ckg.CudaEvaluator(ctx, None, [])
-    srv = ckg.Server(ctx, 2 << 30, max_batch_ks=32, max_inflight=2, ev=io)
+    srv = ckg.Server(ctx, 2 << 30, max_batch_ks=32, max_inflight=2, ev=io, boot_lane=boot_lane)
     srv.enable_bootstrap(ckg.BootParams(log_slots=9), delta)
     owners = []
     for o in range(2):
@@ -301,6 +303,10 @@ def test_serve_bootstrap_requests(ckg, oracle):
         got, scale = io.download_ct(ct)
         assert scale == want.scale and ct.level() == want.level
         assert_same(got, want.data(), f"served {kind} owner {o}")
+        twice = io.add(ct, ct)  # the context's stream reads the output, then the handle goes
+        del ct
+        got2, _ = io.download_ct(twice)
+        assert_same(got2, ev.add(want, want).data(), f"served {kind} owner {o}, used after completion")
     for o, (kg, rk, bs, ev) in enumerate(owners):
         assert srv.owner_counter(o) == ev.counter(), f"owner {o} counter"
     st = srv.stats()
