@@ -316,13 +316,19 @@ class Plain:
         self.cts = [S.ct(PLAIN_LEVEL)[0] for _ in range(PLAIN_CTS)]
         self.ks = 2 * PLAIN_CTS
 
+    slowest = (0.0, None)  # (host seconds, op) of the slowest evaluator call so far
+
     def step(self):
         ev, cts = self.S.ev, self.cts
-        out = []
+        out, clock = [], time.perf_counter
         for i in range(PLAIN_CTS):
+            t0 = clock()
             out.append(ev.rescale(ev.mul(cts[i], cts[(i + 1) % PLAIN_CTS])))
+            self.slowest = max(self.slowest, (clock() - t0, f"mul {i}"))
         for i in range(PLAIN_CTS):
+            t0 = clock()
             out.append(ev.rotate(cts[i], ROT_STEPS[i % len(ROT_STEPS)]))
+            self.slowest = max(self.slowest, (clock() - t0, f"rotate {i}"))
         return out
 
 
@@ -1307,7 +1313,9 @@ def main():
         # section, once in the middle of a per-op run): garbage collected, three warm-up steps, and
         # the better of two timed runs of two steps each (every rank runs both, as timed() reduces).
         gc.collect()
-        ms_p = min(timed(torch, S.ctx, P.step, 2, 3, dist)[0] for _ in range(2))
+        free0 = torch.cuda.mem_get_info()[0]
+        runs_p = [timed(torch, S.ctx, P.step, 2, 3, dist)[0] for _ in range(2)]
+        ms_p = min(runs_p)
         pv = P.ks * 2 * world / (ms_p * 1e-3)
         PM = PlainMix(mix)
         ms_m = min(timed(torch, S.ctx, PM.step, 2, 3, dist)[0] for _ in range(2))
@@ -1316,7 +1324,10 @@ def main():
                  "workload": "128 ciphertexts at 24 limbs: 128 x (HMult+relin+rescale) + 128 rotations, "
                              "one evaluator call per op; better of two timed runs of 2 steps after 3 warm-up steps",
                  "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
-                 "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2)}
+                 "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2),
+                 "runs_ms": [round(x, 3) for x in runs_p],
+                 "slowest_host_call": [round(P.slowest[0] * 1e3, 3), P.slowest[1]],
+                 "device_free_gib_before": round(free0 / 2 ** 30, 1)}
     ks_raw = raw_keyswitch(torch, lambda i, b, a: S.ctx.key_switch(S.relin, i, PLAIN_LEVEL, b, a), S.ctx.stream,
                            S.q_all, S.n)
     ntt32 = ntt_32_limbs(torch, lambda buf, primes, inv: S.ctx.ntt(buf, buf, primes, inv), S.ctx.stream, S.n)
