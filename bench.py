@@ -1336,19 +1336,27 @@ def main():
     # The bootstrap, training-step and bootstrap-serving figures are single-GPU measurements: a run
     # on N > 1 GPUs (one replica per rank) reports the batched stream and the routed serving loop.
     single = world == 1
+
+    def release():
+        """Drops the batched stream's graph and the torch allocator's cached blocks between
+        sections (untimed), so later sections' own pools find the device memory free."""
+        mix.batch = None
+        gc.collect()
+        torch.cuda.empty_cache()
+
     boot = None
     if not args.no_boot and single:
-        mix.batch = None
+        release()
         boot = BootBench(ckg, torch, local).measure()
     mlp_step = None
     if not args.no_mlp and single:
-        mix.batch = None
+        release()
         mb = MlpBench(ckg, torch, local)
         mlp_step = mb.measure()
         del mb
     serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
-        mix.batch = None
+        release()
         sv = BootServing(ckg, torch, local)
         serving = sv.measure(args.serve_requests)
         sv.close()
@@ -1365,7 +1373,7 @@ def main():
         serving_spill = sv.measure(args.serve_requests)
         sv.close()
     elif not args.no_serve:  # N GPUs: owners placed on ranks by the router, one server per rank
-        mix.batch = None
+        release()
         router = ckg.OwnerRouter([Serving.key_bytes_per_owner()] * args.serve_owners, world)
         sv = Serving(S, owners=args.serve_owners, router=router, rank=rank)
         serving_spill = dict(sv.measure(args.serve_requests, dist=dist), ranks=world,

@@ -218,8 +218,21 @@ DevBufPtr Context::alloc(size_t words) {
   b->device = device;
   b->words = words;
   if (words) {
-    if (ln) CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, words * 8, ln->pool, ln->sres->s));
-    else CKG_CUDA(cudaMallocAsync((void**)&b->p, words * 8, sres->s));
+    auto get = [&] {
+      return ln ? cudaMallocFromPoolAsync((void**)&b->p, words * 8, ln->pool, ln->sres->s)
+                : cudaMallocAsync((void**)&b->p, words * 8, sres->s);
+    };
+    cudaError_t e = get();
+    if (e == cudaErrorMemoryAllocation) {
+      // Free memory may sit cached in another pool (each keeps what it frees): hand the unused
+      // blocks of the device's default pool and of the upload pool back, then try once more.
+      cudaGetLastError();
+      cudaMemPool_t def;
+      if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+      if (xpool) cudaMemPoolTrimTo(xpool, 0);
+      e = get();
+    }
+    if (e != cudaSuccess) throw_cuda(e, "device allocation");
   }
   return b;
 }
