@@ -250,18 +250,20 @@ class Mix:
             lv = level if kind == "rot" else level - 1
             self.out_host.append(torch.empty((2, lv + 1, self.S.n), dtype=torch.int64, pin_memory=True))
         self.out_ptrs = [t.data_ptr() for t in self.out_host]
-        self.inflight, self.host_s = [], 0.0
+        self.inflight, self.host_s, self.host_parts = [], 0.0, {}
         self.stream = torch.cuda.ExternalStream(self.S.ctx.stream)
 
     def step_e2e(self):
         """Upload every input from pinned host memory, build and run the batch, download every
         result to pinned host memory, through the C ABI's overlapped list transfers (one call
-        per list): this step's uploads run beside the previous step's compute and downloads. At
-        most two steps are in flight (the host waits for the compute of the step before last)."""
-        torch, ev = self.S.torch, self.S.ev
+        per list): this step's uploads run beside the previous step's compute and downloads. The
+        step's handles are dropped before its completion event is recorded, so that event also
+        covers the frees of its buffers; the host waits for the event of the step before last, so
+        at most two steps are in flight and each upload reuses memory whose free has completed."""
+        torch, ev, clock = self.S.torch, self.S.ev, time.perf_counter
         if len(self.inflight) >= 2:
             self.inflight.pop(0).synchronize()
-        t0 = time.perf_counter()
+        t0 = clock()
         ct_items, pt_items, h2d = [], [], 0
         for (kind, level, steps), (ha, hb) in zip(self.ops, self.host):
             ct_items.append((ha.data_ptr(), 2, level, SCALE))
@@ -278,14 +280,21 @@ class Mix:
         for kind, level, steps in self.ops:
             a = next(cts)
             ins.append((kind, a, next(cts) if kind == "mul" else (next(pts) if kind == "pmul" else None), steps))
+        t1 = clock()
         b, outs = self.make_batch(ins)
+        t2 = clock()
         b.run()
+        t3 = clock()
+        ev.download_ct_overlap_list(outs, self.out_ptrs)
+        del b, outs, ins, cts, pts
         e = torch.cuda.Event()
         e.record(self.stream)
         self.inflight.append(e)
-        ev.download_ct_overlap_list(outs, self.out_ptrs)
+        t4 = clock()
         d2h = sum(t.numel() * 8 for t in self.out_host)
-        self.host_s += time.perf_counter() - t0
+        for k, dt in zip(("upload", "batch_build", "run", "download_and_release"), (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+            self.host_parts[k] = self.host_parts.get(k, 0.0) + dt
+        self.host_s += t4 - t0
         return h2d, d2h
 
 
@@ -438,17 +447,18 @@ class Serving:
         th.join()
         return np.array([(t[0], t[2]) for t in times]).reshape(-1, 2), lag[0]
 
-    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD, dist=None):
-        """Capacity (saturated), then `requests` Poisson arrivals at `load` x capacity. With `dist`
-        (one rank per GPU, owners placed by the router) capacity is the sum over ranks, the
-        latencies of all ranks are pooled and the span is the longest rank's."""
+    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD, dist=None, rate=None):
+        """Capacity (saturated), then `requests` Poisson arrivals at `load` x capacity, or at
+        `rate` requests/s when given (to compare servers at one offered load). With `dist` (one
+        rank per GPU, owners placed by the router) capacity is the sum over ranks, the latencies of
+        all ranks are pooled and the span is the longest rank's."""
         self.run(96)  # warm-up: Galois permutations, pools, first key uploads
         sat, _ = self.run(min(400, requests))
         capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6) if len(sat) else 0.0
         if dist:
             capacity = sum(gather_objects(dist, capacity))
         st0 = self.srv.stats()
-        rate = load * capacity
+        rate = rate or load * capacity
         t, lag = self.run(requests, rate)
         st = self.srv.stats()
         lat = (t[:, 1] - t[:, 0]) * 1e-3
@@ -565,8 +575,8 @@ class BootServing(Serving):
             return lambda: self.srv.submit_matvec(o, SERVE_D, 1, self.diag, a)
         return lambda: self.srv.submit_bootstrap(o, self.level0[o])
 
-    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD):
-        out = super().measure(requests, load)
+    def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD, rate=None):
+        out = super().measure(requests, load, rate=rate)
         out["lanes"] = self.lanes
         return out
 
@@ -579,8 +589,8 @@ class BootServing(Serving):
 
     @staticmethod
     def spill_owners(limit=SERVE_BOOT_SPILL_OWNERS):
-        """Owners for the spill run: `limit`, or fewer so that their keys take at most an eighth
-        of the host's available memory (one GPU's share of an 8-GPU host)."""
+        """Owners for the spill run: `limit`, or fewer so that their pinned keys take at most half
+        of the host's available memory."""
         avail = 0
         try:
             with open("/proc/meminfo") as f:
@@ -589,7 +599,7 @@ class BootServing(Serving):
                         avail = int(line.split()[1]) * 1024
         except OSError:
             pass
-        return max(2, min(limit, int(avail / 8 // BootServing.owner_bytes())))
+        return max(2, min(limit, int(avail / 2 // BootServing.owner_bytes())))
 
 
 class BootBench:
@@ -1259,12 +1269,13 @@ def main():
     S.ctx.ntt_tma = args.ntt == "tma"
     if args.serve_only:
         res = {}
-        for key, kw, count in (("serving", {}, args.serve_requests),
-                               ("serving_one_lane", {"boot_lane": False}, args.serve_requests),
+        for key, kw, count in (("serving_one_lane", {"boot_lane": False}, args.serve_requests),
+                               ("serving", {}, args.serve_requests),
                                ("serving_boot_spill", {"owners": BootServing.spill_owners(),
                                                        "budget": SERVE_BOOT_SPILL_BUDGET}, SERVE_BOOT_SPILL_REQUESTS)):
             sv = BootServing(ckg, torch, local, **kw)
-            res[key] = sv.measure(count)
+            rate = res["serving_one_lane"]["offered_req_s"] if key == "serving" else None
+            res[key] = sv.measure(count, rate=rate)
             sv.close()
             del sv
         sv = Serving(S, owners=args.serve_owners)
@@ -1298,12 +1309,13 @@ def main():
         steps_e = max(8, args.steps)
         mix.step_e2e()
         mix.inflight.clear()
-        mix.host_s = 0.0
+        mix.host_s, mix.host_parts = 0.0, {}
         ms_e, (h2d, d2h) = timed(torch, S.ctx, mix.step_e2e, steps_e, 0, dist, tail=S.ctx.join_transfers)
         e2e = {"value": round(mix.ks * steps_e * world / (ms_e * 1e-3), 2), "unit": unit,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": round(ms_e / steps_e, 3), "steps": steps_e,
-               "host_ms_per_step": round(mix.host_s * 1e3 / steps_e, 2)}
+               "host_ms_per_step": round(mix.host_s * 1e3 / steps_e, 2),
+               "host_ms_per_step_by_phase": {k: round(v * 1e3 / steps_e, 2) for k, v in mix.host_parts.items()}}
         if rank == 0:  # no collective inside: the other ranks skip it
             e2e["host_link"] = pcie_ceiling(torch, h2d, d2h, ms_e / steps_e)
     plain = None
@@ -1357,12 +1369,12 @@ def main():
     serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
         release()
-        sv = BootServing(ckg, torch, local)
-        serving = sv.measure(args.serve_requests)
-        sv.close()
-        del sv
         sv = BootServing(ckg, torch, local, boot_lane=False)
         serving_one_lane = sv.measure(args.serve_requests)
+        sv.close()
+        del sv
+        sv = BootServing(ckg, torch, local)  # two lanes, at the one-lane run's offered load
+        serving = sv.measure(args.serve_requests, rate=serving_one_lane["offered_req_s"])
         sv.close()
         del sv
         sv = BootServing(ckg, torch, local, owners=BootServing.spill_owners(), budget=SERVE_BOOT_SPILL_BUDGET)

@@ -374,11 +374,10 @@ void Batch::build() {
     S.fwd_rs = db.put(fwd_rs);
     S.fin_rs = db.put(fin_rs);
   }
-  // An asynchronous copy from pageable memory has staged the source when it returns, so
-  // `db` may go away at once and the host does not wait for work already on the stream.
+  // Through the context's pinned staging ring: the host does not wait for work already on
+  // the stream, and `db` may go away at once.
   desc_ = c.alloc((db.bytes.size() + 7) / 8);
-  if (!db.bytes.empty())
-    CKG_CUDA(cudaMemcpyAsync(desc_->p, db.bytes.data(), db.bytes.size(), cudaMemcpyHostToDevice, c.stream));
+  c.upload_staged(desc_->p, db.bytes.data(), db.bytes.size());
   for (auto& s : stages) chunks_.push_back(new Stage(s));
   built_ = true;
 }

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -84,7 +85,7 @@ struct Context;
 struct Lane {
   StreamPtr sres;
   cudaMemPool_t pool = nullptr;
-  Lane(int device);
+  Lane(int device, int priority = 0);  // stream priority (lower number: scheduled first)
   ~Lane();
   Lane(const Lane&) = delete;
   Lane& operator=(const Lane&) = delete;
@@ -193,6 +194,20 @@ struct Context {
   void download_overlapped_list(const std::vector<DevPart>& parts);
   void join_transfers();  // `stream` waits for every transfer queued so far
   void sync_transfers();  // the host waits for them
+
+  // Host-built records (batch work lists) copied to the device on `stream` through a pinned
+  // staging ring, so the call returns at once: a copy from pageable memory can make the host
+  // wait for the work already queued on the stream. A slot is reused once its copy completed.
+  // Not allowed while the stream is being captured (the graph would read a reused slot).
+  void upload_staged(void* dst, const void* src, size_t bytes);
+  std::mutex stage_mu;
+  unsigned char* stage = nullptr;
+  size_t stage_cap = 0, stage_head = 0;
+  struct StageUse {
+    size_t off, len;
+    cudaEvent_t done;
+  };
+  std::deque<StageUse> stage_used;
 };
 
 // ---- polynomial-level algorithms (all asynchronous on ctx.stream) -------------------

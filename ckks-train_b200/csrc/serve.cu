@@ -68,8 +68,12 @@ Server::Server(Context* ctx, const ServerConfig& cfg) : ctx_(ctx), cfg_(cfg) {
   copy_->own = true;
   CKG_CUDA(cudaStreamCreateWithFlags(&copy_->s, cudaStreamNonBlocking));
   if (cfg_.boot_lane) {
-    batch_lane_ = std::make_unique<Lane>(ctx_->device);
-    boot_lane_ = std::make_unique<Lane>(ctx_->device);
+    // Bootstraps are the long chains of small launches that bound the tail: their lane gets the
+    // device's highest stream priority, and the batches fill the SMs they leave idle.
+    int least = 0, greatest = 0;
+    CKG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    batch_lane_ = std::make_unique<Lane>(ctx_->device, least);
+    boot_lane_ = std::make_unique<Lane>(ctx_->device, greatest);
   }
   t0_ = Clock::now();
   key_bytes_ = std::make_shared<std::atomic<int64_t>>(0);

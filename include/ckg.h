@@ -441,8 +441,9 @@ CKG_API int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double del
 typedef struct ckg_server ckg_server;
 enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVEC = 3, CKG_REQ_BOOTSTRAP = 4 };
 /* ckg_server_create flag beside the CKG_HOIST / CKG_BSGS / CKG_LAZY_RELIN bits: two compute
- * lanes, bootstrap flights on one stream and all other flights on another (each with its own
- * memory pool and up to max_inflight flights), so bootstraps overlap the other requests. Both
+ * lanes, bootstrap flights on one stream (the device's highest stream priority) and all other
+ * flights on another (each with its own memory pool and up to max_inflight flights), so
+ * bootstraps overlap the other requests. Both
  * lanes start after the client's work queued on the context's stream when the flight is
  * built, and every output is handed back to the context's stream when its request completes. */
 enum { CKG_SERVE_BOOT_LANE = 256 };
