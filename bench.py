@@ -62,6 +62,7 @@ SERVE_REQUESTS = 1000
 SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
 SERVE_BOOT_OWNERS = 8        # n16_boot serving with bootstrap requests
 SERVE_BOOT_BUDGET = 96 << 30
+SERVE_BOOT_LANES = 1          # bootstrap lanes of the bootstrap-serving runs (0: one stream)
 SERVE_BOOT_SPILL_OWNERS = 32  # the same with key spill: up to 32 owners within host memory
 SERVE_BOOT_SPILL_BUDGET = 48 << 30
 SERVE_BOOT_SPILL_REQUESTS = 400
@@ -276,25 +277,25 @@ class Mix:
                 h2d += hb.numel() * 8
         cts = iter(ev.upload_ct_overlap_list(ct_items))
         pts = iter(ev.upload_pt_overlap_list(pt_items) if pt_items else [])
-        ins = []
-        for kind, level, steps in self.ops:
-            a = next(cts)
-            ins.append((kind, a, next(cts) if kind == "mul" else (next(pts) if kind == "pmul" else None), steps))
+        ins = [(kind, next(cts), next(cts) if kind == "mul" else (next(pts) if kind == "pmul" else None), steps)
+               for kind, level, steps in self.ops]
         t1 = clock()
         b, outs = self.make_batch(ins)
         t2 = clock()
         b.run()
         t3 = clock()
         ev.download_ct_overlap_list(outs, self.out_ptrs)
-        del b, outs, ins, cts, pts
+        t4 = clock()
+        del b, outs, ins, cts, pts  # every handle of the step: its frees are queued here
         e = torch.cuda.Event()
         e.record(self.stream)
         self.inflight.append(e)
-        t4 = clock()
+        t5 = clock()
         d2h = sum(t.numel() * 8 for t in self.out_host)
-        for k, dt in zip(("upload", "batch_build", "run", "download_and_release"), (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+        for k, dt in zip(("upload", "batch_build", "run", "download", "release"),
+                         (t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4)):
             self.host_parts[k] = self.host_parts.get(k, 0.0) + dt
-        self.host_s += t4 - t0
+        self.host_s += t5 - t0
         return h2d, d2h
 
 
@@ -504,8 +505,8 @@ class BootServing(Serving):
     mix_text = "1/4 HMult+relin+rescale, 1/4 rotation, 3/10 64x64 BSGS plaintext mat-vec, 1/5 full SSE bootstrap"
 
     def __init__(self, ckg, torch, device, owners=SERVE_BOOT_OWNERS, budget=SERVE_BOOT_BUDGET, seed=9,
-                 boot_lane=True):
-        self.owners, self.lanes = owners, 2 if boot_lane else 1
+                 boot_lanes=SERVE_BOOT_LANES, boot_priority=True):
+        self.owners, self.lanes = owners, {"boot_lanes": boot_lanes, "boot_priority": boot_priority}
         self.rng = np.random.default_rng(seed)
         q, p = ckg.primes_for_bits(16, BOOT_Q_BITS, BOOT_P_BITS)
         self.ctx = ctx = ckg.Context(16, q, p, BOOT_DNUM, device=device)
@@ -524,7 +525,8 @@ class BootServing(Serving):
             return uniform(shape, torch.cat([qall[:qlimbs], qall[len(q):]]).view(1, 1, -1, 1)), shape
 
         self.ev = ckg.CudaEvaluator(ctx, None, [])
-        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=self.ev, boot_lane=boot_lane)
+        self.srv = ckg.Server(ctx, budget, max_batch_ks=256, max_inflight=2, ev=self.ev, boot_lanes=boot_lanes,
+                              boot_priority=boot_priority)
         bp = ckg.BootParams()
         self.srv.enable_bootstrap(bp, BOOT_DELTA)
         boot_steps = ckg.boot_rotation_steps(bp)
@@ -1168,6 +1170,8 @@ def main():
     ap.add_argument("--no-boot", action="store_true")
     ap.add_argument("--boot-only", action="store_true", help="measure the n16_boot bootstrap only")
     ap.add_argument("--serve-only", action="store_true", help="set up and measure the serving loop only")
+    ap.add_argument("--serve-lane-sweep", action="store_true",
+                    help="measure bootstrap serving under each compute-lane layout at one offered load")
     ap.add_argument("--no-mlp", action="store_true")
     ap.add_argument("--ntt", default="plain", choices=["tma", "plain"],
                     help="NTT column passes: per-tile (plain, the default) or persistent TMA-staged (tma)")
@@ -1267,9 +1271,23 @@ def main():
     S = Setup(ckg, torch, local)
     S.ctx.bconv_tc = {"int": 0, "auto": 1, "tc": 2}[args.bconv]
     S.ctx.ntt_tma = args.ntt == "tma"
+    if args.serve_lane_sweep:  # bootstrap serving under every lane layout, one offered load
+        res, rate = {}, None
+        for lanes, prio in ((0, True), (1, True), (1, False), (2, True), (2, False)):
+            sv = BootServing(ckg, torch, local, boot_lanes=lanes, boot_priority=prio)
+            out = sv.measure(args.serve_requests, rate=rate)
+            rate = rate or out["offered_req_s"]
+            res[f"lanes{lanes}_{'prio' if prio else 'equal'}"] = {
+                k: out[k] for k in ("capacity_req_s", "offered_req_s", "throughput_req_s", "p50_ms", "p99_ms",
+                                    "mean_ms", "key_hit_rate", "key_evictions", "batches")}
+            sv.close()
+            del sv
+        if rank == 0:
+            print(json.dumps({"serving_lane_sweep": res}))
+        return
     if args.serve_only:
         res = {}
-        for key, kw, count in (("serving_one_lane", {"boot_lane": False}, args.serve_requests),
+        for key, kw, count in (("serving_one_lane", {"boot_lanes": 0}, args.serve_requests),
                                ("serving", {}, args.serve_requests),
                                ("serving_boot_spill", {"owners": BootServing.spill_owners(),
                                                        "budget": SERVE_BOOT_SPILL_BUDGET}, SERVE_BOOT_SPILL_REQUESTS)):
@@ -1321,24 +1339,20 @@ def main():
     plain = None
     if not args.no_plain:
         P = Plain(S)
-        # The per-op calls stall on the host now and then (90-420 ms seen after the batched
-        # section, once in the middle of a per-op run): garbage collected, three warm-up steps, and
-        # the better of two timed runs of two steps each (every rank runs both, as timed() reduces).
-        gc.collect()
+        # One timed run of 4 steps after 3 warm-up steps; the slowest evaluator call's host time is
+        # reported beside it, so a host stall inside the run shows in the line.
         free0 = torch.cuda.mem_get_info()[0]
-        runs_p = [timed(torch, S.ctx, P.step, 2, 3, dist)[0] for _ in range(2)]
-        ms_p = min(runs_p)
-        pv = P.ks * 2 * world / (ms_p * 1e-3)
+        ms_p = timed(torch, S.ctx, P.step, 4, 3, dist)[0]
+        pv = P.ks * 4 * world / (ms_p * 1e-3)
         PM = PlainMix(mix)
-        ms_m = min(timed(torch, S.ctx, PM.step, 2, 3, dist)[0] for _ in range(2))
+        ms_m = timed(torch, S.ctx, PM.step, 2, 3, dist)[0]
         pm = PM.ks * 2 * world / (ms_m * 1e-3)
         plain = {"value": round(pv, 2), "unit": unit,
                  "workload": "128 ciphertexts at 24 limbs: 128 x (HMult+relin+rescale) + 128 rotations, "
-                             "one evaluator call per op; better of two timed runs of 2 steps after 3 warm-up steps",
-                 "ms_per_step": round(ms_p / 2, 3), "batched_over_plain": round(value / pv, 2),
+                             "one evaluator call per op; 4 timed steps after 3 warm-up steps",
+                 "ms_per_step": round(ms_p / 4, 3), "batched_over_plain": round(value / pv, 2),
                  "same_stream_one_op_at_a_time": round(pm, 2), "batched_over_same_stream_plain": round(value / pm, 2),
-                 "runs_ms": [round(x, 3) for x in runs_p],
-                 "slowest_host_call": [round(P.slowest[0] * 1e3, 3), P.slowest[1]],
+                 "slowest_host_call_ms": [round(P.slowest[0] * 1e3, 3), P.slowest[1]],
                  "device_free_gib_before": round(free0 / 2 ** 30, 1)}
     ks_raw = raw_keyswitch(torch, lambda i, b, a: S.ctx.key_switch(S.relin, i, PLAIN_LEVEL, b, a), S.ctx.stream,
                            S.q_all, S.n)
@@ -1369,7 +1383,7 @@ def main():
     serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
         release()
-        sv = BootServing(ckg, torch, local, boot_lane=False)
+        sv = BootServing(ckg, torch, local, boot_lanes=0)
         serving_one_lane = sv.measure(args.serve_requests)
         sv.close()
         del sv

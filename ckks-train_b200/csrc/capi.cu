@@ -1102,7 +1102,8 @@ int ckg_server_create(ckg_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t max_batc
   cfg.max_batch_ks = max_batch_ks;
   cfg.max_inflight = max_inflight;
   cfg.eval = EvalConfig{(flags & CKG_HOIST) != 0, (flags & CKG_BSGS) != 0, (flags & CKG_LAZY_RELIN) != 0};
-  cfg.boot_lane = (flags & CKG_SERVE_BOOT_LANE) != 0;
+  cfg.boot_lanes = (flags & CKG_SERVE_BOOT_LANES_2) ? 2 : (flags & CKG_SERVE_BOOT_LANE) ? 1 : 0;
+  cfg.boot_priority = (flags & CKG_SERVE_LANES_EQUAL_PRIORITY) == 0;
   auto h = new ckg_server{std::make_unique<Server>(&ctx_of(ctx), cfg), hbm_budget_bytes};
   *out = h;
   CKG_API_END

@@ -67,14 +67,17 @@ Server::Server(Context* ctx, const ServerConfig& cfg) : ctx_(ctx), cfg_(cfg) {
   copy_->device = ctx_->device;
   copy_->own = true;
   CKG_CUDA(cudaStreamCreateWithFlags(&copy_->s, cudaStreamNonBlocking));
-  if (cfg_.boot_lane) {
-    // Bootstraps are the long chains of small launches that bound the tail: their lane gets the
-    // device's highest stream priority, and the batches fill the SMs they leave idle.
+  if (cfg_.boot_lanes > 4) throw Error(ST_INVALID_PARAMS, "at most 4 bootstrap lanes");
+  if (cfg_.boot_lanes) {
+    // Bootstraps are long chains of small launches that bound the tail: their lanes may get the
+    // device's highest stream priority, so the batches fill the SMs they leave idle.
     int least = 0, greatest = 0;
     CKG_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    batch_lane_ = std::make_unique<Lane>(ctx_->device, least);
-    boot_lane_ = std::make_unique<Lane>(ctx_->device, greatest);
+    lanes_.push_back(std::make_unique<Lane>(ctx_->device, least));
+    for (uint32_t i = 0; i < cfg_.boot_lanes; ++i)
+      lanes_.push_back(std::make_unique<Lane>(ctx_->device, cfg_.boot_priority ? greatest : least));
   }
+  inflight_lane_.assign(std::max<size_t>(1, lanes_.size()), 0);
   t0_ = Clock::now();
   key_bytes_ = std::make_shared<std::atomic<int64_t>>(0);
   worker_ = std::thread([this] { worker(); });
@@ -436,14 +439,26 @@ void Server::worker() {
   } catch (...) {
   }
   std::unique_lock<std::mutex> lk(mu_);
-  // The lane of the earliest waiting request whose lane has room (-1: none). One lane: every
-  // request is on lane 0; two: bootstraps on lane 1, and the others may pass a waiting one.
-  auto lane_of = [&](const Req& r) { return boot_lane_ && r.kind == REQ_BOOTSTRAP ? 1 : 0; };
+  // The lane of the earliest waiting request whose lane has room (-1: none). Without lanes every
+  // request is on lane 0 in arrival order; with them bootstraps go to the least loaded bootstrap
+  // lane (1..), the others to lane 0, and either kind may pass a waiting request of the other.
+  const bool laned = !lanes_.empty();
+  auto boot_class = [&](const Req& r) { return laned && r.kind == REQ_BOOTSTRAP; };
+  auto boot_lane_free = [&]() -> int {
+    int best = -1;
+    for (int l = 1; l < (int)lanes_.size(); ++l)
+      if (inflight_lane_[l] < cfg_.max_inflight && (best < 0 || inflight_lane_[l] < inflight_lane_[best])) best = l;
+    return best;
+  };
   auto pick = [&]() -> int {
     for (const ReqPtr& r : pending_) {
-      const int l = lane_of(*r);
-      if (inflight_lane_[l] < cfg_.max_inflight) return l;
-      if (!boot_lane_) break;
+      if (boot_class(*r)) {
+        const int l = boot_lane_free();
+        if (l >= 0) return l;
+      } else if (inflight_lane_[0] < cfg_.max_inflight) {
+        return 0;
+      }
+      if (!laned) break;
     }
     return -1;
   };
@@ -460,7 +475,7 @@ void Server::worker() {
     bool wait_memory = false;
     for (auto pit = pending_.begin(); pit != pending_.end();) {
       ReqPtr r = *pit;
-      if (lane_of(*r) != lane) {  // the other lane's request keeps its place
+      if (boot_class(*r) != (lane >= 1)) {  // the other lanes' request keeps its place
         ++pit;
         continue;
       }
@@ -537,7 +552,7 @@ void Server::worker() {
     f->reqs = batch;
     f->work = work;
     f->lane = lane;
-    Lane* ln = boot_lane_ ? (lane == 1 ? boot_lane_.get() : batch_lane_.get()) : nullptr;
+    Lane* ln = laned ? lanes_[lane].get() : nullptr;
     std::optional<LaneScope> scope;  // this thread's launches through ctx_ go to the lane
     if (ln) scope.emplace(*ctx_, *ln);
     f->stream = ctx_->stream;

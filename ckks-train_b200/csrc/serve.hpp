@@ -40,9 +40,12 @@ struct ServerConfig {
   uint32_t max_batch_ks = 128;   // key switches admitted into one batch
   uint32_t max_inflight = 2;     // batches queued on the device at once (per lane)
   EvalConfig eval;
-  // Two compute lanes: bootstrap flights on one stream, every other flight on another, both
-  // beside the context's stream (which then carries only the client's own work).
-  bool boot_lane = false;
+  // Compute lanes (boot_lanes >= 1): bootstrap flights on `boot_lanes` streams of their own, every
+  // other flight on one more, all beside the context's stream (which then carries only the
+  // client's own work); the bootstrap lanes at the device's highest stream priority unless
+  // boot_priority is off. 0: every flight on the context's stream.
+  uint32_t boot_lanes = 0;
+  bool boot_priority = true;
 };
 
 struct ServerStats {
@@ -141,8 +144,8 @@ class Server {
   std::unordered_map<uint64_t, ReqPtr> reqs_;
   std::deque<ReqPtr> pending_;
   std::deque<Flight*> flights_;
-  uint32_t inflight_lane_[2] = {0, 0};           // flights queued per lane
-  std::unique_ptr<Lane> batch_lane_, boot_lane_;  // with cfg_.boot_lane
+  std::vector<std::unique_ptr<Lane>> lanes_;  // with boot_lanes: [0] the batch lane, then the bootstrap lanes
+  std::vector<uint32_t> inflight_lane_;       // flights queued per lane (one entry without lanes)
   std::list<HostKey*> lru_;  // front = most recently used
   size_t inflight_work_ = 0;
   uint64_t next_id_ = 1;

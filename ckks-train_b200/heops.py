@@ -953,6 +953,8 @@ SERVER_STATS = ("submitted", "completed", "failed", "cancelled", "batches", "mul
 
 
 SERVE_BOOT_LANE = 256  # CKG_SERVE_BOOT_LANE
+SERVE_BOOT_LANES_2 = 512  # CKG_SERVE_BOOT_LANES_2
+SERVE_LANES_EQUAL_PRIORITY = 1024  # CKG_SERVE_LANES_EQUAL_PRIORITY
 
 
 class Server:
@@ -960,9 +962,13 @@ class Server:
     owners, admitted by HBM budget with LRU key spill to pinned host memory and run with
     continuous batching. `ev` is any evaluator of the context; results are wrapped with it."""
 
-    def __init__(self, ctx, hbm_budget, max_batch_ks=128, max_inflight=2, config=None, ev=None, boot_lane=False):
+    def __init__(self, ctx, hbm_budget, max_batch_ks=128, max_inflight=2, config=None, ev=None, boot_lanes=0,
+                 boot_priority=True):
         self.ctx, self.ev = ctx, ev
-        flags = (config or EvalConfig()).flags | (SERVE_BOOT_LANE if boot_lane else 0)
+        if boot_lanes not in (0, 1, 2):
+            raise InvalidParams("boot_lanes must be 0, 1 or 2")
+        flags = (config or EvalConfig()).flags | {0: 0, 1: SERVE_BOOT_LANE, 2: SERVE_BOOT_LANES_2}[boot_lanes]
+        flags |= 0 if boot_priority else SERVE_LANES_EQUAL_PRIORITY
         h = VP()
         _check(lib().ckg_server_create(ctx.h, int(hbm_budget), max_batch_ks, max_inflight, flags, C.byref(h)))
         self.h = h

@@ -440,13 +440,14 @@ CKG_API int ckg_boot_create_encoded(ckg_eval* ev, const uint32_t* bp, double del
  * budget_waits, pending, hbm_budget. */
 typedef struct ckg_server ckg_server;
 enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVEC = 3, CKG_REQ_BOOTSTRAP = 4 };
-/* ckg_server_create flag beside the CKG_HOIST / CKG_BSGS / CKG_LAZY_RELIN bits: two compute
- * lanes, bootstrap flights on one stream (the device's highest stream priority) and all other
- * flights on another (each with its own memory pool and up to max_inflight flights), so
- * bootstraps overlap the other requests. Both
- * lanes start after the client's work queued on the context's stream when the flight is
- * built, and every output is handed back to the context's stream when its request completes. */
-enum { CKG_SERVE_BOOT_LANE = 256 };
+/* ckg_server_create flags beside the CKG_HOIST / CKG_BSGS / CKG_LAZY_RELIN bits: compute lanes.
+ * CKG_SERVE_BOOT_LANE runs bootstrap flights on a stream of their own and all other flights on
+ * another; CKG_SERVE_BOOT_LANES_2 gives bootstraps two streams (two bootstraps at once). Each
+ * lane has its own memory pool and up to max_inflight flights. The bootstrap lanes run at the
+ * device's highest stream priority unless CKG_SERVE_LANES_EQUAL_PRIORITY is set. Lanes start
+ * after the client's work queued on the context's stream when the flight is built, and every
+ * output is handed back to the context's stream when its request completes. */
+enum { CKG_SERVE_BOOT_LANE = 256, CKG_SERVE_BOOT_LANES_2 = 512, CKG_SERVE_LANES_EQUAL_PRIORITY = 1024 };
 CKG_API int ckg_server_create(ckg_ctx* ctx, uint64_t hbm_budget_bytes, uint32_t max_batch_ks, uint32_t max_inflight,
                               uint32_t flags, ckg_server** out);
 CKG_API void ckg_server_destroy(ckg_server* s);

@@ -254,12 +254,12 @@ def test_serve_cancel_and_drain(owners, ckg):
     srv.close()
 
 
-@pytest.mark.parametrize("boot_lane", [False, True])
-def test_serve_bootstrap_requests(ckg, oracle, boot_lane):
+@pytest.mark.parametrize("boot_lanes", [0, 1, 2])
+def test_serve_bootstrap_requests(ckg, oracle, boot_lanes):
     """Bootstrap requests from two owners (each with its own relinearization, rotation,
     conjugation and SSE keys) served beside rotations, on the reference's N = 2^10 bootstrap
-    chain, on one compute lane and on two (bootstraps on their own lane, overlapping the
-    rotations): every output equals the oracle's, each owner's OpCounter equals the CPU's, and
+    chain, on the context's stream and on compute lanes (one or two bootstrap lanes beside the
+    lane of the rotations, overlapping them): every output equals the oracle's, each owner's OpCounter equals the CPU's, and
     outputs handed back from a lane are then used by the context's own stream."""
     O = oracle
     q_bits = [54, 42, 42] + [34] * 4 + [58] * 7 + [56] * 4
@@ -268,7 +268,7 @@ def test_serve_bootstrap_requests(ckg, oracle, boot_lane):
     enc = O.Encoder(P)
     ctx = ckg.Context(10, P.q, P.p, 9, scale=delta)
     io = ckg.CudaEvaluator(ctx, None, [])
-    srv = ckg.Server(ctx, 2 << 30, max_batch_ks=32, max_inflight=2, ev=io, boot_lane=boot_lane)
+    srv = ckg.Server(ctx, 2 << 30, max_batch_ks=32, max_inflight=2, ev=io, boot_lanes=boot_lanes)
     srv.enable_bootstrap(ckg.BootParams(log_slots=9), delta)
     owners = []
     for o in range(2):
