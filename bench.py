@@ -62,7 +62,7 @@ SERVE_REQUESTS = 1000
 SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
 SERVE_BOOT_OWNERS = 8        # n16_boot serving with bootstrap requests
 SERVE_BOOT_BUDGET = 96 << 30
-SERVE_BOOT_LANES = 1          # bootstrap lanes of the bootstrap-serving runs (0: one stream)
+SERVE_BOOT_LANES = 2          # bootstrap lanes of the bootstrap-serving runs (0: one stream)
 SERVE_BOOT_SPILL_OWNERS = 32  # the same with key spill: up to 32 owners within host memory
 SERVE_BOOT_SPILL_BUDGET = 48 << 30
 SERVE_BOOT_SPILL_REQUESTS = 400
@@ -1323,17 +1323,24 @@ def main():
     value = mix.ks * args.steps * world / (ms * 1e-3)
     e2e = None
     if not args.no_e2e:
+        mix.batch = None  # the timed graph's batch is done with: its scratch goes back to the pool
+        gc.collect()
+        torch.cuda.empty_cache()
         mix.prepare_e2e()
         steps_e = max(8, args.steps)
         mix.step_e2e()
         mix.inflight.clear()
         mix.host_s, mix.host_parts = 0.0, {}
+        ts0 = S.ctx.transfer_stats()
         ms_e, (h2d, d2h) = timed(torch, S.ctx, mix.step_e2e, steps_e, 0, dist, tail=S.ctx.join_transfers)
+        ts1 = S.ctx.transfer_stats()
         e2e = {"value": round(mix.ks * steps_e * world / (ms_e * 1e-3), 2), "unit": unit,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": round(ms_e / steps_e, 3), "steps": steps_e,
                "host_ms_per_step": round(mix.host_s * 1e3 / steps_e, 2),
-               "host_ms_per_step_by_phase": {k: round(v * 1e3 / steps_e, 2) for k, v in mix.host_parts.items()}}
+               "host_ms_per_step_by_phase": {k: round(v * 1e3 / steps_e, 2) for k, v in mix.host_parts.items()},
+               "transfer_stats_per_step": {k: (ts1[k] if k == "upload_pool_bytes" else round((ts1[k] - ts0[k]) / steps_e, 1))
+                                           for k in ts1}}
         if rank == 0:  # no collective inside: the other ranks skip it
             e2e["host_link"] = pcie_ceiling(torch, h2d, d2h, ms_e / steps_e)
     plain = None

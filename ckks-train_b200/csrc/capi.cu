@@ -99,6 +99,21 @@ int ckg_device_fault(ckg_ctx* ctx, int32_t* code) {
   CKG_API_END
 }
 
+int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n) {
+  CKG_API_BEGIN
+  if (!out && n) throw Error(CKG_INVALID_PARAMS, "null output");
+  Context& c = ctx_of(ctx);
+  uint64_t reserved = 0;
+  if (c.xpool) {
+    unsigned long long v = 0;
+    if (cudaMemPoolGetAttribute(c.xpool, cudaMemPoolAttrReservedMemCurrent, &v) == cudaSuccess) reserved = v;
+  }
+  const uint64_t w[8] = {c.st_upload_calls, c.st_upload_bytes, c.st_upload_alloc_ns, c.st_upload_copy_ns, reserved,
+                         c.st_download_calls, c.st_download_ns, c.st_alloc_retries};
+  for (uint32_t i = 0; i < n && i < 8; ++i) out[i] = w[i];
+  CKG_API_END
+}
+
 int ckg_ctx_join_transfers(ckg_ctx* ctx) {
   CKG_API_BEGIN
   ctx_of(ctx).join_transfers();

@@ -1,6 +1,7 @@
 // Device context set-up (prime constants, twiddle and conversion tables) and the
 // polynomial-level algorithms of the evaluator path. See engine.hpp for the layouts.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -128,12 +129,19 @@ DevBufPtr Context::upload_overlapped_list(const std::vector<HostPart>& parts, st
   }
   b->words = total;
   if (!total) return b;
+  const auto t0 = std::chrono::steady_clock::now();
   CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, total * 8, xpool, xfer_in->s));
+  const auto t1 = std::chrono::steady_clock::now();
   for (size_t i = 0; i < parts.size(); ++i)
     if (parts[i].words)
       CKG_CUDA(cudaMemcpyAsync(b->p + offsets[i], parts[i].host, parts[i].words * 8, cudaMemcpyHostToDevice,
                                xfer_in->s));
   stream_after(stream, xfer_in->s);
+  const auto t2 = std::chrono::steady_clock::now();
+  st_upload_calls++;
+  st_upload_bytes += total * 8;
+  st_upload_alloc_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count();
+  st_upload_copy_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(t2 - t1).count();
   return b;
 }
 
@@ -168,6 +176,7 @@ void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
   activate();
   transfer_streams();
   if (parts.empty()) return;
+  const auto t0 = std::chrono::steady_clock::now();
   stream_after(xfer_out->s, stream);
   for (const DevPart& d : parts) {
     if (d.pitch_words == d.row_words)
@@ -197,6 +206,8 @@ void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
     CKG_CUDA(cudaEventRecord(e, xfer_out->s));
     w.push_back(e);
   }
+  st_download_calls++;
+  st_download_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
 }
 
 void Context::upload_staged(void* dst, const void* src, size_t bytes) {
@@ -267,12 +278,17 @@ DevBufPtr Context::alloc(size_t words) {
     cudaError_t e = get();
     if (e == cudaErrorMemoryAllocation) {
       // Free memory may sit cached in another pool (each keeps what it frees): hand the unused
-      // blocks of the device's default pool and of the upload pool back, then try once more.
+      // blocks of the device's default pool back and try again, then those of the upload pool.
       cudaGetLastError();
+      st_alloc_retries++;
       cudaMemPool_t def;
       if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
-      if (xpool) cudaMemPoolTrimTo(xpool, 0);
       e = get();
+      if (e == cudaErrorMemoryAllocation && xpool) {
+        cudaGetLastError();
+        cudaMemPoolTrimTo(xpool, 0);
+        e = get();
+      }
     }
     if (e != cudaSuccess) throw_cuda(e, "device allocation");
   }

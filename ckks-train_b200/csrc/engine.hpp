@@ -9,6 +9,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <deque>
 #include <map>
@@ -200,6 +201,10 @@ struct Context {
   // wait for the work already queued on the stream. A slot is reused once its copy completed.
   // Not allowed while the stream is being captured (the graph would read a reused slot).
   void upload_staged(void* dst, const void* src, size_t bytes);
+
+  // Host-side accounting of the overlapped transfers and allocation retries (ckg_ctx_transfer_stats).
+  std::atomic<uint64_t> st_upload_calls{0}, st_upload_bytes{0}, st_upload_alloc_ns{0}, st_upload_copy_ns{0},
+      st_download_calls{0}, st_download_ns{0}, st_alloc_retries{0};
   std::mutex stage_mu;
   unsigned char* stage = nullptr;
   size_t stage_cap = 0, stage_head = 0;

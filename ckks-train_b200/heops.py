@@ -199,6 +199,7 @@ def _declare(L):
     L.ckg_ct_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_pt_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_ct_download_overlap.argtypes = [VP, VP]
+    L.ckg_ctx_transfer_stats.argtypes = [VP, C.POINTER(C.c_uint64), C.c_uint32]
     L.ckg_ct_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.POINTER(VP)]
     L.ckg_pt_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
@@ -317,6 +318,15 @@ class Context:
 
     def sync(self):
         _check(lib().ckg_ctx_sync(self.h))
+
+    TRANSFER_STATS = ("upload_calls", "upload_bytes", "upload_alloc_ns", "upload_copy_ns", "upload_pool_bytes",
+                      "download_calls", "download_ns", "alloc_retries")
+
+    def transfer_stats(self):
+        """Host-side accounting of the overlapped transfers (include/ckg.h, ckg_ctx_transfer_stats)."""
+        out = (C.c_uint64 * 8)()
+        _check(lib().ckg_ctx_transfer_stats(self.h, out, 8))
+        return dict(zip(self.TRANSFER_STATS, [int(x) for x in out]))
 
     def join_transfers(self):
         """The context's stream waits for every overlapped transfer queued so far."""
