@@ -245,11 +245,43 @@ class Mix:
         self.batch.launch_graph()
 
     def prepare_e2e(self):
-        torch = self.S.torch
-        self.out_host = []
-        for (kind, level, steps) in self.ops:
-            lv = level if kind == "rot" else level - 1
-            self.out_host.append(torch.empty((2, lv + 1, self.S.n), dtype=torch.int64, pin_memory=True))
+        """Host buffers of the e2e step: inputs and results each in one pinned allocation, laid out
+        in list order (a client's request and reply buffers), so the list transfers move each run
+        of adjacent buffers with one copy."""
+        torch, n = self.S.torch, self.S.n
+
+        def packed(tensors):
+            flat = torch.empty(sum(t.numel() for t in tensors), dtype=torch.int64, pin_memory=True)
+            views, off = [], 0
+            for t in tensors:
+                v = flat[off:off + t.numel()].view(t.shape)
+                v.copy_(t)
+                views.append(v)
+                off += t.numel()
+            return flat, views
+
+        cts = [ha for ha, hb in self.host]
+        cts_order = []
+        for (kind, _, _), (ha, hb) in zip(self.ops, self.host):
+            cts_order.append(ha)
+            if kind == "mul":
+                cts_order.append(hb)
+        pts = [hb for (kind, _, _), (ha, hb) in zip(self.ops, self.host) if kind == "pmul"]
+        self.host_ct_flat, ct_views = packed(cts_order)
+        self.host_pt_flat, pt_views = packed(pts) if pts else (None, [])
+        ct_it, pt_it, host = iter(ct_views), iter(pt_views), []
+        for kind, _, _ in self.ops:
+            a = next(ct_it)
+            host.append((a, next(ct_it) if kind == "mul" else (next(pt_it) if kind == "pmul" else None)))
+        self.host = host
+        del cts, cts_order, pts
+        shapes = [(2, (level if kind == "rot" else level - 1) + 1, n) for kind, level, _ in self.ops]
+        self.out_flat = torch.empty(sum(int(np.prod(sh)) for sh in shapes), dtype=torch.int64, pin_memory=True)
+        self.out_host, off = [], 0
+        for sh in shapes:
+            m = int(np.prod(sh))
+            self.out_host.append(self.out_flat[off:off + m].view(sh))
+            off += m
         self.out_ptrs = [t.data_ptr() for t in self.out_host]
         self.inflight, self.host_s, self.host_parts = [], 0.0, {}
         self.stream = torch.cuda.ExternalStream(self.S.ctx.stream)

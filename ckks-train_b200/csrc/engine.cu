@@ -33,8 +33,65 @@ DevBuf::~DevBuf() {
     cudaStreamWaitEvent(sres->s, e, 0);
     cudaEventDestroy(e);
   }
-  if (pooled) cudaFreeAsync(p, sres->s);
-  else cudaFree(p);
+  cudaEvent_t done = nullptr;
+  if (cache && cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess &&
+      cudaEventRecord(done, sres->s) == cudaSuccess) {
+    cache->give(p, words, done);
+  } else {
+    if (done) cudaEventDestroy(done);
+    if (pooled) cudaFreeAsync(p, sres->s);
+    else cudaFree(p);
+  }
+  if (cur != device) cudaSetDevice(cur);
+}
+
+uint64_t* XferCache::take(size_t words) {
+  std::lock_guard<std::mutex> lk(mu);
+  int best = -1;
+  for (int i = 0; i < (int)blocks.size(); ++i) {
+    const Block& b = blocks[i];
+    if (b.words < words || b.words > words + words / 4) continue;
+    if (best >= 0 && b.words >= blocks[best].words) continue;
+    if (cudaEventQuery(b.done) != cudaSuccess) continue;
+    best = i;
+  }
+  if (best < 0) return nullptr;
+  uint64_t* p = blocks[best].p;
+  cudaEventDestroy(blocks[best].done);
+  blocks.erase(blocks.begin() + best);
+  return p;
+}
+
+void XferCache::give(uint64_t* p, size_t words, cudaEvent_t done) {
+  std::lock_guard<std::mutex> lk(mu);
+  blocks.push_back({p, words, done});
+}
+
+void XferCache::trim() {
+  std::lock_guard<std::mutex> lk(mu);
+  for (size_t i = 0; i < blocks.size();) {
+    if (cudaEventQuery(blocks[i].done) == cudaSuccess) {
+      cudaEventDestroy(blocks[i].done);
+      cudaFreeAsync(blocks[i].p, stream->s);
+      blocks[i] = blocks.back();
+      blocks.pop_back();
+    } else {
+      ++i;
+    }
+  }
+  if (pool) cudaMemPoolTrimTo(pool, 0);
+}
+
+XferCache::~XferCache() {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  for (Block& b : blocks) {
+    cudaEventSynchronize(b.done);
+    cudaEventDestroy(b.done);
+    cudaFreeAsync(b.p, stream->s);
+  }
+  if (stream) cudaStreamSynchronize(stream->s);
   if (cur != device) cudaSetDevice(cur);
 }
 
@@ -87,6 +144,29 @@ void Context::transfer_streams() {
     CKG_CUDA(cudaMemPoolSetAttribute(xpool, cudaMemPoolAttrReleaseThreshold, &thr));
     CKG_CUDA(cudaMemPoolSetAttribute(xpool, cudaMemPoolReuseAllowInternalDependencies, &no));
   }
+  if (!xcache) {
+    xcache = std::make_shared<XferCache>();
+    xcache->device = device;
+    xcache->pool = xpool;
+    xcache->stream = xfer_in;
+  }
+}
+
+uint64_t* Context::xfer_block(size_t words, cudaStream_t on) {
+  transfer_streams();
+  if (uint64_t* p = xcache->take(words)) return p;  // its last use has completed: any stream may take it
+  uint64_t* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
+  if (e == cudaErrorMemoryAllocation) {  // cached blocks still in flight elsewhere: return the rest
+    cudaGetLastError();
+    st_alloc_retries++;
+    xcache->trim();
+    cudaMemPool_t def;
+    if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+    e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
+  }
+  if (e != cudaSuccess) throw_cuda(e, "transfer block allocation");
+  return p;
 }
 
 namespace {
@@ -109,7 +189,8 @@ DevBufPtr Context::upload_overlapped(const uint64_t* host, size_t words) {
   b->device = device;
   b->words = words;
   if (!words) return b;
-  CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, words * 8, xpool, xfer_in->s));
+  b->p = xfer_block(words, xfer_in->s);
+  b->cache = xcache;
   CKG_CUDA(cudaMemcpyAsync(b->p, host, words * 8, cudaMemcpyHostToDevice, xfer_in->s));
   stream_after(stream, xfer_in->s);
   return b;
@@ -130,12 +211,20 @@ DevBufPtr Context::upload_overlapped_list(const std::vector<HostPart>& parts, st
   b->words = total;
   if (!total) return b;
   const auto t0 = std::chrono::steady_clock::now();
-  CKG_CUDA(cudaMallocFromPoolAsync((void**)&b->p, total * 8, xpool, xfer_in->s));
+  b->p = xfer_block(total, xfer_in->s);
+  b->cache = xcache;
   const auto t1 = std::chrono::steady_clock::now();
-  for (size_t i = 0; i < parts.size(); ++i)
-    if (parts[i].words)
-      CKG_CUDA(cudaMemcpyAsync(b->p + offsets[i], parts[i].host, parts[i].words * 8, cudaMemcpyHostToDevice,
-                               xfer_in->s));
+  // one copy per run of parts that are adjacent both in host memory and in the block
+  for (size_t i = 0; i < parts.size();) {
+    size_t j = i + 1, words = parts[i].words;
+    while (j < parts.size() && parts[j].host == parts[i].host + words && offsets[j] == offsets[i] + words) {
+      words += parts[j].words;
+      ++j;
+    }
+    if (words)
+      CKG_CUDA(cudaMemcpyAsync(b->p + offsets[i], parts[i].host, words * 8, cudaMemcpyHostToDevice, xfer_in->s));
+    i = j;
+  }
   stream_after(stream, xfer_in->s);
   const auto t2 = std::chrono::steady_clock::now();
   st_upload_calls++;
@@ -177,79 +266,61 @@ void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
   transfer_streams();
   if (parts.empty()) return;
   const auto t0 = std::chrono::steady_clock::now();
-  stream_after(xfer_out->s, stream);
-  for (const DevPart& d : parts) {
-    if (d.pitch_words == d.row_words)
-      CKG_CUDA(cudaMemcpyAsync(d.host, d.dev, d.rows * d.row_words * 8, cudaMemcpyDeviceToHost, xfer_out->s));
-    else
-      CKG_CUDA(cudaMemcpy2DAsync(d.host, d.row_words * 8, d.dev, d.pitch_words * 8, d.row_words * 8, d.rows,
-                                 cudaMemcpyDeviceToHost, xfer_out->s));
+  const cudaStream_t st = stream;
+  // One kernel packs every part into one staging block on the compute stream; the download
+  // stream then copies each run of adjacent host destinations with one transfer (the copies
+  // read only the staging block, so the parts' buffers are free once the pack has run).
+  std::vector<PackSeg> segs(parts.size());
+  size_t total = 0;
+  for (size_t i = 0; i < parts.size(); ++i) {
+    const DevPart& d = parts[i];
+    const size_t w = d.rows * d.row_words;
+    if (w >= ((size_t)1 << 32) || d.row_words >= ((size_t)1 << 32))
+      throw Error(ST_INVALID_PARAMS, "a download part above 2^32 words");
+    segs[i] = PackSeg{d.dev, nullptr, d.pitch_words, (uint32_t)d.rows, (uint32_t)d.row_words};
+    total += w;
   }
-  // every buffer's free waits for the copies (one event per distinct buffer)
+  if (!total) return;
+  uint64_t* stage = xfer_block(total, st);
+  size_t off = 0;
+  for (PackSeg& sg : segs) {
+    sg.dst = stage + off;
+    off += (size_t)sg.rows * sg.row_words;
+  }
+  DevBufPtr desc = alloc((segs.size() * sizeof(PackSeg) + 7) / 8);
+  upload_staged(desc->p, segs.data(), segs.size() * sizeof(PackSeg));
+  launch_pack(reinterpret_cast<const PackSeg*>(desc->p), (int)segs.size(), st);
+  CKG_CUDA(cudaGetLastError());
+  // a part whose buffer is freed on another stream: that free waits for the pack
   std::vector<DevBuf*> seen;
   for (const DevPart& d : parts) {
     DevBuf* b = d.buf->get();
-    if (std::find(seen.begin(), seen.end(), b) != seen.end()) continue;
+    if (b->sres->s == st || std::find(seen.begin(), seen.end(), b) != seen.end()) continue;
     seen.push_back(b);
-    auto& w = b->waits;
-    for (size_t i = 0; i < w.size();) {
-      if (cudaEventQuery(w[i]) == cudaSuccess) {
-        cudaEventDestroy(w[i]);
-        w[i] = w.back();
-        w.pop_back();
-      } else {
-        ++i;
-      }
-    }
     cudaEvent_t e;
     CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    CKG_CUDA(cudaEventRecord(e, xfer_out->s));
-    w.push_back(e);
+    CKG_CUDA(cudaEventRecord(e, st));
+    b->waits.push_back(e);
   }
+  stream_after(xfer_out->s, st);
+  off = 0;
+  for (size_t i = 0; i < parts.size();) {
+    size_t j = i + 1, bytes = (size_t)segs[i].rows * segs[i].row_words * 8;
+    while (j < parts.size() &&
+           (const unsigned char*)parts[j].host == (const unsigned char*)parts[i].host + bytes) {
+      bytes += (size_t)segs[j].rows * segs[j].row_words * 8;
+      ++j;
+    }
+    CKG_CUDA(cudaMemcpyAsync(parts[i].host, stage + off, bytes, cudaMemcpyDeviceToHost, xfer_out->s));
+    off += bytes / 8;
+    i = j;
+  }
+  cudaEvent_t copied;
+  CKG_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
+  CKG_CUDA(cudaEventRecord(copied, xfer_out->s));
+  xcache->give(stage, total, copied);  // reused once the copies are done
   st_download_calls++;
   st_download_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
-}
-
-void Context::upload_staged(void* dst, const void* src, size_t bytes) {
-  if (!bytes) return;
-  activate();
-  cudaStream_t st = stream;
-  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  CKG_CUDA(cudaStreamIsCapturing(st, &cap));
-  if (cap != cudaStreamCaptureStatusNone)
-    throw Error(ST_INVALID_PARAMS, "a batch is built before stream capture (use the batch's own graph capture)");
-  std::lock_guard<std::mutex> lk(stage_mu);
-  const size_t need = (bytes + 255) & ~(size_t)255;
-  if (need > stage_cap) {  // grow: every copy out of the old ring completes first
-    for (auto& u : stage_used) {
-      cudaEventSynchronize(u.done);
-      cudaEventDestroy(u.done);
-    }
-    stage_used.clear();
-    if (stage) cudaFreeHost(stage);
-    stage = nullptr;
-    stage_cap = std::max(need * 4, (size_t)32 << 20);
-    CKG_CUDA(cudaMallocHost((void**)&stage, stage_cap));
-    stage_head = 0;
-  }
-  if (stage_head + need > stage_cap) stage_head = 0;
-  for (auto it = stage_used.begin(); it != stage_used.end();) {
-    const bool overlap = it->off < stage_head + need && stage_head < it->off + it->len;
-    if (overlap) CKG_CUDA(cudaEventSynchronize(it->done));
-    if (overlap || cudaEventQuery(it->done) == cudaSuccess) {
-      cudaEventDestroy(it->done);
-      it = stage_used.erase(it);
-    } else {
-      ++it;
-    }
-  }
-  std::memcpy(stage + stage_head, src, bytes);
-  CKG_CUDA(cudaMemcpyAsync(dst, stage + stage_head, bytes, cudaMemcpyHostToDevice, st));
-  cudaEvent_t e;
-  CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  CKG_CUDA(cudaEventRecord(e, st));
-  stage_used.push_back({stage_head, need, e});
-  stage_head += need;
 }
 
 void Context::join_transfers() {
@@ -284,9 +355,9 @@ DevBufPtr Context::alloc(size_t words) {
       cudaMemPool_t def;
       if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
       e = get();
-      if (e == cudaErrorMemoryAllocation && xpool) {
+      if (e == cudaErrorMemoryAllocation && xcache) {
         cudaGetLastError();
-        cudaMemPoolTrimTo(xpool, 0);
+        xcache->trim();
         e = get();
       }
     }

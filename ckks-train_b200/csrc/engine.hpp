@@ -60,6 +60,27 @@ struct StreamRes {
 };
 typedef std::shared_ptr<StreamRes> StreamPtr;
 
+// Device blocks of the overlapped transfers, kept for reuse: a block comes back with an event
+// that completes when its last reader is done, and is handed out again only after that event
+// (so the next step's uploads never depend on how a memory pool tracks cross-stream frees).
+struct XferCache {
+  struct Block {
+    uint64_t* p;
+    size_t words;
+    cudaEvent_t done;
+  };
+  std::mutex mu;
+  std::vector<Block> blocks;
+  int device = 0;
+  cudaMemPool_t pool = nullptr;  // where new blocks come from and trimmed ones go back
+  StreamPtr stream;               // the upload stream (allocations and trims)
+  uint64_t* take(size_t words);  // a completed block of words..5/4 words, or null
+  void give(uint64_t* p, size_t words, cudaEvent_t done);  // takes ownership of `done`
+  void trim();  // completed blocks back to the pool
+  ~XferCache();
+};
+typedef std::shared_ptr<XferCache> XferCachePtr;
+
 // A stream-ordered device allocation of `words` u64.
 struct DevBuf {
   uint64_t* p = nullptr;
@@ -70,6 +91,7 @@ struct DevBuf {
   std::vector<cudaEvent_t> waits;
   int device = 0;
   bool pooled = true;
+  XferCachePtr cache;  // set: the block returns to this cache instead of being freed
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -175,6 +197,8 @@ struct Context {
   // has completed (no stream wait inserted): the next uploads never wait for queued compute.
   StreamPtr xfer_in, xfer_out;
   cudaMemPool_t xpool = nullptr;
+  XferCachePtr xcache;
+  uint64_t* xfer_block(size_t words, cudaStream_t on);  // from the cache, else a new block of the upload pool
   void transfer_streams();
   DevBufPtr upload_overlapped(const uint64_t* host, size_t words);
   // Several host buffers into one allocation (one copy each, one stream dependency):

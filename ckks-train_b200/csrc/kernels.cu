@@ -10,6 +10,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <stdexcept>
 #include <vector>
@@ -1257,6 +1258,27 @@ __global__ void __launch_bounds__(256)
   r.dst[c] = v;
 }
 
+// Packed download: each blockIdx.y copies one segment (rows at a source pitch) into its
+// contiguous destination, 16 bytes per access when every address and length is even.
+__global__ void __launch_bounds__(256) k_pack(const PackSeg* __restrict__ segs) {
+  const PackSeg sg = segs[blockIdx.y];
+  const uint32_t total = sg.rows * sg.row_words;
+  const uint32_t step = gridDim.x * blockDim.x;
+  const bool vec = ((((uintptr_t)sg.src | (uintptr_t)sg.dst) & 15) == 0) && !(sg.pitch & 1) && !(sg.row_words & 1);
+  if (vec) {
+    for (uint32_t w = 2 * (blockIdx.x * blockDim.x + threadIdx.x); w < total; w += 2 * step) {
+      const uint32_t r = w / sg.row_words, c = w - r * sg.row_words;
+      const ulonglong2 v = __ldcs(reinterpret_cast<const ulonglong2*>(sg.src + r * sg.pitch + c));
+      __stcs(reinterpret_cast<ulonglong2*>(sg.dst + w), v);
+    }
+  } else {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += step) {
+      const uint32_t r = w / sg.row_words, c = w - r * sg.row_words;
+      sg.dst[w] = __ldcs(sg.src + r * sg.pitch + c);
+    }
+  }
+}
+
 template <class B>
 __global__ void __launch_bounds__(256) k_gather(const __grid_constant__ B gb, int n) {
   const GatherRef& r = gb.r[blockIdx.y];
@@ -1671,6 +1693,14 @@ void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, co
     b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
     for (int i = 0; i < b.count; ++i) b.r[i] = refs[off + i];
     k_unary<<<dim3((n + 255) / 256, b.count), 256, 0, st>>>(b, d.prime, n, op, consts, perm);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+}
+
+void launch_pack(const PackSeg* dev_segs, int count, cudaStream_t st) {
+  for (int i = 0; i < count; i += 65535) {
+    const int m = std::min(65535, count - i);
+    k_pack<<<dim3(64, m), 256, 0, st>>>(dev_segs + i);
     g_launches.fetch_add(1, std::memory_order_relaxed);
   }
 }

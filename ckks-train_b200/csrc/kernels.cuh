@@ -241,4 +241,14 @@ struct GatherPtrs {
   const GatherRef* r;
 };
 
+// One segment of a packed download: `rows` rows of `row_words` words at `pitch` words apart in
+// the source, written contiguously at dst (rows * row_words < 2^32).
+struct PackSeg {
+  const uint64_t* src;
+  uint64_t* dst;
+  uint64_t pitch;
+  uint32_t rows;
+  uint32_t row_words;
+};
+
 }  // namespace ckg

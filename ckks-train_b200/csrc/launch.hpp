@@ -71,6 +71,8 @@ void launch_finish_ptr(const DevTables& d, const FinRef* dev_refs, int count, cu
 void launch_binary_ptr(const DevTables& d, const BinRef* dev_refs, int count, int op, cudaStream_t st);
 void launch_tensor_ptr(const DevTables& d, const TensorRef* dev_refs, int count, cudaStream_t st);
 void launch_gather_ptr(const DevTables& d, const GatherRef* dev_refs, int count, cudaStream_t st);
+// Copies `count` segments (a device array) into their contiguous destinations.
+void launch_pack(const PackSeg* dev_segs, int count, cudaStream_t st);
 // mode 0: multiply by the per-prime Shoup constant; mode 1: add the per-prime constant.
 void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st,
                    int mode = 0);

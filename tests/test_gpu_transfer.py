@@ -98,6 +98,19 @@ def test_overlapped_lists_match_oracle(env):
     for i, (a, p) in enumerate(zip(ins, pts)):
         w = cpu.rescale(cpu.mul_plain(cpu.ct(a, env.scale), p, env.scale))
         assert_same(outs_host[i].numpy().view(np.uint64), w.data(), f"list entry {i}")
+    # adjacent host buffers (one pinned allocation, list order): one copy per run, same words
+    torch = torch_dev()
+    flat_in = torch.from_numpy(np.concatenate([np.ascontiguousarray(a, np.uint64).ravel() for a in ins])
+                               .view(np.int64)).pin_memory()
+    offs = np.cumsum([0] + [a.size for a in ins])
+    g = gpu.upload_ct_overlap_list([(flat_in.data_ptr() + 8 * int(offs[i]), 2, lv, env.scale)
+                                    for i, lv in enumerate(levels)])
+    flat_out = _empty_pinned((int(offs[-1]),))
+    gpu.download_ct_overlap_list(g, [flat_out.data_ptr() + 8 * int(offs[i]) for i in range(len(levels))])
+    del g
+    env.ctx.join_transfers()
+    env.ctx.sync()
+    assert np.array_equal(flat_out.numpy(), flat_in.numpy()), "contiguous list round trip"
     with pytest.raises(ckg.InvalidParams):  # a bad entry late in the list: nothing is made
         gpu.upload_ct_overlap_list([(host_in[0].data_ptr(), 2, L, env.scale), (0, 2, L, env.scale)])
     with pytest.raises(ckg.InvalidParams):
