@@ -323,6 +323,48 @@ void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
   st_download_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
 }
 
+void Context::upload_staged(void* dst, const void* src, size_t bytes) {
+  if (!bytes) return;
+  activate();
+  cudaStream_t st = stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CKG_CUDA(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone)
+    throw Error(ST_INVALID_PARAMS, "a batch is built before stream capture (use the batch's own graph capture)");
+  std::lock_guard<std::mutex> lk(stage_mu);
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  if (need > stage_cap) {  // grow: every copy out of the old ring completes first
+    for (auto& u : stage_used) {
+      cudaEventSynchronize(u.done);
+      cudaEventDestroy(u.done);
+    }
+    stage_used.clear();
+    if (stage) cudaFreeHost(stage);
+    stage = nullptr;
+    stage_cap = std::max(need * 4, (size_t)32 << 20);
+    CKG_CUDA(cudaMallocHost((void**)&stage, stage_cap));
+    stage_head = 0;
+  }
+  if (stage_head + need > stage_cap) stage_head = 0;
+  for (auto it = stage_used.begin(); it != stage_used.end();) {
+    const bool overlap = it->off < stage_head + need && stage_head < it->off + it->len;
+    if (overlap) CKG_CUDA(cudaEventSynchronize(it->done));
+    if (overlap || cudaEventQuery(it->done) == cudaSuccess) {
+      cudaEventDestroy(it->done);
+      it = stage_used.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  std::memcpy(stage + stage_head, src, bytes);
+  CKG_CUDA(cudaMemcpyAsync(dst, stage + stage_head, bytes, cudaMemcpyHostToDevice, st));
+  cudaEvent_t e;
+  CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CKG_CUDA(cudaEventRecord(e, st));
+  stage_used.push_back({stage_head, need, e});
+  stage_head += need;
+}
+
 void Context::join_transfers() {
   activate();
   if (xfer_in) stream_after(stream, xfer_in->s);
