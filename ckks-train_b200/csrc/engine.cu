@@ -65,6 +65,16 @@ uint64_t* XferCache::take(size_t words) {
 void XferCache::give(uint64_t* p, size_t words, cudaEvent_t done) {
   std::lock_guard<std::mutex> lk(mu);
   blocks.push_back({p, words, done});
+  // at most kMaxBlocks kept: the oldest completed ones beyond that go back to the pool
+  for (size_t i = 0; blocks.size() > kMaxBlocks && i < blocks.size();) {
+    if (cudaEventQuery(blocks[i].done) == cudaSuccess) {
+      cudaEventDestroy(blocks[i].done);
+      cudaFreeAsync(blocks[i].p, stream->s);
+      blocks.erase(blocks.begin() + i);
+    } else {
+      ++i;
+    }
+  }
 }
 
 void XferCache::trim() {

@@ -69,8 +69,9 @@ struct XferCache {
     size_t words;
     cudaEvent_t done;
   };
+  static constexpr size_t kMaxBlocks = 16;
   std::mutex mu;
-  std::vector<Block> blocks;
+  std::vector<Block> blocks;  // oldest first
   int device = 0;
   cudaMemPool_t pool = nullptr;  // where new blocks come from and trimmed ones go back
   StreamPtr stream;               // the upload stream (allocations and trims)
