@@ -28,6 +28,7 @@ from .heops import (  # noqa: F401
     NoLevelsLeft,
     OutOfMemory,
     Plaintext,
+    PinnedBuffer,
     SERVER_STATS,
     ScaleMismatch,
     Server,

@@ -114,6 +114,19 @@ int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n) {
   CKG_API_END
 }
 
+int ckg_host_alloc(uint64_t bytes, void** out) {
+  CKG_API_BEGIN
+  if (!out) throw Error(CKG_INVALID_PARAMS, "null output");
+  *out = nullptr;
+  if (!bytes) throw Error(CKG_INVALID_PARAMS, "zero bytes");
+  CKG_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+  CKG_API_END
+}
+
+void ckg_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
 int ckg_ctx_join_transfers(ckg_ctx* ctx) {
   CKG_API_BEGIN
   ctx_of(ctx).join_transfers();

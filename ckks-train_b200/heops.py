@@ -200,6 +200,9 @@ def _declare(L):
     L.ckg_pt_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_ct_download_overlap.argtypes = [VP, VP]
     L.ckg_ctx_transfer_stats.argtypes = [VP, C.POINTER(C.c_uint64), C.c_uint32]
+    L.ckg_host_alloc.argtypes = [C.c_uint64, C.POINTER(VP)]
+    L.ckg_host_free.argtypes = [VP]
+    L.ckg_host_free.restype = None
     L.ckg_ct_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_double), C.POINTER(VP)]
     L.ckg_pt_upload_overlap_list.argtypes = [VP, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_uint32),
@@ -960,6 +963,33 @@ class Batch:
 SERVER_STATS = ("submitted", "completed", "failed", "cancelled", "batches", "multi_owner_batches",
                 "max_batch_requests", "key_hits", "key_misses", "key_evictions", "key_upload_bytes", "key_bytes",
                 "peak_key_bytes", "peak_device_bytes", "budget_waits", "pending", "hbm_budget")
+
+
+class PinnedBuffer:
+    """Pinned host memory from the library's CUDA runtime (ckg_host_alloc), for the overlapped
+    transfers; `array(dtype, shape)` views it as a numpy array. Freed when the object goes."""
+
+    def __init__(self, nbytes):
+        h = VP()
+        _check(lib().ckg_host_alloc(int(nbytes), C.byref(h)))
+        self.ptr, self.nbytes = h.value, int(nbytes)
+
+    def array(self, dtype=np.int64, shape=None, offset=0):
+        dt = np.dtype(dtype)
+        count = (self.nbytes - offset) // dt.itemsize if shape is None else int(np.prod(shape))
+        if offset + count * dt.itemsize > self.nbytes:
+            raise InvalidParams("view beyond the buffer")
+        buf = (C.c_char * (count * dt.itemsize)).from_address(self.ptr + offset)
+        a = np.frombuffer(buf, dtype=dt, count=count)
+        return a if shape is None else a.reshape(shape)
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None):
+                lib().ckg_host_free(VP(self.ptr))
+                self.ptr = None
+        except Exception:
+            pass
 
 
 SERVE_BOOT_LANE = 256  # CKG_SERVE_BOOT_LANE

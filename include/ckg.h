@@ -199,6 +199,10 @@ CKG_API int ckg_ctx_join_transfers(ckg_ctx* ctx);
  * bytes the upload pool holds now, download calls, host ns queueing downloads, and device
  * allocations retried after handing cached pool memory back. */
 CKG_API int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n);
+/* Pinned host memory for the overlapped transfers, allocated by the library's own CUDA runtime
+ * (portable: pinned for every context). Free it only when no queued copy still uses it. */
+CKG_API int ckg_host_alloc(uint64_t bytes, void** out);
+CKG_API void ckg_host_free(void* p);
 /* Lists of the same in one call each: the uploads share one device allocation and one
  * stream dependency (every entry is checked before anything is queued; on an error no handle
  * is made); the downloads share one stream dependency and must come from one context. */

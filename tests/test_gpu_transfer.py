@@ -116,3 +116,24 @@ def test_overlapped_lists_match_oracle(env):
     with pytest.raises(ckg.InvalidParams):
         gpu.upload_pt_overlap_list([(host_pt[0].data_ptr(), L + 1, env.scale)])
     assert gpu.upload_ct_overlap_list([]) == []
+
+
+def test_pinned_buffer_round_trip(env):
+    """Host buffers from the library's own pinned allocation (ckg_host_alloc) carry a list
+    round trip like any pinned memory."""
+    ckg, P, gpu = env.ckg, env.P, env.gpu
+    L = P.max_level
+    ins = [random_ct(P, 70 + i, L) for i in range(3)]
+    words = ins[0].size
+    buf_in, buf_out = ckg.PinnedBuffer(8 * words * 3), ckg.PinnedBuffer(8 * words * 3)
+    a_in = buf_in.array(np.uint64, (3,) + ins[0].shape)
+    for i, a in enumerate(ins):
+        a_in[i] = a
+    g = gpu.upload_ct_overlap_list([(buf_in.ptr + 8 * words * i, 2, L, env.scale) for i in range(3)])
+    gpu.download_ct_overlap_list(g, [buf_out.ptr + 8 * words * i for i in range(3)])
+    del g
+    env.ctx.join_transfers()
+    env.ctx.sync()
+    assert np.array_equal(buf_out.array(np.uint64, a_in.shape), a_in)
+    with pytest.raises(ckg.InvalidParams):
+        buf_in.array(np.uint64, (4,) + ins[0].shape)
