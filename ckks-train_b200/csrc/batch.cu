@@ -330,9 +330,7 @@ void Batch::build() {
         for (uint32_t t = 0; t < T; ++t) fwd_conv.push_back(LimbRef{base + t * N, base + t * N, target_prime(c, l, j, t), 0});
       }
       ip.push_back(jb);
-      // the batched inner product indexes limbs by key limb (data limbs, then the key's special
-      // limbs), so jobs of one key at different levels read each key limb together
-      S.ip_max_limbs = std::max(S.ip_max_limbs, (int)(jb.key_q + k));
+      S.ip_max_limbs = std::max(S.ip_max_limbs, (int)ext);
       const size_t per = k + l + 1;
       for (int ba = 0; ba < 2; ++ba) {
         const uint64_t* x = acc + ba * ext * N;

@@ -1076,23 +1076,13 @@ __global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 4 : 1)
     k_inner_product(const __grid_constant__ B ib, const PrimeConst* __restrict__ pc, int log_n) {
   const int n = 1 << log_n;
   // By-value lists: grid (coefficient-pair blocks, limbs, jobs). Device-resident lists (the
-  // batched path, jobs sorted by key): grid (jobs, coefficient-pair blocks, key limbs), so the
-  // jobs that share a key read the same key block back to back and it is served from L2; the
-  // third index is the key's limb (data limbs 0..key_q-1, then its special limbs), the same for
-  // jobs of one key at different levels, and key loads keep the default cache policy there.
+  // batched path, jobs sorted by key): grid (jobs, coefficient-pair blocks, limbs), so the jobs
+  // that share a key read the same key block back to back and it is served from L2.
   constexpr bool kJobFast = std::is_same<B, IpPtrs>::value;
   const IpJob& job = ib.j[kJobFast ? blockIdx.x : blockIdx.z];
-  const int l = job.level;
-  int i;  // limb of Q_l * P: 0..l data, l+1..l+k special
-  if (kJobFast) {
-    const int z = blockIdx.z;
-    if (z <= l) i = z;
-    else if (z >= job.key_q) i = l + 1 + (z - job.key_q);
-    else return;  // a data limb above this job's level
-  } else {
-    i = blockIdx.y;
-  }
+  const int i = kJobFast ? blockIdx.z : blockIdx.y;  // limb of Q_l * P: 0..l data, l+1..l+k special
   const int c = 2 * ((kJobFast ? blockIdx.y : blockIdx.x) * blockDim.x + threadIdx.x);
+  const int l = job.level;
   if (c >= n || i > l + ib.k) return;
   const bool is_q = i <= l;
   const uint32_t prime = is_q ? i : (ib.L + 1) + (i - l - 1);
@@ -1129,10 +1119,8 @@ __global__ void __launch_bounds__(256, std::is_same<B, IpPtrs>::value ? 4 : 1)
           vec = !gather && aligned16(job.conv[j]);
         }
         dv[u] = gather ? make_ulonglong2(__ldg(base + s0), __ldg(base + s1)) : ld_pair(base + c, vec);
-        const uint64_t* kb = job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c;
-        const uint64_t* ka = job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c;
-        kbv[u] = kJobFast ? ld_pair(kb, vkey) : ldcs_pair(kb, vkey);
-        kav[u] = kJobFast ? ld_pair(ka, vkey) : ldcs_pair(ka, vkey);
+        kbv[u] = ldcs_pair(job.key + ((size_t)(2 * j) * key_limbs + key_limb) * n + c, vkey);
+        kav[u] = ldcs_pair(job.key + ((size_t)(2 * j + 1) * key_limbs + key_limb) * n + c, vkey);
       }
     }
   };

@@ -440,14 +440,15 @@ void Server::worker() {
   }
   std::unique_lock<std::mutex> lk(mu_);
   // The lane of the earliest waiting request whose lane has room (-1: none). Without lanes every
-  // request is on lane 0 in arrival order; with them bootstraps go to the least loaded bootstrap
-  // lane (1..), the others to lane 0, and either kind may pass a waiting request of the other.
+  // request is on lane 0 in arrival order; with them bootstraps go to a free bootstrap lane (1..,
+  // one bootstrap in flight per lane, so the lanes add concurrency without holding more working
+  // space and keys), the others to lane 0, and either kind may pass a waiting request of the other.
   const bool laned = !lanes_.empty();
   auto boot_class = [&](const Req& r) { return laned && r.kind == REQ_BOOTSTRAP; };
   auto boot_lane_free = [&]() -> int {
     int best = -1;
     for (int l = 1; l < (int)lanes_.size(); ++l)
-      if (inflight_lane_[l] < cfg_.max_inflight && (best < 0 || inflight_lane_[l] < inflight_lane_[best])) best = l;
+      if (inflight_lane_[l] < 1 && (best < 0 || inflight_lane_[l] < inflight_lane_[best])) best = l;
     return best;
   };
   auto pick = [&]() -> int {

@@ -452,7 +452,8 @@ enum { CKG_REQ_MUL = 0, CKG_REQ_ROTATE = 1, CKG_REQ_MUL_PLAIN = 2, CKG_REQ_MATVE
 /* ckg_server_create flags beside the CKG_HOIST / CKG_BSGS / CKG_LAZY_RELIN bits: compute lanes.
  * CKG_SERVE_BOOT_LANE runs bootstrap flights on a stream of their own and all other flights on
  * another; CKG_SERVE_BOOT_LANES_2 gives bootstraps two streams (two bootstraps at once). Each
- * lane has its own memory pool and up to max_inflight flights. The bootstrap lanes run at the
+ * lane has its own memory pool; the other flights' lane takes up to max_inflight flights, a
+ * bootstrap lane one. The bootstrap lanes run at the
  * device's highest stream priority unless CKG_SERVE_LANES_EQUAL_PRIORITY is set. Lanes start
  * after the client's work queued on the context's stream when the flight is built, and every
  * output is handed back to the context's stream when its request completes. */
