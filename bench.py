@@ -959,7 +959,7 @@ def pcie_ceiling(torch, h2d_bytes, d2h_bytes, ms_per_step, nbytes=1 << 30):
 # (dram__bytes_read.sum + dram__bytes_write.sum) of `bench.py --profile ntt`: its twelve
 # launches (three 256-limb chunks, a column and a row pass each, forward then inverse) summed
 # and halved.
-NTT_TRAFFIC_PER_TRANSFORM = 1358850304
+NTT_TRAFFIC_PER_TRANSFORM = 1370446208
 
 
 def ntt_pair(torch, ctx, n, limbs=768):
