@@ -62,7 +62,7 @@ SERVE_REQUESTS = 1000
 SERVE_LOAD = 0.7             # offered Poisson rate / measured capacity
 SERVE_BOOT_OWNERS = 8        # n16_boot serving with bootstrap requests
 SERVE_BOOT_BUDGET = 96 << 30
-SERVE_BOOT_LANES = 2          # bootstrap lanes of the bootstrap-serving runs (0: one stream)
+SERVE_BOOT_LANES = 1          # bootstrap lanes of the bootstrap-serving runs (0: one stream)
 SERVE_BOOT_SPILL_OWNERS = 32  # the same with key spill: up to 32 owners within host memory
 SERVE_BOOT_SPILL_BUDGET = 48 << 30
 SERVE_BOOT_SPILL_REQUESTS = 400
