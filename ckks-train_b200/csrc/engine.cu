@@ -65,8 +65,13 @@ uint64_t* XferCache::take(size_t words) {
 void XferCache::give(uint64_t* p, size_t words, cudaEvent_t done) {
   std::lock_guard<std::mutex> lk(mu);
   blocks.push_back({p, words, done});
-  // at most kMaxBlocks kept: the oldest completed ones beyond that go back to the pool
-  for (size_t i = 0; blocks.size() > kMaxBlocks && i < blocks.size();) {
+  // at most kMaxBlocks and max_bytes kept: the oldest completed ones beyond that go back to the pool
+  auto bytes = [&] {
+    size_t b = 0;
+    for (const Block& x : blocks) b += x.words * 8;
+    return b;
+  };
+  for (size_t i = 0; (blocks.size() > kMaxBlocks || bytes() > max_bytes) && i < blocks.size();) {
     if (cudaEventQuery(blocks[i].done) == cudaSuccess) {
       cudaEventDestroy(blocks[i].done);
       cudaFreeAsync(blocks[i].p, stream->s);
@@ -158,6 +163,12 @@ void Context::transfer_streams() {
     xcache = std::make_shared<XferCache>();
     xcache->device = device;
     xcache->pool = xpool;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      total_b = (size_t)96 << 30;
+    }
+    xcache->max_bytes = total_b / 3;
     xcache->stream = xfer_in;
   }
 }

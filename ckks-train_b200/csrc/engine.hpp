@@ -72,6 +72,7 @@ struct XferCache {
   static constexpr size_t kMaxBlocks = 16;
   std::mutex mu;
   std::vector<Block> blocks;  // oldest first
+  size_t max_bytes = 0;       // kept at most (a third of the device's memory)
   int device = 0;
   cudaMemPool_t pool = nullptr;  // where new blocks come from and trimmed ones go back
   StreamPtr stream;               // the upload stream (allocations and trims)
