@@ -1,7 +1,9 @@
 """Key-switching throughput of the B200 RNS-CKKS evaluator path (one JSON line).
 
-Beside it: `bootstrap` -- one full n16_boot bootstrap (ms, device events) -- and `serving`
--- the serving loop's throughput and p50/p99 latency under Poisson arrivals.
+Beside it: `bootstrap` -- one full n16_boot bootstrap (ms, device events); `mlp_step` -- the
+encrypted training step; `serving_one_lane` / `serving` / `serving_boot_spill` / `serving_spill`
+-- the serving loop's throughput and p50/p99 latency under Poisson arrivals (one stream, a
+bootstrap lane at the same offered load, bootstrap-key spill, key spill without bootstraps).
 
 Parameters: N = 2^16, 24 x 50-bit data primes + 8 x 60-bit special primes, dnum = 3
 (alpha = 8), 31 evaluation keys (relinearization + 30 Galois keys for +-2^k, k = 0..14).
@@ -20,10 +22,14 @@ individual evaluator call.
 pinned host memory, the batch built and run, every result downloaded to pinned host
 memory, all inside the timed region. `--impl reference` times the reference's CPU path
 (the oracle's restatement of crates/ckks-train-ckks with OpenMP over the units of its
-`parallel` feature) on a bounded sample of the same op mix.
+`parallel` feature) on a bounded sample of the same op mix, cross-checks it against the
+reference's published CPU time, and times the reference's own CUDA kernels on the same GPU
+(`reference_gpu`).
 
 Multi-GPU: each rank runs the same stream on its own GPU with its own keys and inputs
-(independent ciphertexts shard with no exchange: weak scaling); time = max over ranks.
+(independent ciphertexts shard with no exchange: weak scaling); time = max over ranks. Serving
+on N GPUs places every key owner on one rank (ckks-train_b200/router.py) and pools the ranks'
+latencies.
 """
 
 import argparse
