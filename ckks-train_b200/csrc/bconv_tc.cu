@@ -184,32 +184,24 @@ struct TcSmem {
 // soon as A is complete while warpgroup 0 sums the products in source order into e; both
 // warpgroups prefetch their half of the next tile's sources, wait for the MMA, and reduce half
 // of the targets each, four at a time (one 32-column TMEM load).
-// With part_targets > 0 the targets are split over gridDim.z parts of part_targets each (an even
-// count): part z computes targets z * part_targets.. with the slice of B that holds them, so a
-// CTA's MMA width and TMEM allocation halve and more CTAs fit on an SM.
 template <int NS, class B>
 __global__ void __launch_bounds__(kTcThreads)
     k_bconv_tc(const __grid_constant__ B cb, const PrimeConst* __restrict__ pc, int n, int tiles_per_cta,
-               uint32_t ncols, int part_targets) {
+               uint32_t ncols) {
   constexpr int KB = NS <= 4 ? 32 : 64;  // operand bytes per coefficient (y words, zero-padded)
   constexpr int NW = KB / 8;
   constexpr int H = (NS + 1) / 2;        // sources of warpgroup 0; warpgroup 1 takes the rest
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TcSmem<KB>& S = *reinterpret_cast<TcSmem<KB>*>(smem_raw);
   const ConvJob& job = cb.j[blockIdx.y];
-  const int nd_all = job.n_dst;
-  const int o0 = part_targets > 0 ? (int)blockIdx.z * part_targets : 0;  // first target of this part
-  const int nd = part_targets > 0 ? min(part_targets, nd_all - o0) : nd_all;
-  if (nd <= 0) return;  // a part beyond this job's targets (the whole CTA, before any barrier)
+  const int nd = job.n_dst;
   const uint64_t* tab = job.table;
-  const uint64_t* tc = tab + ConvLayout::tc_offset(NS, nd_all);
+  const uint64_t* tc = tab + ConvLayout::tc_offset(NS, nd);
   const uint64_t head = __ldg(tc);
-  const uint32_t n_all = (uint32_t)(head >> 32);
-  const uint32_t N = part_targets > 0 ? min(8u * (uint32_t)part_targets, n_all - 8u * (uint32_t)o0) : n_all;
+  const uint32_t N = (uint32_t)(head >> 32);
   // a table without a valid block for this width (the host never launches one) does nothing
-  const bool bad = (uint32_t)head != (uint32_t)KB || n_all < 8 * (uint32_t)nd_all || n_all > 256 || (n_all & 15) ||
-                   (part_targets & 1) || 8u * (uint32_t)o0 >= n_all || N < 8 * (uint32_t)nd || (N & 15) ||
-                   N > ncols || ncols < 32 * (uint32_t)((nd + 3) / 4);
+  const bool bad = (uint32_t)head != (uint32_t)KB || N < 8 * (uint32_t)nd || N > 256 || (N & 15) || N > ncols ||
+                   ncols < 32 * (uint32_t)((nd + 3) / 4);
   const int tid = threadIdx.x, warp = tid >> 5, g = tid >> 7, r = tid & (kTcRows - 1);
   if (tid == 0) {
     mbar_init(&S.bar[0], 1);
@@ -219,14 +211,13 @@ __global__ void __launch_bounds__(kTcThreads)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) tmem_alloc(&S.tslot, ncols);
-  for (int i = tid; i < kTcRec * nd; i += kTcThreads) S.trec[i] = __ldg(tc + 2 + kTcRec * o0 + i);
+  for (int i = tid; i < kTcRec * nd; i += kTcThreads) S.trec[i] = __ldg(tc + 2 + i);
   for (int i = tid; i < ConvLayout::kSrcWords * NS; i += kTcThreads) S.srec[i] = __ldg(tab + ConvLayout::kHeadWords + i);
   tc_before_sync();
   __syncthreads();
   tc_after_sync();
   const uint32_t tmem = S.tslot;
-  // this part's rows of B: targets o0.. (8 rows of KB bytes each, KB / 8 words per row)
-  if (tid == 0 && !bad) bulk_g2s(S.b, tc + 2 + kTcRec * nd_all + (size_t)o0 * KB, N * KB, &S.bar[0]);
+  if (tid == 0 && !bad) bulk_g2s(S.b, tc + 2 + kTcRec * nd, N * KB, &S.bar[0]);
   const int tile0 = blockIdx.x * tiles_per_cta;
   const int tile_end = bad ? tile0 : min(tile0 + tiles_per_cta, n / kTcRows);
   const int j0 = g == 0 ? 0 : H, j1 = g == 0 ? H : NS;  // this thread's sources
@@ -301,7 +292,7 @@ __global__ void __launch_bounds__(kTcThreads)
       const uint64_t e = S.e[r];
       const double ed = (double)e;
       const size_t dstride = job.dst_stride;
-      uint64_t* dst = job.dst + (size_t)tile * kTcRows + r + (size_t)(o0 + 4 * ga) * dstride;
+      uint64_t* dst = job.dst + (size_t)tile * kTcRows + r + (size_t)(4 * ga) * dstride;
       for (int gi = ga; gi < gb; ++gi) {
         uint32_t v[32];
         tmem_ld32(tmem + lane_base + 32 * gi, v);
@@ -334,26 +325,18 @@ void tc_launch(const DevTables& d, const B& cb, int count, int max_dst, cudaStre
   constexpr int KB = NS <= 4 ? 32 : 64;
   const int n = 1 << d.log_n;
   const int tiles = n / kTcRows;
-  // More than 16 targets would need 256 TMEM columns per CTA (two CTAs per SM): split them into two
-  // parts of an even count each instead (128 columns, so TMEM admits four and registers three).
-  int parts = 1, per = 0, width = max_dst;
-  if (8 * max_dst > 128) {
-    parts = 2;
-    per = (((max_dst + 1) / 2) + 1) & ~1;
-    width = per;
-  }
   uint32_t ncols = 32;
-  while (ncols < (uint32_t)(8 * width) || ncols < 32u * (uint32_t)((width + 3) / 4)) ncols <<= 1;
+  while (ncols < (uint32_t)(8 * max_dst)) ncols <<= 1;  // the MMA width N <= ncols
   // CTAs per SM are capped by shared memory so that their TMEM never exceeds the SM's 512 columns.
   const int per_sm = std::min(8, 512 / (int)ncols);
   int smem = (int)sizeof(TcSmem<KB>);
   if (per_sm < 8) smem = std::max(smem, 233472 / (per_sm + 1));
   // enough CTAs for every SM, several tiles each
-  const long total = (long)tiles * count * parts;
+  const long total = (long)tiles * count;
   const int tpc = (int)std::max(1L, std::min(16L, total / (148L * per_sm * 2)));
   auto fn = k_bconv_tc<NS, B>;
   cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  fn<<<dim3((tiles + tpc - 1) / tpc, count, parts), kTcThreads, smem, st>>>(cb, d.prime, n, tpc, ncols, per);
+  fn<<<dim3((tiles + tpc - 1) / tpc, count), kTcThreads, smem, st>>>(cb, d.prime, n, tpc, ncols);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
