@@ -285,7 +285,8 @@ CKG_API uint64_t ckg_batch_key_switches(const ckg_batch* b);
  * - the chunk size of a batch: key-switching ops per launch sequence (default 128).
  * ckg_batch_autotune times every pair of the grid {0, 32, 64, 128, 256} x {64, 128, 256} on
  * the batch's own ops (`reps` graph replays each after a warm-up, no OpCounter change), keeps
- * the fastest: the wave on the context, the chunk size on the batch (rebuilt at its next
+ * the fastest (the default shape 0 x 128 when it is within 1% of it): the wave on the context,
+ * the chunk size on the batch (rebuilt at its next
  * run or capture). `trials` receives 3 words per trial (wave, chunk size, microseconds per
  * replay), at most `max_trials` of them; `n_trials` the count. */
 CKG_API int ckg_ctx_set_ntt_wave(ckg_ctx* ctx, int32_t limbs);
