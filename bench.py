@@ -197,6 +197,97 @@ class Setup:
         return p, t
 
 
+CFG1_LOG_N, CFG1_Q_BITS, CFG1_P_BITS, CFG1_DNUM, CFG1_SCALE_BITS = 13, [45] * 4, [60], 4, 45
+CFG1_PAIRS = 64
+
+
+class Config1:
+    """The small-ring workload: N = 2^13, 4 x 45-bit q (descending prime search from 2^45), one
+    60-bit p, dnum 4; 64 seeded uniform ciphertext pairs at the top level; 64 x (HMult + relin +
+    rescale) and 64 x rotation by +1 per step (128 key switches), per op and as one batched
+    CUDA-graph replay. Synthetic uniform key material (relinearization and the +1 Galois key)."""
+
+    text = ("N=2^13, 4x45-bit q + 1x60-bit p, dnum 4; 64 ciphertext pairs; 64 x (HMult+relin+rescale) + "
+            "64 x rotation by +1 per step")
+
+    def __init__(self, ckg, torch, device):
+        self.torch = torch
+        self.ctx = ctx = ckg.Context.from_bits(CFG1_LOG_N, CFG1_Q_BITS, CFG1_P_BITS, CFG1_DNUM, device=device,
+                                               scale_bits=CFG1_SCALE_BITS)
+        n, L = ctx.n, len(ctx.q) - 1
+        gen = torch.Generator(device=f"cuda:{device}")
+        gen.manual_seed(13)
+        qall = torch.tensor(ctx.q + ctx.p, dtype=torch.int64, device=f"cuda:{device}")
+
+        def uniform(shape, qcol):
+            t = torch.randint(0, 1 << 62, shape, generator=gen, device=qall.device, dtype=torch.int64) % qcol
+            torch.cuda.synchronize()
+            return t
+
+        shape = (CFG1_DNUM, 2, len(ctx.q) + ctx.k, n)
+        keys = [uniform(shape, qall.view(1, 1, -1, 1)) for _ in range(2)]
+        self.relin = ctx.upload_key_device(keys[0].data_ptr(), shape, 0)
+        self.gk = ctx.upload_key_device(keys[1].data_ptr(), shape, galois_elt(n, 1))
+        self.ev = ev = ckg.CudaEvaluator(ctx, self.relin, [self.gk])
+        scale = 2.0 ** CFG1_SCALE_BITS
+        self.pairs = []
+        for _ in range(CFG1_PAIRS):
+            a, b = (uniform((2, L + 1, n), qall[: L + 1].view(1, -1, 1)) for _ in range(2))
+            self.pairs.append((ev.upload_ct_device(a.data_ptr(), 2, L, scale),
+                               ev.upload_ct_device(b.data_ptr(), 2, L, scale)))
+        ctx.sync()
+        self.batch = ckg.Batch(ev)
+        self.outs = [self.batch.mul_relin_rescale(a, b) for a, b in self.pairs]
+        self.outs += [self.batch.rotate(a, 1) for a, _ in self.pairs]
+        self.batch.capture_graph()
+
+    def step_per_op(self):
+        ev = self.ev
+        return [(ev.rescale(ev.mul(a, b)), ev.rotate(a, 1)) for a, b in self.pairs]
+
+    def measure(self, steps=20, warmup=3):
+        torch, ctx = self.torch, self.ctx
+        ms_op = timed(torch, ctx, self.step_per_op, steps, warmup)[0]
+        ms_b = timed(torch, ctx, self.batch.launch_graph, steps, warmup)[0]
+        ks = 2 * CFG1_PAIRS
+        return {"workload": self.text, "unit": "keyswitch/s",
+                "per_op": round(ks * steps / (ms_op * 1e-3), 1), "per_op_ms_per_step": round(ms_op / steps, 3),
+                "batched": round(ks * steps / (ms_b * 1e-3), 1), "batched_ms_per_step": round(ms_b / steps, 3),
+                "data": "synthetic uniform ciphertexts and key material"}
+
+
+def cpu_config1(threads, reps=3):
+    """Config 1's workload on the CPU path (the oracle's evaluator) with keys from its key
+    generator: key switches per second on `threads` OpenMP threads (the best of `reps` steps) and
+    on one thread (one step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.set_threads(threads)
+    P = O.Params.from_bits(CFG1_LOG_N, CFG1_Q_BITS, CFG1_P_BITS, CFG1_SCALE_BITS, CFG1_DNUM)
+    kg = O.KeyGenerator(P, 13)
+    e1 = O.galois_elt(P.n, 1)
+    ev = O.Evaluator(P, kg.relin_key(), {e1: kg.galois_key(e1)})
+    L, scale = P.max_level, 2.0 ** CFG1_SCALE_BITS
+    pairs = [(ev.ct(np.stack([P.random_q(4 * i + 1, L), P.random_q(4 * i + 2, L)]), scale),
+              ev.ct(np.stack([P.random_q(4 * i + 3, L), P.random_q(4 * i + 4, L)]), scale))
+             for i in range(CFG1_PAIRS)]
+    def step():
+        t0 = time.perf_counter()
+        for a, b in pairs:
+            ev.rescale(ev.mul(a, b))
+            ev.rotate(a, 1)
+        return time.perf_counter() - t0
+
+    best = min(step() for _ in range(reps))
+    O.set_threads(1)
+    one = step()
+    O.set_threads(threads)
+    return {"value": round(2 * CFG1_PAIRS / best, 1), "unit": "keyswitch/s", "cores": threads,
+            "one_thread": round(2 * CFG1_PAIRS / one, 1), "kind": "port",
+            "sample": f"the whole workload: best of {reps} steps on {threads} threads {best * 1e3:.1f} ms, "
+                      f"one step on 1 thread {one * 1e3:.1f} ms"}
+
+
 class Mix:
     """The batched uneven-level stream."""
 
@@ -1219,6 +1310,7 @@ def main():
     ap.add_argument("--ntt-wave", type=int, default=None, help="fixed NTT limb wave (with --chunk-items; default: autotune)")
     ap.add_argument("--chunk-items", type=int, default=None, help="fixed batch chunk size (with --ntt-wave)")
     ap.add_argument("--mlp-only", action="store_true", help="measure the encrypted MLP training step only")
+    ap.add_argument("--config1-only", action="store_true", help="measure the N=2^13 small-ring workload only")
     ap.add_argument("--serve-owners", type=int, default=SERVE_OWNERS)
     ap.add_argument("--serve-requests", type=int, default=SERVE_REQUESTS)
     ap.add_argument("--profile", default=None, choices=["batch", "plain", "boot", "ntt"],
@@ -1300,6 +1392,13 @@ def main():
         out = MlpBench(ckg, torch, local).measure()
         if rank == 0:
             print(json.dumps({"mlp_step": out}))
+        return
+    if args.config1_only:
+        out = Config1(ckg, torch, local).measure()
+        if not args.no_cpu_baseline:
+            out["cpu"] = cpu_config1(os.cpu_count() or 1)
+        if rank == 0:
+            print(json.dumps({"config1": out}))
         return
     if args.boot_only:
         out = BootBench(ckg, torch, local).measure()
@@ -1425,6 +1524,12 @@ def main():
         mb = MlpBench(ckg, torch, local)
         mlp_step = mb.measure()
         del mb
+    config1 = None
+    if single:
+        release()
+        c1 = Config1(ckg, torch, local)
+        config1 = c1.measure()
+        del c1
     serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
         release()
@@ -1456,6 +1561,8 @@ def main():
         v, sample = cpu_sample(CpuPath(threads))
         cpu = dict({"value": round(v, 3), "unit": unit, "cores": threads, "kind": "port", "sample": sample},
                    **cpu_host(), crosscheck=cpu_crosscheck(threads))
+        if config1:
+            config1["cpu"] = cpu_config1(threads)
     if rank == 0:
         line = {"metric": metric, "value": round(value, 2), "unit": unit, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -1468,7 +1575,7 @@ def main():
                 "gpu_launches": int(launches_per_step * args.steps), "plain": plain,
                 "keyswitch_raw": ks_raw, "ntt_pair_32_limbs": ntt32, "roofline": roof,
                 "roofline_stream": roof_stream,
-                "bootstrap": boot, "mlp_step": mlp_step, "serving": serving, "serving_one_lane": serving_one_lane,
+                "bootstrap": boot, "mlp_step": mlp_step, "config1": config1, "serving": serving, "serving_one_lane": serving_one_lane,
                 "serving_boot_spill": serving_boot_spill, "serving_spill": serving_spill, "cpu_baseline": cpu,
                 "clocks": clk.summary()}
         print(json.dumps(line))
