@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 #include <optional>
+#include <thread>
 
 #include "boot.hpp"
 
@@ -596,12 +597,62 @@ uint32_t Bootstrapper::output_level() const {
   return ctx_->L - (bp_.ctos_levels + bp_.evalmod_levels + bp_.stoc_levels);
 }
 
+namespace {
+// `to` waits for the work queued on `from` so far.
+void wait_for(cudaStream_t to, cudaStream_t from) {
+  cudaEvent_t e;
+  CKG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaError_t err = cudaEventRecord(e, from);
+  if (err == cudaSuccess) err = cudaStreamWaitEvent(to, e, 0);
+  cudaEventDestroy(e);
+  if (err != cudaSuccess) throw_cuda(err, "cudaStreamWaitEvent");
+}
+}  // namespace
+
+// The real and imaginary EvalMods are independent (the same ops on two ciphertexts): they run
+// concurrently, each on one of the context's two auxiliary lanes, issued from two host threads,
+// so the small launches of one fill the SMs the other leaves idle. Each keeps its own op order,
+// so the results are those of the sequential evaluation; the caller's stream waits for both
+// lanes, and the results' buffers are freed on the caller's stream from then on.
+std::pair<Ct, Ct> Bootstrapper::eval_mod_pair(Evaluator& inner, const Ct& re_in, const Ct& im_in) {
+  Lane& la = ctx_->aux_lane(0);
+  Lane& lb = ctx_->aux_lane(1);
+  const cudaStream_t caller = ctx_->stream;
+  const StreamPtr caller_res = ctx_->cur_sres();
+  wait_for(la.sres->s, caller);
+  wait_for(lb.sres->s, caller);
+  Ct re, im;
+  std::exception_ptr err_re, err_im;
+  std::thread t([&] {
+    try {
+      ctx_->activate();
+      LaneScope scope(*ctx_, lb);
+      im = eval_mod(inner, im_in, bp_, coeffs_);
+    } catch (...) {
+      err_im = std::current_exception();
+    }
+  });
+  try {
+    LaneScope scope(*ctx_, la);
+    re = eval_mod(inner, re_in, bp_, coeffs_);
+  } catch (...) {
+    err_re = std::current_exception();
+  }
+  t.join();
+  wait_for(caller, la.sres->s);  // before anything the caller queues or frees next
+  wait_for(caller, lb.sres->s);
+  if (err_re) std::rethrow_exception(err_re);
+  if (err_im) std::rethrow_exception(err_im);
+  re->buf->sres = caller_res;
+  im->buf->sres = caller_res;
+  return {re, im};
+}
+
 Ct Bootstrapper::pipeline(Evaluator& inner, const Ct& ct) {  // bootstrapper.rs:431-473
   Ct raised = to_sparse_ ? inner.mod_raise(ct, *to_sparse_, *to_dense_) : inner.mod_raise_main_key(ct);
   raised = inner.relabel(raised, (double)ctx_->primes[0]);
   auto reim = coeff_to_slot(inner, raised, ctos_);
-  Ct re = eval_mod(inner, reim.first, bp_, coeffs_);
-  Ct im = eval_mod(inner, reim.second, bp_, coeffs_);
+  auto [re, im] = eval_mod_pair(inner, reim.first, reim.second);
   const uint32_t start = stoc_[0]->level;
   auto to_stoc = [&](const Ct& c) {
     if (c->scale != evalmod_scale_) throw Error(ST_SCALE_MISMATCH, "scale mismatch");

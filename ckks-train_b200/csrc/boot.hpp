@@ -66,6 +66,7 @@ class Bootstrapper {
 
  private:
   Ct pipeline(Evaluator& inner, const Ct& ct);
+  std::pair<Ct, Ct> eval_mod_pair(Evaluator& inner, const Ct& re, const Ct& im);
   Context* ctx_;
   BootParams bp_;
   std::vector<LtPtr> ctos_, stoc_;

@@ -386,6 +386,13 @@ void Context::upload_staged(void* dst, const void* src, size_t bytes) {
   stage_head += need;
 }
 
+Lane& Context::aux_lane(int i) {
+  if (i < 0 || i > 1) throw Error(ST_INVALID_PARAMS, "auxiliary lane index out of range");
+  std::lock_guard<std::mutex> lk(aux_mu);
+  if (!aux_lanes[i]) aux_lanes[i] = std::make_unique<Lane>(device);
+  return *aux_lanes[i];
+}
+
 void Context::join_transfers() {
   activate();
   if (xfer_in) stream_after(stream, xfer_in->s);

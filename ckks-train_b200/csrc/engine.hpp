@@ -228,6 +228,12 @@ struct Context {
   // Not allowed while the stream is being captured (the graph would read a reused slot).
   void upload_staged(void* dst, const void* src, size_t bytes);
 
+  // Two lanes for work one caller splits over concurrent host threads (the bootstrap's two
+  // independent EvalMods), created on first use and kept for the context's life.
+  Lane& aux_lane(int i);
+  std::mutex aux_mu;
+  std::unique_ptr<Lane> aux_lanes[2];
+
   // Host-side accounting of the overlapped transfers and allocation retries (ckg_ctx_transfer_stats).
   std::atomic<uint64_t> st_upload_calls{0}, st_upload_bytes{0}, st_upload_alloc_ns{0}, st_upload_copy_ns{0},
       st_download_calls{0}, st_download_ns{0}, st_alloc_retries{0};
