@@ -254,6 +254,32 @@ Ct Evaluator::matvec_plain_sum_sparse(const std::vector<std::pair<const SparseDi
     xs.push_back(std::move(row));
   }
   Ct acc;
+  // With shared giant steps the giant blocks are independent until their sum: their inner sums
+  // first, then every block's giant rotation in one launch sequence (rotate_many), then the sum in
+  // block order.
+  if (cfg_.bsgs) {
+    std::vector<std::pair<Ct, int32_t>> blocks;
+    for (uint32_t k1 = 0; k1 < giant; ++k1) {
+      const int64_t shift = (offset + (int64_t)baby * k1) * (int64_t)stride;
+      std::vector<std::pair<Ct, Pt>> prods;
+      for (size_t ti = 0; ti < terms.size(); ++ti)
+        for (uint32_t k2 = 0; k2 < baby; ++k2) {
+          const Pt& w = terms[ti].first->entries[k1 * baby + k2];
+          if (w) prods.push_back({xs[ti][k2], w});
+        }
+      if (!prods.empty()) blocks.push_back({mac_plain(prods), (int32_t)shift});
+    }
+    std::vector<std::pair<Ct, int32_t>> to_rotate;
+    for (auto& b : blocks)
+      if (b.second != 0) to_rotate.push_back(b);
+    std::vector<Ct> rotated = rotate_many(to_rotate);
+    size_t ri = 0;
+    for (auto& b : blocks) {
+      const Ct block = b.second != 0 ? rotated[ri++] : b.first;
+      acc = acc ? add(acc, block) : block;
+    }
+    return acc;
+  }
   for (uint32_t k1 = 0; k1 < giant; ++k1) {
     const int64_t shift = (offset + (int64_t)baby * k1) * (int64_t)stride;
     Ct block;

@@ -468,6 +468,52 @@ Ct Evaluator::apply_galois(const Ct& a, uint64_t elt) {  // evaluator.rs:640-646
   return r;
 }
 
+std::vector<Ct> Evaluator::rotate_many(const std::vector<std::pair<Ct, int32_t>>& items) {
+  // rotate() of each item (same checks, same counts), the key switches of one level as one
+  // launch sequence
+  for (auto& it : items) check_galois_input(it.first);
+  std::vector<Ct> out(items.size());
+  std::map<uint32_t, std::vector<size_t>> by_level;
+  for (size_t i = 0; i < items.size(); ++i) {
+    if (!rotation_elt(items[i].second)) {
+      out[i] = items[i].first;
+    } else {
+      galois_key(*rotation_elt(items[i].second));  // the key exists (before any work)
+      by_level[items[i].first->level].push_back(i);
+    }
+  }
+  ctx_->activate();
+  uint64_t rotations = 0;
+  for (auto& kv : by_level) {
+    const uint32_t l = kv.first, limbs = l + 1;
+    auto tmp = ctx_->alloc(kv.second.size() * (size_t)limbs * ctx_->n);
+    std::vector<KsJob> ks;
+    for (size_t k = 0; k < kv.second.size(); ++k) {
+      const Ct& a = items[kv.second[k]].first;
+      const uint64_t elt = *rotation_elt(items[kv.second[k]].second);
+      const uint32_t* perm = ctx_->perm(elt);
+      uint64_t* t = tmp->p + k * (size_t)limbs * ctx_->n;
+      std::vector<LimbRef> refs;
+      unary_comp(*ctx_, a->comp(1), t, limbs, refs);
+      launch_unary(ctx_->dt, refs.data(), (int)refs.size(), 3, nullptr, perm, ctx_->stream);  // sigma_g(c1)
+      Ct r = new_ct(2, l, a->scale);
+      KsJob j;
+      j.in = t;
+      j.key = &galois_key(elt);
+      j.out_b = r->comp_mut(0);
+      j.out_a = r->comp_mut(1);
+      j.add_b = a->comp(0);
+      j.add_b_perm = perm;  // + sigma_g(c0)
+      ks.push_back(j);
+      out[kv.second[k]] = r;
+      rotations++;
+    }
+    key_switch_many(*ctx_, ks, l);
+  }
+  count([&](OpCounter& c) { c.rotations += rotations; });
+  return out;
+}
+
 Ct Evaluator::rotate(const Ct& a, int32_t steps) {  // evaluator.rs:534-540
   check_galois_input(a);
   auto e = rotation_elt(steps);

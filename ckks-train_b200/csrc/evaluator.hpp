@@ -127,6 +127,9 @@ class Evaluator {
   Ct rotate(const Ct& a, int32_t steps);
   Ct conjugate(const Ct& a);
   std::vector<Ct> hoisted_rotate(const Ct& a, const std::vector<int32_t>& steps);
+  // rotate() of several ciphertexts by their own steps: the key switches of each level as one
+  // launch sequence (same results and counts as one rotate() per item)
+  std::vector<Ct> rotate_many(const std::vector<std::pair<Ct, int32_t>>& items);
   double exact_product_scale(uint32_t level, double target) const;
   Ct matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x);
   Ct matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x);
