@@ -788,7 +788,7 @@ class BootBench:
     def step(self):
         self.out = self.bs.bootstrap(self.ev, self.ct)
 
-    def measure(self, steps=5, warmup=2):
+    def measure(self, steps=8, warmup=4):
         ckg, torch = self.ckg, self.torch
         self.step()
         self.ctx.sync()
