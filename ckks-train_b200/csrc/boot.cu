@@ -239,18 +239,22 @@ Ct Evaluator::matvec_plain_sum_sparse(const std::vector<std::pair<const SparseDi
   const uint32_t baby = d0.baby, giant = d0.giant, stride = d0.stride;
   const int64_t offset = d0.offset;
   std::vector<std::vector<Ct>> xs;  // xs[t][k2] = rot(x_t, k2 stride) for the baby steps in use
-  for (auto& t : terms) {
-    std::vector<uint32_t> used;
+  std::vector<std::vector<uint32_t>> used(terms.size());
+  std::vector<std::pair<Ct, std::vector<int32_t>>> hoists;
+  for (size_t ti = 0; ti < terms.size(); ++ti) {
     for (uint32_t k2 = 0; k2 < baby; ++k2) {
       bool any = false;
-      for (uint32_t k1 = 0; k1 < giant; ++k1) any = any || t.first->entries[k1 * baby + k2] != nullptr;
-      if (any) used.push_back(k2);
+      for (uint32_t k1 = 0; k1 < giant; ++k1) any = any || terms[ti].first->entries[k1 * baby + k2] != nullptr;
+      if (any) used[ti].push_back(k2);
     }
     std::vector<int32_t> steps;
-    for (uint32_t k2 : used) steps.push_back((int32_t)(k2 * stride));
-    auto rotated = hoisted_rotate(t.second, steps);
+    for (uint32_t k2 : used[ti]) steps.push_back((int32_t)(k2 * stride));
+    hoists.push_back({terms[ti].second, steps});
+  }
+  auto rotated = hoisted_rotate_many(hoists);  // every term's baby steps in one launch sequence
+  for (size_t ti = 0; ti < terms.size(); ++ti) {
     std::vector<Ct> row(baby);
-    for (size_t i = 0; i < used.size(); ++i) row[used[i]] = rotated[i];
+    for (size_t i = 0; i < used[ti].size(); ++i) row[used[ti][i]] = rotated[ti][i];
     xs.push_back(std::move(row));
   }
   Ct acc;

@@ -576,6 +576,78 @@ std::vector<Ct> Evaluator::hoisted_rotate(const Ct& a, const std::vector<int32_t
   return out;
 }
 
+std::vector<std::vector<Ct>> Evaluator::hoisted_rotate_many(
+    const std::vector<std::pair<Ct, std::vector<int32_t>>>& items) {
+  // hoisted_rotate() of each item (same checks, results and counts); items at one level share
+  // one decomposition launch sequence and one key-switch launch sequence
+  bool same = cfg_.hoist && !items.empty();
+  for (auto& it : items) same = same && it.first->level == items[0].first->level;
+  if (!same) {
+    std::vector<std::vector<Ct>> out;
+    for (auto& it : items) out.push_back(hoisted_rotate(it.first, it.second));
+    return out;
+  }
+  for (auto& it : items) check_galois_input(it.first);
+  std::vector<std::vector<Ct>> out(items.size());
+  std::vector<std::vector<std::pair<uint64_t, const DevKey*>>> keys(items.size());
+  std::vector<size_t> with;  // items with a nontrivial step
+  for (size_t t = 0; t < items.size(); ++t) {
+    keys[t].assign(items[t].second.size(), {0, nullptr});
+    bool any = false;
+    for (size_t i = 0; i < items[t].second.size(); ++i) {
+      auto e = rotation_elt(items[t].second[i]);
+      if (e) {
+        keys[t][i] = {*e, &galois_key(*e)};
+        any = true;
+      }
+    }
+    out[t].resize(items[t].second.size());
+    if (any) with.push_back(t);
+  }
+  uint64_t nontrivial = 0;
+  if (!with.empty()) {
+    ctx_->activate();
+    const uint32_t l = items[0].first->level;
+    const size_t cl = conv_limbs(*ctx_, l) * ctx_->n;
+    auto conv = ctx_->alloc(cl * with.size());
+    std::vector<const uint64_t*> ins;
+    std::vector<uint64_t*> convs;
+    for (size_t k = 0; k < with.size(); ++k) {
+      ins.push_back(items[with[k]].first->comp(1));
+      convs.push_back(conv->p + k * cl);
+    }
+    mod_up_many(*ctx_, ins, l, convs);
+    std::vector<KsJob> jobs;
+    for (size_t k = 0; k < with.size(); ++k) {
+      const size_t t = with[k];
+      const Ct& a = items[t].first;
+      for (size_t i = 0; i < items[t].second.size(); ++i) {
+        if (!keys[t][i].second) continue;
+        const uint32_t* perm = ctx_->perm(keys[t][i].first);
+        Ct r = new_ct(2, l, a->scale);
+        KsJob j;
+        j.in = a->comp(1);
+        j.key = keys[t][i].second;
+        j.out_b = r->comp_mut(0);
+        j.out_a = r->comp_mut(1);
+        j.add_b = a->comp(0);
+        j.add_b_perm = perm;
+        j.perm = perm;
+        j.conv = convs[k];
+        jobs.push_back(j);
+        out[t][i] = r;
+        nontrivial++;
+      }
+    }
+    key_switch_many(*ctx_, jobs, l);
+  }
+  for (size_t t = 0; t < items.size(); ++t)
+    for (size_t i = 0; i < items[t].second.size(); ++i)
+      if (!keys[t][i].second) out[t][i] = items[t].first;
+  count([&](OpCounter& c) { c.rotations += nontrivial; });
+  return out;
+}
+
 // ---- BSGS matrix-vector products (crates/ckks-train-ckks/src/linalg.rs:608-893) -------
 
 namespace {

@@ -130,6 +130,9 @@ class Evaluator {
   // rotate() of several ciphertexts by their own steps: the key switches of each level as one
   // launch sequence (same results and counts as one rotate() per item)
   std::vector<Ct> rotate_many(const std::vector<std::pair<Ct, int32_t>>& items);
+  // hoisted_rotate() of several ciphertexts, each by its own steps: at one level, one
+  // decomposition and one key-switch launch sequence for all (same results and counts)
+  std::vector<std::vector<Ct>> hoisted_rotate_many(const std::vector<std::pair<Ct, std::vector<int32_t>>>& items);
   double exact_product_scale(uint32_t level, double target) const;
   Ct matvec_plain(uint32_t d, uint32_t stride, const std::vector<Pt>& entries, const Ct& x);
   Ct matvec_enc(uint32_t d, uint32_t stride, const std::vector<Ct>& entries, const Ct& x);
