@@ -72,6 +72,7 @@ SERVE_BOOT_LANES = 1          # bootstrap lanes of the bootstrap-serving runs (0
 SERVE_BOOT_SPILL_OWNERS = 32  # the same with key spill: up to 32 owners within host memory
 SERVE_BOOT_SPILL_BUDGET = 48 << 30
 SERVE_BOOT_SPILL_REQUESTS = 400
+SERVE_RESULT_DEADLINE_S = 600  # a serving run stops collecting (and counts the rest as failed) after this
 
 
 def load_package():
@@ -548,33 +549,55 @@ class Serving:
         gaps = self.rng.exponential(1.0 / rate, count) if rate else np.zeros(count)
         dues = np.cumsum(gaps)
         local = [(d, q) for d, q in zip(dues, reqs) if q is not None]
-        count = len(local)
-        ids, times, lag = [], [], [0.0]
+        ids, times, lag, failed, collected = [], [], [0.0], [], [0]
+        submitted = threading.Event()  # every submit() has returned (or raised)
         done = threading.Event()
+        deadline = time.perf_counter() + SERVE_RESULT_DEADLINE_S
 
         def collect():
-            i = 0
-            while i < count:
-                if i >= len(ids):
-                    time.sleep(0.0002)
-                    continue
-                code, _, t = self.srv.result_times(ids[i], -1)
-                assert code == 0, f"served request failed with status {code}"
-                times.append(t)
-                i += 1
-            done.set()
+            # Never dies silently: a failed request is recorded with its status, an exception or
+            # the deadline ends the collection, and done is always set, so the submitter cannot
+            # wait forever.
+            try:
+                while not (submitted.is_set() and collected[0] >= len(ids)):
+                    if collected[0] >= len(ids):
+                        time.sleep(0.0002)
+                        continue
+                    left_ms = int(np.ceil((deadline - time.perf_counter()) * 1e3))
+                    code, _, t = self.srv.result_times(ids[collected[0]], max(1, left_ms))
+                    collected[0] += 1
+                    if code == 0:
+                        times.append(t)
+                        continue
+                    failed.append(f"status {code}")
+                    if time.perf_counter() >= deadline:
+                        break
+            except Exception as e:  # noqa: BLE001 -- counted and reported below
+                failed.append(repr(e))
+            finally:
+                done.set()
 
         th = threading.Thread(target=collect, daemon=True)
         th.start()
         start = time.perf_counter()
-        for due, submit in local:
-            now = time.perf_counter() - start
-            if due > now:
-                time.sleep(due - now)
-            lag[0] = max(lag[0], time.perf_counter() - start - due)
-            ids.append(submit())
-        done.wait()
-        th.join()
+        try:
+            for due, submit in local:
+                if done.is_set():
+                    break
+                now = time.perf_counter() - start
+                if due > now:
+                    time.sleep(due - now)
+                lag[0] = max(lag[0], time.perf_counter() - start - due)
+                ids.append(submit())
+        finally:
+            submitted.set()
+            done.wait()
+            th.join()
+        lost = len(local) - len(times)
+        if lost:
+            print(f"serving: {lost} of {len(local)} requests not served, first failure: "
+                  f"{failed[0] if failed else 'not submitted'}", file=sys.stderr)
+        self.failed = getattr(self, "failed", 0) + lost
         return np.array([(t[0], t[2]) for t in times]).reshape(-1, 2), lag[0]
 
     def measure(self, requests=SERVE_REQUESTS, load=SERVE_LOAD, dist=None, rate=None):
@@ -582,6 +605,7 @@ class Serving:
         `rate` requests/s when given (to compare servers at one offered load). With `dist` (one
         rank per GPU, owners placed by the router) capacity is the sum over ranks, the latencies of
         all ranks are pooled and the span is the longest rank's."""
+        self.failed = 0
         self.run(96)  # warm-up: Galois permutations, pools, first key uploads
         sat, _ = self.run(min(400, requests))
         capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6) if len(sat) else 0.0
@@ -595,19 +619,25 @@ class Serving:
         span = (t[:, 1].max() - t[:, 0].min()) * 1e-6 if len(t) else 0.0
         d = {k: st[k] - st0[k] for k in ("batches", "multi_owner_batches", "key_hits", "key_misses",
                                           "key_evictions", "key_upload_bytes", "budget_waits")}
-        peak_dev, key_bytes = st["peak_device_bytes"], self.key_bytes
+        peak_dev, key_bytes, failed = st["peak_device_bytes"], self.key_bytes, self.failed
         if dist:
-            parts = gather_objects(dist, (lat.tolist(), span, lag, d, peak_dev, key_bytes))
+            parts = gather_objects(dist, (lat.tolist(), span, lag, d, peak_dev, key_bytes, failed))
             lat = np.array([x for p in parts for x in p[0]])
             span, lag = max(p[1] for p in parts), max(p[2] for p in parts)
             d = {k: sum(p[3][k] for p in parts) for k in d}
             peak_dev, key_bytes = max(p[4] for p in parts), sum(p[5] for p in parts)
-        return {"requests": requests, "served": int(len(lat)), "owners": self.owners, "params": self.params_text,
-                "mix": self.mix_text,
+            failed = sum(p[6] for p in parts)
+
+        def pct(v):
+            return round(float(np.percentile(lat, v)), 3) if len(lat) else None
+
+        return {"requests": requests, "served": int(len(lat)), "failed": int(failed), "owners": self.owners,
+                "params": self.params_text, "mix": self.mix_text,
                 "capacity_req_s": round(capacity, 2), "offered_req_s": round(rate, 2),
-                "throughput_req_s": round(requests / span, 2),
-                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                "mean_ms": round(float(lat.mean()), 3), "max_submit_lag_ms": round(lag * 1e3, 3),
+                "throughput_req_s": round(len(lat) / span, 2) if span else 0.0,
+                "p50_ms": pct(50), "p99_ms": pct(99),
+                "mean_ms": round(float(lat.mean()), 3) if len(lat) else None,
+                "max_submit_lag_ms": round(lag * 1e3, 3),
                 "hbm_budget_gib": round(self.srv.stats()["hbm_budget"] / 2 ** 30, 2),
                 "key_set_gib": round(key_bytes / 2 ** 30, 2),
                 "peak_device_gib": round(peak_dev / 2 ** 30, 2),
@@ -1508,10 +1538,13 @@ def main():
     single = world == 1
 
     def release():
-        """Drops the batched stream's graph and the torch allocator's cached blocks between
-        sections (untimed), so later sections' own pools find the device memory free."""
+        """Drops the batched stream's graph, the library's cached device memory and the torch
+        allocator's cached blocks between sections (untimed), so later sections' own pools find
+        the device memory free."""
         mix.batch = None
         gc.collect()
+        S.ctx.sync()
+        S.ctx.trim()
         torch.cuda.empty_cache()
 
     boot = None

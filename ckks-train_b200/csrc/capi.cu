@@ -114,6 +114,12 @@ int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n) {
   CKG_API_END
 }
 
+int ckg_ctx_trim(ckg_ctx* ctx) {
+  CKG_API_BEGIN
+  ctx_of(ctx).trim();
+  CKG_API_END
+}
+
 int ckg_host_alloc(uint64_t bytes, void** out) {
   CKG_API_BEGIN
   if (!out) throw Error(CKG_INVALID_PARAMS, "null output");

@@ -94,6 +94,11 @@ void XferCache::trim() {
       ++i;
     }
   }
+  // The frees above are stream-ordered: let them land (unless the stream is being captured)
+  // so that the trim below hands the blocks back to the device.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream->s, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone)
+    cudaStreamSynchronize(stream->s);
   if (pool) cudaMemPoolTrimTo(pool, 0);
 }
 
@@ -114,6 +119,16 @@ void Context::activate() const { CKG_CUDA(cudaSetDevice(device)); }
 
 thread_local LaneBinding tl_lane;
 
+namespace {
+// Two registries under two locks that are never held together: a context's trim takes its
+// auxiliary-lane lock under g_ctx_mu, and creating an auxiliary lane registers it under
+// g_lane_mu while that lock is held.
+std::mutex g_ctx_mu;
+std::vector<Context*> g_ctxs;  // every live context (Context::trim_all)
+std::mutex g_lane_mu;
+std::vector<const Lane*> g_lanes;  // every live lane (their pools are trimmed too)
+}  // namespace
+
 CtxStream::operator cudaStream_t() const {
   return tl_lane.ctx == c_ && tl_lane.lane ? tl_lane.lane->sres->s : c_->sres->s;
 }
@@ -132,9 +147,15 @@ Lane::Lane(int device, int priority) {
   int no = 0;
   CKG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
   CKG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+  std::lock_guard<std::mutex> lk(g_lane_mu);
+  g_lanes.push_back(this);
 }
 
 Lane::~Lane() {
+  {
+    std::lock_guard<std::mutex> lk(g_lane_mu);
+    g_lanes.erase(std::remove(g_lanes.begin(), g_lanes.end(), this), g_lanes.end());
+  }
   if (sres && sres->s) cudaStreamSynchronize(sres->s);
   if (pool) cudaMemPoolDestroy(pool);  // released once its last block is freed
 }
@@ -181,9 +202,7 @@ uint64_t* Context::xfer_block(size_t words, cudaStream_t on) {
   if (e == cudaErrorMemoryAllocation) {  // cached blocks still in flight elsewhere: return the rest
     cudaGetLastError();
     st_alloc_retries++;
-    xcache->trim();
-    cudaMemPool_t def;
-    if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+    trim_all();
     e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
   }
   if (e != cudaSuccess) throw_cuda(e, "transfer block allocation");
@@ -386,6 +405,36 @@ void Context::upload_staged(void* dst, const void* src, size_t bytes) {
   stage_head += need;
 }
 
+void Context::trim() {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != device) cudaSetDevice(device);
+  if (xcache) xcache->trim();
+  if (xpool) cudaMemPoolTrimTo(xpool, 0);
+  {
+    std::lock_guard<std::mutex> lk(aux_mu);
+    for (auto& l : aux_lanes)
+      if (l && l->pool) cudaMemPoolTrimTo(l->pool, 0);
+  }
+  cudaMemPool_t def;
+  if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+  cudaGetLastError();
+  if (cur != device) cudaSetDevice(cur);
+}
+
+void Context::trim_all() {
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    for (Context* c : g_ctxs) c->trim();
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_lane_mu);
+    for (const Lane* l : g_lanes)
+      if (l->pool) cudaMemPoolTrimTo(l->pool, 0);
+  }
+  cudaGetLastError();
+}
+
 Lane& Context::aux_lane(int i) {
   if (i < 0 || i > 1) throw Error(ST_INVALID_PARAMS, "auxiliary lane index out of range");
   std::lock_guard<std::mutex> lk(aux_mu);
@@ -419,17 +468,11 @@ DevBufPtr Context::alloc(size_t words) {
     cudaError_t e = get();
     if (e == cudaErrorMemoryAllocation) {
       // Free memory may sit cached in another pool (each keeps what it frees): hand the unused
-      // blocks of the device's default pool back and try again, then those of the upload pool.
+      // blocks of every context's pools and transfer caches back, then try once more.
       cudaGetLastError();
       st_alloc_retries++;
-      cudaMemPool_t def;
-      if (cudaDeviceGetDefaultMemPool(&def, device) == cudaSuccess) cudaMemPoolTrimTo(def, 0);
+      trim_all();
       e = get();
-      if (e == cudaErrorMemoryAllocation && xcache) {
-        cudaGetLastError();
-        xcache->trim();
-        e = get();
-      }
     }
     if (e != cudaSuccess) throw_cuda(e, "device allocation");
   }
@@ -773,9 +816,15 @@ Context::Context(uint32_t log_n_, const std::vector<uint64_t>& q, const std::vec
       qlinv[l].push_back({v, m.shoup(v)});
     }
   CKG_CUDA(cudaDeviceSynchronize());
+  std::lock_guard<std::mutex> lk(g_ctx_mu);  // last: a constructor that throws registers nothing
+  g_ctxs.push_back(this);
 }
 
 Context::~Context() {
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    g_ctxs.erase(std::remove(g_ctxs.begin(), g_ctxs.end(), this), g_ctxs.end());
+  }
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
   if (xpool) cudaMemPoolDestroy(xpool);  // released once its last block is freed

@@ -228,6 +228,13 @@ struct Context {
   // Not allowed while the stream is being captured (the graph would read a reused slot).
   void upload_staged(void* dst, const void* src, size_t bytes);
 
+  // Hands the device memory this context keeps cached back to the driver: completed transfer
+  // blocks, the unused blocks of the upload pool, of its lanes' pools and of the device's
+  // default pool. trim_all() does it for every live context of the process (an allocation that
+  // runs out of memory calls it before it fails).
+  void trim();
+  static void trim_all();
+
   // Two lanes for work one caller splits over concurrent host threads (the bootstrap's two
   // independent EvalMods), created on first use and kept for the context's life.
   Lane& aux_lane(int i);

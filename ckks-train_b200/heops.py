@@ -200,6 +200,7 @@ def _declare(L):
     L.ckg_pt_upload_overlap.argtypes = [VP, U64P, C.c_uint32, C.c_double, C.POINTER(VP)]
     L.ckg_ct_download_overlap.argtypes = [VP, VP]
     L.ckg_ctx_transfer_stats.argtypes = [VP, C.POINTER(C.c_uint64), C.c_uint32]
+    L.ckg_ctx_trim.argtypes = [VP]
     L.ckg_host_alloc.argtypes = [C.c_uint64, C.POINTER(VP)]
     L.ckg_host_free.argtypes = [VP]
     L.ckg_host_free.restype = None
@@ -324,6 +325,10 @@ class Context:
 
     TRANSFER_STATS = ("upload_calls", "upload_bytes", "upload_alloc_ns", "upload_copy_ns", "upload_pool_bytes",
                       "download_calls", "download_ns", "alloc_retries")
+
+    def trim(self):
+        """Hands the device memory this context keeps cached back to the driver (ckg_ctx_trim)."""
+        _check(lib().ckg_ctx_trim(self.h))
 
     def transfer_stats(self):
         """Host-side accounting of the overlapped transfers (include/ckg.h, ckg_ctx_transfer_stats)."""

@@ -199,6 +199,11 @@ CKG_API int ckg_ctx_join_transfers(ckg_ctx* ctx);
  * bytes the upload pool holds now, download calls, host ns queueing downloads, and device
  * allocations retried after handing cached pool memory back. */
 CKG_API int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n);
+/* Hands the device memory the context keeps cached back to the driver: completed transfer
+ * blocks and the unused blocks of its pools and of the device's default pool (nothing in use
+ * is touched). A device allocation that runs out of memory does this for every context of the
+ * process before it fails. */
+CKG_API int ckg_ctx_trim(ckg_ctx* ctx);
 /* Pinned host memory for the overlapped transfers, allocated by the library's own CUDA runtime
  * (portable: pinned for every context). Free it only when no queued copy still uses it. */
 CKG_API int ckg_host_alloc(uint64_t bytes, void** out);
