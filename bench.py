@@ -741,6 +741,17 @@ class BootServing(Serving):
         out["lanes"] = self.lanes
         return out
 
+    def close(self):
+        """Closes the server and drops every device object of this run's own context (its keys
+        cache, inputs, matrix and the context itself), so the device memory is free for the next."""
+        self.srv.close()
+        self.srv = self.level0 = self.inputs = self.diag = self.ev = None
+        ctx, self.ctx = self.ctx, None
+        ctx.sync()
+        ctx.trim()
+        del ctx
+        gc.collect()
+
     @staticmethod
     def owner_bytes():
         """Pinned host bytes of one owner's keys: 38 switching keys at 32 + 4 limbs, dnum 8,
@@ -1546,6 +1557,8 @@ def main():
         S.ctx.sync()
         S.ctx.trim()
         torch.cuda.empty_cache()
+        free, total = torch.cuda.mem_get_info(local)
+        print(f"release: {free / 2 ** 30:.1f} of {total / 2 ** 30:.1f} GiB free", file=sys.stderr)
 
     boot = None
     if not args.no_boot and single:
@@ -1566,18 +1579,22 @@ def main():
     serving = serving_spill = serving_boot_spill = serving_one_lane = None
     if not args.no_serve and single:
         release()
+        # each server is closed and its context released before the next one fills the device
         sv = BootServing(ckg, torch, local, boot_lanes=0)
         serving_one_lane = sv.measure(args.serve_requests)
         sv.close()
         del sv
+        release()
         sv = BootServing(ckg, torch, local)  # two lanes, at the one-lane run's offered load
         serving = sv.measure(args.serve_requests, rate=serving_one_lane["offered_req_s"])
         sv.close()
         del sv
+        release()
         sv = BootServing(ckg, torch, local, owners=BootServing.spill_owners(), budget=SERVE_BOOT_SPILL_BUDGET)
         serving_boot_spill = sv.measure(SERVE_BOOT_SPILL_REQUESTS)
         sv.close()
         del sv
+        release()
         sv = Serving(S, owners=args.serve_owners)
         serving_spill = sv.measure(args.serve_requests)
         sv.close()
