@@ -1327,6 +1327,7 @@ def cpu_crosscheck(threads):
 
 
 def main():
+    t_start = time.time()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -1558,7 +1559,8 @@ def main():
         S.ctx.trim()
         torch.cuda.empty_cache()
         free, total = torch.cuda.mem_get_info(local)
-        print(f"release: {free / 2 ** 30:.1f} of {total / 2 ** 30:.1f} GiB free", file=sys.stderr)
+        print(f"release at {time.time() - t_start:.0f} s: {free / 2 ** 30:.1f} of {total / 2 ** 30:.1f} GiB free",
+              file=sys.stderr)
 
     boot = None
     if not args.no_boot and single:
