@@ -748,7 +748,6 @@ class BootServing(Serving):
         self.srv = self.level0 = self.inputs = self.diag = self.ev = None
         ctx, self.ctx = self.ctx, None
         ctx.sync()
-        ctx.trim()
         del ctx
         gc.collect()
 
@@ -1550,13 +1549,11 @@ def main():
     single = world == 1
 
     def release():
-        """Drops the batched stream's graph, the library's cached device memory and the torch
-        allocator's cached blocks between sections (untimed), so later sections' own pools find
-        the device memory free."""
+        """Drops the batched stream's graph and the torch allocator's cached blocks between
+        sections (untimed), so later sections' own pools find the device memory free."""
         mix.batch = None
         gc.collect()
         S.ctx.sync()
-        S.ctx.trim()
         torch.cuda.empty_cache()
         free, total = torch.cuda.mem_get_info(local)
         print(f"release at {time.time() - t_start:.0f} s: {free / 2 ** 30:.1f} of {total / 2 ** 30:.1f} GiB free",

@@ -498,6 +498,7 @@ void Server::worker() {
         if (hk->dev.use_count() != 1) continue;  // a batch on the device still reads it
         it = lru_.erase(it);
         hk->dev.reset();  // stream-ordered free on the copy stream
+        hk->ready.reset();
         st_.key_evictions++;
       }
       if (used() + extra + r->work_bytes > cfg_.hbm_budget) {
@@ -535,10 +536,13 @@ void Server::worker() {
       continue;
     }
     std::vector<HostKey*> to_upload;
+    std::vector<std::shared_ptr<CUevent_st>> hit_ready;  // copies of resident keys, maybe in flight
     for (HostKey* hk : need) {
       if (hk->dev) {
         st_.key_hits++;
         lru_.splice(lru_.begin(), lru_, hk->lru);
+        if (hk->ready && std::find(hit_ready.begin(), hit_ready.end(), hk->ready) == hit_ready.end())
+          hit_ready.push_back(hk->ready);
       } else {
         st_.key_misses++;
         to_upload.push_back(hk);
@@ -560,6 +564,7 @@ void Server::worker() {
     f->rehome = ln != nullptr;
     std::map<HostKey*, std::pair<int, std::string>> failed;
     std::map<HostKey*, KeyPtr> fresh;
+    std::shared_ptr<CUevent_st> copied_ev;
     try {
       ctx_->activate();
       if (ln) {  // the lane runs after the client's work queued on the context's stream so far
@@ -569,6 +574,8 @@ void Server::worker() {
         cudaStreamWaitEvent(ln->sres->s, ready, 0);
         cudaEventDestroy(ready);
       }
+      // resident keys whose copy another flight issued (possibly on another lane)
+      for (auto& e : hit_ready) CKG_CUDA(cudaStreamWaitEvent(ctx_->stream, e.get(), 0));
       for (HostKey* hk : to_upload) {
         try {
           fresh[hk] = upload(hk);
@@ -579,9 +586,9 @@ void Server::worker() {
       if (!fresh.empty()) {  // the compute stream waits for the key copies
         cudaEvent_t copied;
         CKG_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
-        cudaEventRecord(copied, copy_->s);
-        cudaStreamWaitEvent(ctx_->stream, copied, 0);
-        cudaEventDestroy(copied);
+        copied_ev.reset(copied, [](cudaEvent_t e) { cudaEventDestroy(e); });
+        CKG_CUDA(cudaEventRecord(copied, copy_->s));
+        CKG_CUDA(cudaStreamWaitEvent(ctx_->stream, copied, 0));
       }
     } catch (const std::exception& e) {
       for (HostKey* hk : to_upload)
@@ -592,6 +599,7 @@ void Server::worker() {
       std::lock_guard<std::mutex> g(mu_);
       for (auto& kv : fresh) {
         kv.first->dev = kv.second;
+        kv.first->ready = copied_ev;
         lru_.push_front(kv.first);
         kv.first->lru = lru_.begin();
         st_.key_upload_bytes += kv.first->words * 8;

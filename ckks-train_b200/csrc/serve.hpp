@@ -97,6 +97,9 @@ class Server {
     uint64_t elt = 0;
     int role = 0;  // 0 relinearization, 1 Galois, 2 SSE to_sparse, 3 SSE to_dense
     KeyPtr dev;  // the cache's reference to the device copy
+    // Completes when the copy that made `dev` has landed: a flight on another lane than the
+    // one whose upload made it waits for this before its first read.
+    std::shared_ptr<CUevent_st> ready;
     std::list<HostKey*>::iterator lru;
     ~HostKey();
   };
