@@ -45,17 +45,32 @@ DevBuf::~DevBuf() {
   if (cur != device) cudaSetDevice(cur);
 }
 
-uint64_t* XferCache::take(size_t words) {
+uint64_t* XferCache::take(size_t words, cudaStream_t on) {
   std::lock_guard<std::mutex> lk(mu);
+  auto fits = [&](const Block& b) { return b.words >= words && b.words <= words + words / 4; };
+  // the smallest fitting block whose last use has completed
   int best = -1;
   for (int i = 0; i < (int)blocks.size(); ++i) {
     const Block& b = blocks[i];
-    if (b.words < words || b.words > words + words / 4) continue;
-    if (best >= 0 && b.words >= blocks[best].words) continue;
+    if (!fits(b) || (best >= 0 && b.words >= blocks[best].words)) continue;
     if (cudaEventQuery(b.done) != cudaSuccess) continue;
     best = i;
   }
-  if (best < 0) return nullptr;
+  if (best < 0) {
+    // else the oldest fitting block still in use, which `on` waits for (stream-ordered reuse):
+    // a new block would cost a fresh mapping of device memory on the host's critical path,
+    // while the wait costs only the rest of a copy the device is already running
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(on, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (int i = 0; i < (int)blocks.size() && best < 0; ++i)
+      if (fits(blocks[i]) && cudaStreamWaitEvent(on, blocks[i].done, 0) == cudaSuccess) best = i;
+    cudaGetLastError();
+    if (best < 0) return nullptr;
+    waited++;
+  }
   uint64_t* p = blocks[best].p;
   cudaEventDestroy(blocks[best].done);
   blocks.erase(blocks.begin() + best);
@@ -196,7 +211,7 @@ void Context::transfer_streams() {
 
 uint64_t* Context::xfer_block(size_t words, cudaStream_t on) {
   transfer_streams();
-  if (uint64_t* p = xcache->take(words)) return p;  // its last use has completed: any stream may take it
+  if (uint64_t* p = xcache->take(words, on)) return p;  // free, or `on` waits for its last use
   uint64_t* p = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
   if (e == cudaErrorMemoryAllocation) {  // cached blocks still in flight elsewhere: return the rest

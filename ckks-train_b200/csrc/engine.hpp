@@ -76,7 +76,10 @@ struct XferCache {
   int device = 0;
   cudaMemPool_t pool = nullptr;  // where new blocks come from and trimmed ones go back
   StreamPtr stream;               // the upload stream (allocations and trims)
-  uint64_t* take(size_t words);  // a completed block of words..5/4 words, or null
+  // A block of words..5/4 words: a completed one, else the oldest still in use with `on` made
+  // to wait for its last use; null when none fits.
+  uint64_t* take(size_t words, cudaStream_t on);
+  uint64_t waited = 0;  // blocks handed out still in use
   void give(uint64_t* p, size_t words, cudaEvent_t done);  // takes ownership of `done`
   void trim();  // completed blocks back to the pool
   ~XferCache();

@@ -324,7 +324,7 @@ class Context:
         _check(lib().ckg_ctx_sync(self.h))
 
     TRANSFER_STATS = ("upload_calls", "upload_bytes", "upload_alloc_ns", "upload_copy_ns", "upload_pool_bytes",
-                      "download_calls", "download_ns", "alloc_retries")
+                      "download_calls", "download_ns", "alloc_retries", "reused_in_use")
 
     def trim(self):
         """Hands the device memory this context keeps cached back to the driver (ckg_ctx_trim)."""
@@ -332,8 +332,8 @@ class Context:
 
     def transfer_stats(self):
         """Host-side accounting of the overlapped transfers (include/ckg.h, ckg_ctx_transfer_stats)."""
-        out = (C.c_uint64 * 8)()
-        _check(lib().ckg_ctx_transfer_stats(self.h, out, 8))
+        out = (C.c_uint64 * len(self.TRANSFER_STATS))()
+        _check(lib().ckg_ctx_transfer_stats(self.h, out, len(self.TRANSFER_STATS)))
         return dict(zip(self.TRANSFER_STATS, [int(x) for x in out]))
 
     def join_transfers(self):

@@ -194,10 +194,11 @@ CKG_API int ckg_ct_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t n
 CKG_API int ckg_pt_upload_overlap(ckg_eval* ev, const uint64_t* host, uint32_t level, double scale, ckg_pt** out);
 CKG_API int ckg_ct_download_overlap(const ckg_ct* ct, uint64_t* host);
 CKG_API int ckg_ctx_join_transfers(ckg_ctx* ctx);
-/* Host-side accounting since the context was created, up to 8 words in this order: upload calls,
+/* Host-side accounting since the context was created, up to 9 words in this order: upload calls,
  * bytes uploaded, host ns in the upload pool's allocations, host ns queueing the upload copies,
- * bytes the upload pool holds now, download calls, host ns queueing downloads, and device
- * allocations retried after handing cached pool memory back. */
+ * bytes the upload pool holds now, download calls, host ns queueing downloads, device
+ * allocations retried after handing cached pool memory back, and transfer blocks reused while
+ * still in use (the new transfer waits on the device for the block's last use). */
 CKG_API int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n);
 /* Hands the device memory the context keeps cached back to the driver: completed transfer
  * blocks and the unused blocks of its pools and of the device's default pool (nothing in use
