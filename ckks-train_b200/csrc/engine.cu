@@ -57,9 +57,13 @@ uint64_t* XferCache::take(size_t words, cudaStream_t on) {
     best = i;
   }
   if (best < 0) {
-    // else the oldest fitting block still in use, which `on` waits for (stream-ordered reuse):
-    // a new block would cost a fresh mapping of device memory on the host's critical path,
-    // while the wait costs only the rest of a copy the device is already running
+    // Else, once kReuseDepth fitting blocks are in use (enough for the transfers of one step to
+    // overlap the compute and copies of the steps before it), the oldest of them, which `on`
+    // waits for (stream-ordered reuse): a further block would cost a fresh mapping of device
+    // memory on the host's critical path, the wait only the rest of work the device is running.
+    int in_use = 0;
+    for (const Block& b : blocks) in_use += fits(b);
+    if (in_use < kReuseDepth) return nullptr;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(on, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
       cudaGetLastError();

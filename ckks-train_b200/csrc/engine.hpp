@@ -70,14 +70,15 @@ struct XferCache {
     cudaEvent_t done;
   };
   static constexpr size_t kMaxBlocks = 16;
+  static constexpr int kReuseDepth = 2;  // fitting blocks in use before one is reused in use
   std::mutex mu;
   std::vector<Block> blocks;  // oldest first
   size_t max_bytes = 0;       // kept at most (a third of the device's memory)
   int device = 0;
   cudaMemPool_t pool = nullptr;  // where new blocks come from and trimmed ones go back
   StreamPtr stream;               // the upload stream (allocations and trims)
-  // A block of words..5/4 words: a completed one, else the oldest still in use with `on` made
-  // to wait for its last use; null when none fits.
+  // A block of words..5/4 words: a completed one, else (when kReuseDepth fitting blocks are in
+  // use) the oldest of them with `on` made to wait for its last use; null otherwise.
   uint64_t* take(size_t words, cudaStream_t on);
   uint64_t waited = 0;  // blocks handed out still in use
   void give(uint64_t* p, size_t words, cudaEvent_t done);  // takes ownership of `done`
