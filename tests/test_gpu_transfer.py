@@ -137,3 +137,33 @@ def test_pinned_buffer_round_trip(env):
     assert np.array_equal(buf_out.array(np.uint64, a_in.shape), a_in)
     with pytest.raises(ckg.InvalidParams):
         buf_in.array(np.uint64, (4,) + ins[0].shape)
+
+
+def test_pipelined_steps_reuse_blocks_safely(env):
+    """Six steps queued back to back with no host wait, each with its own inputs and its own
+    host outputs: transfer blocks come back to the cache while the device still reads or copies
+    them, and a block handed out again (completed, or still in use behind a device-side wait)
+    never lets a later step's upload or pack overwrite an earlier step's data early."""
+    ckg, P, gpu, cpu = env.ckg, env.P, env.gpu, env.cpu
+    L = P.max_level
+    steps = 6
+    ins = [[random_ct(P, 100 + 4 * s + i, L) for i in range(4)] for s in range(steps)]
+    host_in = [[_pinned(a) for a in step] for step in ins]
+    outs_host = [[_empty_pinned((2, L, P.n)) for _ in range(2)] for _ in range(steps)]
+    before = env.ctx.transfer_stats()
+    for s in range(steps):
+        g = gpu.upload_ct_overlap_list([(h.data_ptr(), 2, L, env.scale) for h in host_in[s]])
+        b = ckg.Batch(gpu)
+        res = [b.mul_relin_rescale(g[0], g[1]), b.mul_relin_rescale(g[2], g[3])]
+        b.run()
+        gpu.download_ct_overlap_list(res, [h.data_ptr() for h in outs_host[s]])
+        del res, g, b
+    env.ctx.join_transfers()
+    env.ctx.sync()
+    after = env.ctx.transfer_stats()
+    assert after["upload_calls"] - before["upload_calls"] == steps
+    for s in range(steps):
+        c = [cpu.ct(a, env.scale) for a in ins[s]]
+        for k in range(2):
+            w = cpu.rescale(cpu.mul(c[2 * k], c[2 * k + 1]))
+            assert_same(outs_host[s][k].numpy().view(np.uint64), w.data(), f"step {s} result {k}")
