@@ -110,7 +110,7 @@ int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n) {
   }
   const uint64_t w[9] = {c.st_upload_calls, c.st_upload_bytes,   c.st_upload_alloc_ns, c.st_upload_copy_ns,
                          reserved,          c.st_download_calls, c.st_download_ns,      c.st_alloc_retries,
-                         c.xcache ? c.xcache->waited : 0};
+                         c.xcache ? c.xcache->waited.load() : 0};
   for (uint32_t i = 0; i < n && i < 9; ++i) out[i] = w[i];
   CKG_API_END
 }

@@ -80,7 +80,7 @@ struct XferCache {
   // A block of words..5/4 words: a completed one, else (when kReuseDepth fitting blocks are in
   // use) the oldest of them with `on` made to wait for its last use; null otherwise.
   uint64_t* take(size_t words, cudaStream_t on);
-  uint64_t waited = 0;  // blocks handed out still in use
+  std::atomic<uint64_t> waited{0};  // blocks handed out still in use
   void give(uint64_t* p, size_t words, cudaEvent_t done);  // takes ownership of `done`
   void trim();  // completed blocks back to the pool
   ~XferCache();
