@@ -1506,7 +1506,8 @@ def main():
         torch.cuda.empty_cache()
         mix.prepare_e2e()
         steps_e = max(8, args.steps)
-        mix.step_e2e()
+        for _ in range(max(3, args.warmup)):  # warm-up: the transfer blocks reach their working set
+            mix.step_e2e()
         mix.inflight.clear()
         mix.host_s, mix.host_parts = 0.0, {}
         ts0 = S.ctx.transfer_stats()
