@@ -295,6 +295,24 @@ class Mix:
     def __init__(self, S, ops, keep_host=True):
         self.S, self.ops = S, ops
         self.inputs = []  # (kind, a, b_or_pt, steps)
+        torch, n = S.torch, S.n
+        # With keep_host, the inputs' host copies for the e2e step, each list in one pinned
+        # allocation laid out in list order (a client's request buffer: ciphertexts a, b of each
+        # op in op order; plaintexts in op order), filled straight from the device: no second
+        # host copy, so N ranks on one host hold one copy of their inputs each.
+        ct_words = sum(2 * (lv + 1) * n * (2 if kind == "mul" else 1) for kind, lv, _ in ops)
+        pt_words = sum((lv + 1) * n for kind, lv, _ in ops if kind == "pmul")
+        self.host_ct_flat = torch.empty(ct_words, dtype=torch.int64, pin_memory=True) if keep_host else None
+        self.host_pt_flat = (torch.empty(pt_words, dtype=torch.int64, pin_memory=True)
+                             if keep_host and pt_words else None)
+        offs = [0, 0]
+
+        def keep(t, flat, i):
+            v = flat[offs[i]:offs[i] + t.numel()].view(t.shape)
+            v.copy_(t)
+            offs[i] += t.numel()
+            return v
+
         host = []
         for kind, level, steps in ops:
             a, ta = S.ct(level)
@@ -306,7 +324,10 @@ class Mix:
                 extra, tb = None, None
             self.inputs.append((kind, a, extra, steps))
             if keep_host:
-                host.append((ta.cpu().pin_memory(), None if tb is None else tb.cpu().pin_memory()))
+                ha = keep(ta, self.host_ct_flat, 0)
+                hb = None if tb is None else keep(tb, self.host_ct_flat, 0) if kind == "mul" else keep(
+                    tb, self.host_pt_flat, 1)
+                host.append((ha, hb))
             del ta, tb
         self.host = host
         self.chunk_items = None
@@ -343,36 +364,10 @@ class Mix:
         self.batch.launch_graph()
 
     def prepare_e2e(self):
-        """Host buffers of the e2e step: inputs and results each in one pinned allocation, laid out
-        in list order (a client's request and reply buffers), so the list transfers move each run
-        of adjacent buffers with one copy."""
+        """Result buffers of the e2e step: one pinned allocation laid out in list order (a client's
+        reply buffer), so the list download moves the whole run with one copy. The inputs were
+        packed the same way when the stream was built."""
         torch, n = self.S.torch, self.S.n
-
-        def packed(tensors):
-            flat = torch.empty(sum(t.numel() for t in tensors), dtype=torch.int64, pin_memory=True)
-            views, off = [], 0
-            for t in tensors:
-                v = flat[off:off + t.numel()].view(t.shape)
-                v.copy_(t)
-                views.append(v)
-                off += t.numel()
-            return flat, views
-
-        cts = [ha for ha, hb in self.host]
-        cts_order = []
-        for (kind, _, _), (ha, hb) in zip(self.ops, self.host):
-            cts_order.append(ha)
-            if kind == "mul":
-                cts_order.append(hb)
-        pts = [hb for (kind, _, _), (ha, hb) in zip(self.ops, self.host) if kind == "pmul"]
-        self.host_ct_flat, ct_views = packed(cts_order)
-        self.host_pt_flat, pt_views = packed(pts) if pts else (None, [])
-        ct_it, pt_it, host = iter(ct_views), iter(pt_views), []
-        for kind, _, _ in self.ops:
-            a = next(ct_it)
-            host.append((a, next(ct_it) if kind == "mul" else (next(pt_it) if kind == "pmul" else None)))
-        self.host = host
-        del cts, cts_order, pts
         shapes = [(2, (level if kind == "rot" else level - 1) + 1, n) for kind, level, _ in self.ops]
         self.out_flat = torch.empty(sum(int(np.prod(sh)) for sh in shapes), dtype=torch.int64, pin_memory=True)
         self.out_host, off = [], 0
