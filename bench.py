@@ -601,6 +601,7 @@ class Serving:
         rank per GPU, owners placed by the router) capacity is the sum over ranks, the latencies of
         all ranks are pooled and the span is the longest rank's."""
         self.failed = 0
+        retries0 = self.alloc_retries()
         self.run(96)  # warm-up: Galois permutations, pools, first key uploads
         sat, _ = self.run(min(400, requests))
         capacity = len(sat) / ((sat[:, 1].max() - sat[:, 0].min()) * 1e-6) if len(sat) else 0.0
@@ -615,6 +616,8 @@ class Serving:
         d = {k: st[k] - st0[k] for k in ("batches", "multi_owner_batches", "key_hits", "key_misses",
                                           "key_evictions", "key_upload_bytes", "budget_waits")}
         peak_dev, key_bytes, failed = st["peak_device_bytes"], self.key_bytes, self.failed
+        retries = self.alloc_retries()
+        retries = None if retries is None or retries0 is None else retries - retries0
         if dist:
             parts = gather_objects(dist, (lat.tolist(), span, lag, d, peak_dev, key_bytes, failed))
             lat = np.array([x for p in parts for x in p[0]])
@@ -640,7 +643,17 @@ class Serving:
                 "key_upload_gib": round(d["key_upload_bytes"] / 2 ** 30, 2),
                 "batches": d["batches"], "multi_owner_batches": d["multi_owner_batches"],
                 "key_evictions": d["key_evictions"], "budget_waits": d["budget_waits"],
-                "register_s": round(self.register_s, 1)}
+                "register_s": round(self.register_s, 1),
+                "alloc_retries": retries}
+
+    def alloc_retries(self):
+        """Device allocations of the serving context retried after out-of-memory (each hands
+        every pool's cached memory back first): nonzero means the run was memory-bound."""
+        try:
+            ctx = getattr(self, "ctx", None) or self.S.ctx
+            return ctx.transfer_stats()["alloc_retries"]
+        except Exception:  # noqa: BLE001 -- a stand-in server in the CPU tests has no context
+            return None
 
     def close(self):
         self.srv.close()
