@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "batch.hpp"
+#include "bounds_refs.hpp"
 
 namespace ckg {
 
@@ -353,6 +354,19 @@ void Batch::build() {
       }
       if (it.kind == MUL)
         for (int cc = 0; cc < 2; ++cc) rescale_poly(relin + cc * (l + 1) * N, l, it.out->comp_mut(cc));
+    }
+    if (bounds::enabled()) {  // every entry's buffers, before the lists reach the device
+      bounds::refs(tensor.data(), tensor.size(), N, "batch tensor product");
+      bounds::refs(pmul.data(), pmul.size(), N, "batch plaintext product");
+      bounds::refs(gather.data(), gather.size(), N, "batch Galois gather");
+      for (auto* v : {&intt_in, &fwd_conv, &intt_p, &fwd_md, &intt_last, &fwd_rs})
+        bounds::refs(v->data(), v->size(), N, "batch NTT limb");
+      for (int ns = 1; ns <= kMaxSrc; ++ns) bounds::refs(modup[ns].data(), modup[ns].size(), ns, N, "batch ModUp");
+      bounds::refs(md_conv.data(), md_conv.size(), (int)k, N, "batch ModDown");
+      bounds::refs(rs_conv.data(), rs_conv.size(), 1, N, "batch rescale lift");
+      bounds::refs(ip.data(), ip.size(), (int)c.alpha, (int)k, N, "batch inner product");
+      bounds::refs(fin_ks.data(), fin_ks.size(), N, "batch key-switch finish");
+      bounds::refs(fin_rs.data(), fin_rs.size(), N, "batch rescale finish");
     }
     S.tensor = db.put(tensor);
     S.pmul = db.put(pmul);

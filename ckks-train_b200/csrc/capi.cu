@@ -6,6 +6,7 @@
 
 #include "../../include/ckg.h"
 #include "bootsetup.hpp"
+#include "bounds.hpp"
 #include "handles.hpp"
 #include "seal.hpp"
 
@@ -112,6 +113,19 @@ int ckg_ctx_transfer_stats(ckg_ctx* ctx, uint64_t* out, uint32_t n) {
                          reserved,          c.st_download_calls, c.st_download_ns,      c.st_alloc_retries,
                          c.xcache ? c.xcache->waited.load() : 0};
   for (uint32_t i = 0; i < n && i < 9; ++i) out[i] = w[i];
+  CKG_API_END
+}
+
+int ckg_debug_bounds(int op, uint64_t p, uint64_t bytes) {
+  CKG_API_BEGIN
+  const void* a = reinterpret_cast<const void*>((uintptr_t)p);
+  switch (op) {
+    case 0: bounds::set_enabled(bytes != 0); break;
+    case 1: bounds::track(a, bytes); break;
+    case 2: bounds::untrack(a); break;
+    case 3: bounds::check(a, bytes, "checked range"); break;
+    default: throw Error(CKG_INVALID_PARAMS, "unknown bounds operation");
+  }
   CKG_API_END
 }
 

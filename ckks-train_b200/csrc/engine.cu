@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "engine.hpp"
+#include "bounds.hpp"
 
 namespace ckg {
 
@@ -26,6 +27,7 @@ StreamRes::~StreamRes() {
 
 DevBuf::~DevBuf() {
   if (!p) return;
+  bounds::untrack(p);
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != device) cudaSetDevice(device);
@@ -215,7 +217,10 @@ void Context::transfer_streams() {
 
 uint64_t* Context::xfer_block(size_t words, cudaStream_t on) {
   transfer_streams();
-  if (uint64_t* p = xcache->take(words, on)) return p;  // free, or `on` waits for its last use
+  if (uint64_t* p = xcache->take(words, on)) {  // free, or `on` waits for its last use
+    bounds::track(p, words * 8);
+    return p;
+  }
   uint64_t* p = nullptr;
   cudaError_t e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
   if (e == cudaErrorMemoryAllocation) {  // cached blocks still in flight elsewhere: return the rest
@@ -225,6 +230,7 @@ uint64_t* Context::xfer_block(size_t words, cudaStream_t on) {
     e = cudaMallocFromPoolAsync((void**)&p, words * 8, xpool, on);
   }
   if (e != cudaSuccess) throw_cuda(e, "transfer block allocation");
+  bounds::track(p, words * 8);
   return p;
 }
 
@@ -377,6 +383,7 @@ void Context::download_overlapped_list(const std::vector<DevPart>& parts) {
   cudaEvent_t copied;
   CKG_CUDA(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
   CKG_CUDA(cudaEventRecord(copied, xfer_out->s));
+  bounds::untrack(stage);
   xcache->give(stage, total, copied);  // reused once the copies are done
   st_download_calls++;
   st_download_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
@@ -494,6 +501,7 @@ DevBufPtr Context::alloc(size_t words) {
       e = get();
     }
     if (e != cudaSuccess) throw_cuda(e, "device allocation");
+    bounds::track(b->p, words * 8);
   }
   return b;
 }

@@ -18,6 +18,7 @@
 
 #include "kernels.cuh"
 #include "launch.hpp"
+#include "bounds_refs.hpp"
 
 namespace ckg {
 
@@ -1537,6 +1538,7 @@ void bconv_launch(const DevTables& d, const B& cb, int count, int n_src, cudaStr
 std::atomic<uint64_t> g_launches{0};
 
 void launch_ntt(const DevTables& d, const LimbRef* refs, int count, bool inverse, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "NTT limb");
   LimbBatch b;
   for (int off = 0; off < count; off += kMaxLimbs) {
     b.count = count - off < kMaxLimbs ? count - off : kMaxLimbs;
@@ -1557,6 +1559,11 @@ void launch_ntt_ptr(const DevTables& d, const LimbRef* dev_refs, int count, bool
 }
 
 void launch_bconv(const DevTables& d, const ConvJob* jobs, int count, int n_src, int n_dst, cudaStream_t st) {
+  if (bounds::enabled()) {
+    std::vector<ConvJob> chk(jobs, jobs + count);
+    for (ConvJob& j : chk) j.n_dst = n_dst;
+    bounds::refs(chk.data(), chk.size(), n_src, (size_t)1 << d.log_n, "base conversion");
+  }
   ConvBatch cb;
   cb.n_src = n_src;
   cb.n_dst = n_dst;
@@ -1578,6 +1585,7 @@ void launch_bconv_ptr(const DevTables& d, const ConvJob* dev_jobs, int count, in
 }
 
 void launch_inner_product(const DevTables& d, int alpha, int L, int k, const IpJob* jobs, int count, cudaStream_t st) {
+  bounds::refs(jobs, count, alpha, k, (size_t)1 << d.log_n, "inner product");
   IpBatch ib;
   ib.alpha = alpha;
   ib.L = L;
@@ -1605,6 +1613,8 @@ void launch_inner_product_ptr(const DevTables& d, int alpha, int L, int k, const
 }
 
 void launch_ntt_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st, const LimbRef* cols) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "NTT + finish");
+  if (cols) bounds::refs(cols, count, (size_t)1 << d.log_n, "NTT + finish column pass");
   if (cols && d.log_n <= 11) throw std::logic_error("launch_ntt_finish: explicit column passes need N >= 2^12");
   if (d.log_n <= 11) {  // small transforms: separate NTT and finish
     std::vector<LimbRef> lr(count);
@@ -1649,6 +1659,7 @@ void launch_ntt_finish_ptr(const DevTables& d, const LimbRef* dev_cols, const Fi
 }
 
 void launch_finish(const DevTables& d, const FinRef* refs, int count, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "finish");
   FinBatch fb;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxFin) {
@@ -1667,6 +1678,7 @@ void launch_finish_ptr(const DevTables& d, const FinRef* dev_refs, int count, cu
 }
 
 void launch_binary(const DevTables& d, const BinRef* refs, int count, int op, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "element-wise op");
   BinBatch bb;
   bb.op = op;
   const int n = 1 << d.log_n;
@@ -1687,6 +1699,8 @@ void launch_binary_ptr(const DevTables& d, const BinRef* dev_refs, int count, in
 
 void launch_unary(const DevTables& d, const LimbRef* refs, int count, int op, const uint64_t* consts,
                   const uint32_t* perm, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "unary op");
+  bounds::perm(perm, (size_t)1 << d.log_n, "unary op permutation");
   LimbBatch b;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxLimbs) {
@@ -1713,6 +1727,7 @@ void launch_gather_ptr(const DevTables& d, const GatherRef* dev_refs, int count,
 }
 
 void launch_tensor(const DevTables& d, const TensorRef* refs, int count, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "tensor product");
   TensorBatch tb;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxTensor) {
@@ -1732,6 +1747,7 @@ void launch_tensor_ptr(const DevTables& d, const TensorRef* dev_refs, int count,
 
 void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const ScalarTable& table, cudaStream_t st,
                    int mode) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "scalar op");
   LimbBatch b;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxLimbs) {
@@ -1744,17 +1760,35 @@ void launch_scalar(const DevTables& d, const LimbRef* refs, int count, const Sca
 
 void launch_mac_plain(const DevTables& d, const MacBatch& b, cudaStream_t st) {
   const int n = 1 << d.log_n;
+  if (bounds::enabled()) {
+    const size_t w = (size_t)b.limbs * n;
+    bounds::limb(b.out0, w, "plaintext MAC");
+    bounds::limb(b.out1, w, "plaintext MAC");
+    for (int t = 0; t < b.count; ++t) {
+      bounds::limb(b.x0[t], w, "plaintext MAC");
+      bounds::limb(b.x1[t], w, "plaintext MAC");
+      bounds::limb(b.w[t], w, "plaintext MAC");
+    }
+  }
   k_mac_plain<<<dim3((n + 255) / 256, b.limbs), 256, 0, st>>>(b, d.prime, n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_mac_tensor(const DevTables& d, const MacTensorBatch& b, cudaStream_t st) {
   const int n = 1 << d.log_n;
+  if (bounds::enabled()) {
+    const size_t w = (size_t)b.limbs * n;
+    for (const void* o : {(const void*)b.out0, (const void*)b.out1, (const void*)b.out2}) bounds::limb(o, w, "tensor MAC");
+    for (int t = 0; t < b.count; ++t)
+      for (const void* x : {(const void*)b.a0[t], (const void*)b.a1[t], (const void*)b.b0[t], (const void*)b.b1[t]})
+        bounds::limb(x, w, "tensor MAC");
+  }
   k_mac_tensor<<<dim3((n + 255) / 256, b.limbs), 256, 0, st>>>(b, d.prime, n);
   g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
 void launch_lift_level0(const DevTables& d, const LimbRef* refs, int count, cudaStream_t st) {
+  bounds::refs(refs, count, (size_t)1 << d.log_n, "level-0 lift");
   LimbBatch b;
   const int n = 1 << d.log_n;
   for (int off = 0; off < count; off += kMaxLimbs) {

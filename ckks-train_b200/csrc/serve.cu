@@ -7,6 +7,7 @@
 
 #include "bootsetup.hpp"
 #include "serve.hpp"
+#include "bounds.hpp"
 
 namespace ckg {
 
@@ -418,6 +419,7 @@ KeyPtr Server::upload(HostKey* hk) {
   buf->device = ctx_->device;
   buf->words = hk->words;
   CKG_CUDA(cudaMallocAsync((void**)&buf->p, hk->words * 8, copy_->s));
+  bounds::track(buf->p, hk->words * 8);
   CKG_CUDA(cudaMemcpyAsync(buf->p, hk->host, hk->words * 8, cudaMemcpyHostToDevice, copy_->s));
   auto counter = key_bytes_;
   *counter += bytes;

@@ -201,6 +201,7 @@ def _declare(L):
     L.ckg_ct_download_overlap.argtypes = [VP, VP]
     L.ckg_ctx_transfer_stats.argtypes = [VP, C.POINTER(C.c_uint64), C.c_uint32]
     L.ckg_ctx_trim.argtypes = [VP]
+    L.ckg_debug_bounds.argtypes = [C.c_int, C.c_uint64, C.c_uint64]
     L.ckg_host_alloc.argtypes = [C.c_uint64, C.POINTER(VP)]
     L.ckg_host_free.argtypes = [VP]
     L.ckg_host_free.restype = None

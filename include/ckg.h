@@ -494,6 +494,16 @@ CKG_API int ckg_server_owner_counter(const ckg_server* s, uint32_t owner, uint64
 /* Test hook: the next `count` key uploads fail as an allocation failure would. */
 CKG_API int ckg_server_inject_upload_failures(ckg_server* s, uint32_t count);
 
+/* Opt-in bounds checking (CKG_CHECK_BOUNDS=1 in the environment): before each launch, and before
+ * a batch uploads its work lists, every buffer a kernel will touch is checked on the host against
+ * the device allocations the library made: a range that starts in a live allocation must end in
+ * it, and one that starts in recently freed memory is a use after free. A violation fails the call
+ * with CKG_DEVICE and a message naming the buffer; nothing is queued. Buffers the library did not
+ * allocate pass unchecked. Test hook over the registry: op 0 turns checking on (bytes != 0) or off,
+ * 1 records an allocation [p, p + bytes), 2 records the free of the allocation at p, 3 checks
+ * [p, p + bytes). */
+CKG_API int ckg_debug_bounds(int op, uint64_t p, uint64_t bytes);
+
 #ifdef __cplusplus
 }
 #endif
