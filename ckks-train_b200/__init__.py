@@ -45,6 +45,7 @@ from .heops import (  # noqa: F401
     seal_decode,
     seal_encode,
     seal_parms_id,
+    set_bounds_checking,
 )
 from . import nn  # noqa: F401,E402
 from .router import OwnerRouter  # noqa: F401,E402

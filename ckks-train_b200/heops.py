@@ -274,6 +274,13 @@ def launch_count():
     return lib().ckg_launch_count()
 
 
+def set_bounds_checking(on):
+    """Turns the library's host-side bounds checking of kernel work lists on or off (ckg_debug_bounds;
+    the CKG_CHECK_BOUNDS environment variable sets the initial state). Only allocations made while
+    it is on are known to it."""
+    _check(lib().ckg_debug_bounds(0, 0, 1 if on else 0))
+
+
 def primes_for_bits(log_n, q_bits, p_bits):
     """The data and special primes CkksParams::new hands out (params.rs:87-157)."""
     qb = (C.c_uint32 * len(q_bits))(*q_bits)

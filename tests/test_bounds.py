@@ -46,3 +46,13 @@ def test_off_checks_nothing(bounds):
     call(0, 0, 1)
     assert call(3, BASE + (1 << 32), 1 << 20) == ckg.Device.code
     call(2, BASE + (1 << 32))
+
+
+def test_python_switch(bounds):
+    call, ckg = bounds
+    call(1, BASE + (1 << 34), 64)
+    ckg.set_bounds_checking(False)
+    assert call(3, BASE + (1 << 34), 128) == 0
+    ckg.set_bounds_checking(True)
+    assert call(3, BASE + (1 << 34), 128) == ckg.Device.code
+    call(2, BASE + (1 << 34))
