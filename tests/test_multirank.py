@@ -53,9 +53,10 @@ class _FakeServer:
     """Stands in for the GPU server: records each submission's owner and completes it 0.5 ms
     after submission."""
 
-    def __init__(self):
+    def __init__(self, fail_every=0):
         import time
         self.time, self.t0, self.times, self.seen = time, time.perf_counter(), [], []
+        self.fail_every, self.failures = fail_every, 0
 
     def _submit(self, owner):
         t = (self.time.perf_counter() - self.t0) * 1e6
@@ -73,6 +74,9 @@ class _FakeServer:
         return self._submit(o)
 
     def result_times(self, i, timeout_ms):
+        if self.fail_every and i % self.fail_every == self.fail_every - 1:
+            self.failures += 1
+            return 7, None, (0.0, 0.0, 0.0)  # an out-of-memory status
         return 0, None, self.times[i]
 
     def stats(self):
@@ -81,7 +85,7 @@ class _FakeServer:
         return dict.fromkeys(keys, 0)
 
 
-def _serving_worker(rank, world, port, owners, out):
+def _serving_worker(rank, world, port, owners, out, fail_every=(0, 0)):
     import numpy as np
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -89,14 +93,14 @@ def _serving_worker(rank, world, port, owners, out):
     router = b.load_package().OwnerRouter([b.Serving.key_bytes_per_owner()] * owners, world)
     sv = b.Serving.__new__(b.Serving)
     local = router.owners_of(rank)
-    sv.rng, sv.owners, sv.srv = np.random.default_rng(7), owners, _FakeServer()
+    sv.rng, sv.owners, sv.srv = np.random.default_rng(7), owners, _FakeServer(fail_every[rank])
     sv.steps = list(range(1, 8)) + [8 * k for k in range(1, 8)]
     sv.slot = {g: i for i, g in enumerate(local)}
     sv.inputs = {g: [("ct", g, lv) for lv in (23, 17, 11, 5)] for g in local}
     sv.diag = {23: "diag23", 11: "diag11"}
     sv.key_bytes, sv.register_s = len(local) * b.Serving.key_bytes_per_owner(), 0.0
     res = sv.measure(requests=64, load=0.7, dist=dist)
-    out[rank] = (res, sorted({local[o] for o in sv.srv.seen}), local, len(sv.srv.seen))
+    out[rank] = (res, sorted({local[o] for o in sv.srv.seen}), local, len(sv.srv.seen), sv.srv.failures)
     dist.barrier()
     dist.destroy_process_group()
 
@@ -117,6 +121,22 @@ def test_two_rank_routed_serving():
     assert set(r0[2]).isdisjoint(r1[2]) and sorted(r0[2] + r1[2]) == list(range(owners))
     assert set(r0[1]) <= set(r0[2]) and set(r1[1]) <= set(r1[2])
     assert r0[3] + r1[3] == 96 + 64 + 64  # warm-up, saturation and timed runs, split between ranks
+
+
+def test_two_rank_routed_serving_counts_failures():
+    """A rank whose server fails some requests: the pooled result counts every rank's failures,
+    serves the rest, and both ranks report the same pooled figures (no rank hangs on a failure)."""
+    owners = 6
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_serving_worker, args=(2, _free_port(), owners, out, (0, 5)), nprocs=2, join=True,
+                           start_method="spawn")
+        r0, r1 = out[0], out[1]
+    assert r0[0] == r1[0]
+    assert r0[4] == 0 and r1[4] > 0
+    assert r0[0]["failed"] == r1[4]
+    assert 0 < r0[0]["served"] < 64
 
 
 def test_owner_router_balances_key_bytes():
