@@ -139,6 +139,20 @@ def test_two_rank_routed_serving_counts_failures():
     assert 0 < r0[0]["served"] < 64
 
 
+def test_two_rank_routed_serving_with_an_idle_rank():
+    """One owner on two ranks: the rank without owners submits nothing, and both still finish the
+    same collective steps with the same pooled result."""
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_serving_worker, args=(2, _free_port(), 1, out), nprocs=2, join=True,
+                           start_method="spawn")
+        r0, r1 = out[0], out[1]
+    assert r0[0] == r1[0]
+    assert r0[2] == [0] and r1[2] == [] and r1[3] == 0
+    assert r0[0]["served"] == 64 and r0[0]["failed"] == 0
+
+
 def test_owner_router_balances_key_bytes():
     b = _bench()
     R = b.load_package().OwnerRouter
